@@ -1,0 +1,260 @@
+/*
+ * origami_gpu.h -- C ABI of the B200 force-and-integrate engine for origami's
+ * implicit-solvent MD hot path.
+ *
+ * origami (Rust) evaluates forces through
+ *   energy::total_force_with_scratch(&Structure, &TopologyGraph, &ForceField,
+ *        cutoff_a, include_sasa, &mut ForceScratch, &mut Vec<Vec3>)
+ *        -- crates/energy/src/forces.rs:78-128
+ * with per-atom caches built by ForceScratch::new (crates/energy/src/scratch.rs:143),
+ * energies through bonded_energy / nonbonded_energy / gb_energy
+ * (crates/energy/src/bonded.rs:34, nonbonded.rs:97, gb.rs:146), and steps with
+ * BAOAB + SHAKE inside run_langevin / run_remd / run_cotranslate
+ * (crates/dynamics/src/langevin.rs:128, remd.rs:136, cotranslate.rs:174).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions (all entry points):
+ *   - plain C types only; every pointer is borrowed for the duration of the
+ *     call; the engine owns its device memory.
+ *   - positions in Angstrom, velocities in Angstrom/fs, forces in kJ/mol/A,
+ *     energies in kJ/mol, masses in Da, temperatures in K, times in fs --
+ *     origami's unit system (crates/dynamics/src/langevin.rs:19-34).
+ *   - coordinate arrays are interleaved xyz, 3*n_atoms doubles, in origami's
+ *     atom order (residue order, then template order inside a residue).
+ *   - every function returns an og_status; nothing aborts the process.
+ *   - an engine is not thread safe; calls on one engine are stream ordered.
+ */
+#ifndef ORIGAMI_GPU_H
+#define ORIGAMI_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum og_status {
+  OG_OK = 0,
+  OG_E_BADARG = 1,     /* invalid argument (null pointer, size, index) */
+  OG_E_NONFINITE = 2,  /* a velocity or force became NaN/Inf (langevin.rs:316-319 "diverged") */
+  OG_E_SHAKE = 3,      /* SHAKE did not converge within max iterations (shake.rs:86-125) */
+  OG_E_TIMEOUT = 4,    /* a bounded device wait gave up */
+  OG_E_CUDA = 5,       /* CUDA runtime error (see og_last_error) */
+  OG_E_NOMEM = 6,      /* device or host allocation failed */
+  OG_E_STATE = 7,      /* call not valid in the engine's current state */
+  OG_E_DATA = 8,       /* force-field / template table missing or malformed */
+  OG_E_UNSUPPORTED = 9 /* feature not built into this library */
+} og_status;
+
+/* Human-readable text of the most recent error on this thread. */
+const char* og_last_error(void);
+const char* og_status_string(int status);
+/* Library version string, e.g. "origami-b200 0.1 (sm_100a)". */
+const char* og_version(void);
+
+/* -------------------------------------------------------------- topology
+ * Flat description of one molecular system: what origami's ForceScratch
+ * caches per atom (scratch.rs:35-133 -- charges, CHARMM LJ params incl. 1-4,
+ * GB rho / HCT scale) plus the TopologyGraph term lists with their force-field
+ * parameters already resolved (forcefield.rs:84-158 lookups) and the 1-2/1-3
+ * exclusion and 1-4 pair list (scratch.rs:233-251 rebuild_exclusions; graph
+ * predicates geom/src/topology_graph.rs:81-112).  Terms whose parameters are
+ * missing from the force field are simply absent, which is what the
+ * reference's `let Some(p) = ... else { continue }` skips do.
+ * Parameter units are CHARMM's (kcal/mol, Angstrom, degrees); the engine
+ * converts at the leaves exactly where origami does (units.rs).
+ */
+typedef struct og_topology {
+  int32_t n_atoms;
+  const double* charge;        /* e */
+  const double* rmin_half;     /* LJ Rmin/2, A */
+  const double* epsilon;       /* LJ epsilon, kcal/mol (positive) */
+  const double* rmin_half_14;  /* 1-4 Rmin/2 (equals rmin_half when the FF has none) */
+  const double* epsilon_14;    /* 1-4 epsilon */
+  const double* gb_rho;        /* intrinsic Born radius rho, A (gb.rs:58-68) */
+  const double* gb_scale;      /* HCT descreening scale (gb.rs:73-83) */
+  const double* mass;          /* Da (element.rs:27-37) */
+  const int32_t* element;      /* 0 H, 1 C, 2 N, 3 O, 4 P, 5 S */
+
+  int32_t n_bonds;
+  const int32_t* bond_atoms;   /* 2 per bond, a < b, sorted (topology_graph.rs:252) */
+  const double* bond_k;        /* kcal/mol/A^2, V = K (r - r0)^2 */
+  const double* bond_r0;       /* A */
+
+  int32_t n_angles;
+  const int32_t* angle_atoms;  /* 3 per angle, central atom in the middle */
+  const double* angle_k;       /* kcal/mol/rad^2 */
+  const double* angle_theta0;  /* degrees */
+
+  int32_t n_dihedrals;
+  const int32_t* dihedral_atoms;      /* 4 per dihedral, canonical (b < c) */
+  const int32_t* dihedral_term_start; /* n_dihedrals + 1 offsets into the term arrays */
+  int32_t n_dihedral_terms;
+  const double* term_k;               /* kcal/mol */
+  const int32_t* term_n;              /* multiplicity */
+  const double* term_delta;           /* degrees */
+
+  int32_t n_impropers;
+  const int32_t* improper_atoms; /* 4 per improper, central atom first */
+  const double* improper_k;      /* kcal/mol/rad^2 */
+  const double* improper_psi0;   /* degrees */
+
+  int32_t n_exclusions;
+  const int32_t* exclusion_atoms; /* 2 per pair, i < j, sorted */
+  const int8_t* exclusion_kind;   /* 1 = excluded (1-2 or 1-3), 2 = 1-4 pair */
+
+  int32_t n_constraints;            /* X-H bonds (shake.rs:47-76), bond order */
+  const int32_t* constraint_atoms;  /* 2 per constraint */
+  const double* constraint_length;  /* A (force-field r0) */
+} og_topology;
+
+/* ------------------------------------------------- host model (sequence ->
+ * system).  Restates origami's chain builder and topology graph so callers
+ * without a structure of their own can build one:
+ *   build_extended_chain / build_chain / append_residue  geom/src/builder.rs:50-90
+ *   build_topology_graph                                  geom/src/topology_graph.rs:134
+ *   ForceScratch::rebuild_params (per-atom params)        energy/src/scratch.rs:196
+ *   build_h_bond_constraints                              dynamics/src/shake.rs:47
+ * The force-field and template tables are read from the data directory next
+ * to the shared library (override with og_set_data_dir).
+ */
+typedef struct og_chain og_chain;
+
+og_status og_set_data_dir(const char* path);
+/* One-letter sequence; phi/psi/omega in radians (NAN = origami's defaults
+ * phi -120 deg, psi 140 deg, omega 180 deg). */
+og_status og_chain_build(const char* sequence, double phi, double psi, double omega, og_chain** out);
+/* Appends one residue at the C terminus (cotranslate.rs:204 append_residue). */
+og_status og_chain_append(og_chain* chain, char residue, double phi, double psi, double omega);
+og_status og_chain_n_atoms(const og_chain* chain, int32_t* n_atoms);
+og_status og_chain_n_residues(const og_chain* chain, int32_t* n_residues);
+/* Topology arrays stay valid until the chain is modified or freed. */
+og_status og_chain_topology(og_chain* chain, const og_topology** topo);
+og_status og_chain_get_positions(const og_chain* chain, double* xyz);
+og_status og_chain_set_positions(og_chain* chain, const double* xyz);
+/* Per-atom metadata: residue index, CHARMM atom-type index (chem atom_type.rs
+ * declaration order), and the atom name into a caller buffer (<= 8 chars + NUL). */
+og_status og_chain_atom_info(const og_chain* chain, int32_t atom, int32_t* residue,
+                             int32_t* atom_type, char name[8]);
+/* Counts of bonded tuples the force field could not parameterise
+ * (bonded.rs:21-23 missing_count; nonbonded.rs:92). */
+og_status og_chain_missing_params(const og_chain* chain, int32_t* missing);
+void og_chain_free(og_chain* chain);
+
+/* ------------------------------------------------------------------ engine */
+typedef struct og_params {
+  /* Cutoffs in A.  origami's integrator path uses 10 (LJ + reaction-field
+   * Coulomb, forces_nonbonded.rs:125), 20 (Born descreening, gb.rs:40) and 10
+   * (GB pair force, forces_gb.rs:33).  A value <= 0 or >= 1e30 means "no
+   * cutoff": all pairs, bare Coulomb (the reaction field's Rc -> infinity limit). */
+  double nb_cutoff;
+  double born_cutoff;
+  double gb_force_cutoff;
+  /* Integrator (LangevinOptions, langevin.rs:52-95). */
+  double dt_fs;
+  double friction_ps_inv;
+  int32_t constrain_h_bonds;  /* SHAKE X-H bonds, tol 1e-6 A^2, 64 iterations */
+  int32_t shake_max_iters;    /* 0 -> 64 */
+  double shake_tol_sq;        /* 0 -> 1e-6 */
+  /* Analytical PowerSasa hydrophobic force (analytical.rs:451); gamma scale as
+   * ORIGAMI_SASA_GAMMA_SCALE. */
+  int32_t include_sasa;
+  double sasa_gamma_scale;
+  /* Born radii: 0 = plain OBC-II descreening pass, 1 = learned radii. */
+  int32_t born_mode;
+  uint64_t seed;
+} og_params;
+
+/* Fills origami's defaults (10/20/10 A cutoffs, dt 1 fs, gamma 1 ps^-1, no
+ * SHAKE, no SASA, plain Born radii, seed 0). */
+void og_params_default(og_params* p);
+
+typedef struct og_energies {
+  double bond, angle, dihedral, improper;  /* bonded.rs BondedBreakdown */
+  double lj, coulomb;                      /* nonbonded.rs NonbondedBreakdown */
+  double gb, gb_self, gb_pair;             /* gb.rs GbBreakdown */
+  double sasa;
+  double total;
+  int32_t born_clamped;                    /* gb.rs GbBreakdown::clamped_count */
+  int32_t nb_pairs;                        /* pairs inside the LJ/Coulomb cutoff */
+} og_energies;
+
+typedef struct og_engine og_engine;
+
+/* Creates an engine on the current CUDA device.  Systems are added, then the
+ * engine is finalised (device upload, tile lists), then stepped. */
+og_status og_engine_create(const og_params* params, og_engine** out);
+/* Adds one system (a replica or an independent chain).  xyz = initial
+ * positions; temperature for its heat bath.  The topology is copied. */
+og_status og_engine_add_system(og_engine* e, const og_topology* topo, const double* xyz,
+                               double temperature_k, int32_t* system_index);
+og_status og_engine_finalize(og_engine* e);
+og_status og_engine_n_systems(const og_engine* e, int32_t* n);
+/* Runs kernels on this CUDA stream (cudaStream_t as void*; NULL = the
+ * engine's own stream). */
+og_status og_engine_set_stream(og_engine* e, void* cuda_stream);
+og_status og_engine_synchronize(og_engine* e);
+void og_engine_destroy(og_engine* e);
+
+/* Positions / velocities of one system, host arrays of 3*n_atoms doubles. */
+og_status og_set_positions(og_engine* e, int32_t sys, const double* xyz);
+og_status og_get_positions(og_engine* e, int32_t sys, double* xyz);
+og_status og_set_velocities(og_engine* e, int32_t sys, const double* v);
+og_status og_get_velocities(og_engine* e, int32_t sys, double* v);
+/* Draw Maxwell-Boltzmann velocities at the system's temperature with
+ * origami's own generator: xoshiro256++ seeded by SplitMix64 from `seed`,
+ * Box-Muller gaussians drawn x, y, z per atom in atom order (rng.rs:18-98,
+ * langevin.rs:487-513).  remove_com = 1 subtracts the centre-of-mass velocity
+ * as run_langevin does; 0 leaves it, as run_remd does with seed
+ * base + i * 0xC0FFEE for replica i (remd.rs:209-212). */
+og_status og_init_velocities(og_engine* e, int32_t sys, uint64_t seed, int32_t remove_com);
+og_status og_set_temperature(og_engine* e, int32_t sys, double temperature_k);
+
+/* Forces at the current positions of every system: replaces
+ * total_force_with_scratch (forces.rs:78).  f_out (optional) receives
+ * 3*n_atoms doubles for system `sys` (or nothing when NULL).  The same
+ * evaluation also leaves the forces on the device for the next og_step. */
+og_status og_compute_forces(og_engine* e, int32_t sys, double* f_out);
+/* Potential energy of system `sys` at its current positions, the sum that
+ * origami's REMD swap and L-BFGS line search use (remd.rs:529
+ * potential_energy, energy_eval.rs:20 total_energy_with_options): bonded +
+ * LJ/RF-Coulomb within nb_cutoff + GB (Born radii within born_cutoff, pair
+ * sum over ALL pairs, gb.rs:146-182) [+ SASA].  FP64 on the device.
+ * sys = -1 evaluates every system at once; out then holds n_systems entries. */
+og_status og_compute_energies(og_engine* e, int32_t sys, og_energies* out);
+/* Effective Born radii of system `sys` (gb.rs:203 compute_born_radii_into_scratch);
+ * out receives n_atoms doubles. */
+og_status og_get_born_radii(og_engine* e, int32_t sys, double* radii);
+
+/* Advance every system by n_steps BAOAB(+SHAKE) steps (the loop body of
+ * run_langevin, langevin.rs:223-342).  Per-system status words record
+ * divergence and SHAKE failures; the call returns OG_E_NONFINITE if any
+ * system diverged (it is then frozen, like REMD skips diverged replicas). */
+og_status og_step(og_engine* e, int32_t n_steps);
+/* Per-system counters: steps run, SHAKE failures, diverged flag. */
+og_status og_system_stats(og_engine* e, int32_t sys, int64_t* steps, int64_t* shake_failures,
+                          int32_t* diverged);
+/* Instantaneous kinetic energy (langevin.rs:469) and temperature with
+ * 3N degrees of freedom. */
+og_status og_kinetic(og_engine* e, int32_t sys, double* ke_kj_mol, double* temperature_k);
+
+/* Replica exchange (remd.rs:425-474): for each adjacent pair (a, a+1) with
+ * a = parity, parity+2, ... of the temperature-sorted systems, Metropolis on
+ * delta = (beta_a - beta_b)(E_a - E_b) with uniforms u[pair]; on acceptance
+ * positions, velocities and forces are exchanged and velocities rescaled by
+ * sqrt(T_a/T_b).  accepted[pair] (optional) receives 0/1. */
+og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int32_t* accepted);
+
+/* CUDA-event timing of the kernels the last og_step launched: fills up to
+ * `cap` entries of (kernel id, milliseconds) summed over the call. */
+typedef struct og_kernel_time { const char* name; double ms; int64_t launches; } og_kernel_time;
+og_status og_profile_enable(og_engine* e, int32_t on);
+og_status og_profile_read(og_engine* e, og_kernel_time* out, int32_t cap, int32_t* n_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORIGAMI_GPU_H */

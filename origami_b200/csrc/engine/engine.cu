@@ -1,0 +1,1196 @@
+// og_engine_*: the device half of the C ABI.
+//
+// An engine holds any number of systems (REMD replicas of one chain or
+// independent chains of different lengths) concatenated in one padded atom
+// space: every system starts on a 32-atom tile boundary, so a tile never
+// straddles two systems.  Pair work is a list of (i-block, j-tile range)
+// items; bonded terms, SHAKE clusters and per-system state are flat arrays
+// with global atom indices.  One MD step is a fixed sequence of launches that
+// is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../../include/origami_gpu.h"
+#include "../host/status.h"
+#include "common.cuh"
+#include "pair_kernels.cuh"
+#include "step_kernels.cuh"
+
+namespace ogk {
+int pair_warps_per_cta();
+}
+
+namespace {
+
+using ogk::kTile;
+
+bool no_cutoff(double c) { return !(c > 0.0) || c >= 1e30; }
+
+og_status cuda_fail(cudaError_t e, const char* what) {
+  return og_fail(OG_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define OG_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+template <class T>
+struct DVec {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DVec() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+  }
+  cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
+    cudaError_t e = alloc(h.size());
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+struct TopoCopy {
+  int n = 0;
+  std::vector<double> charge, rmin, eps, rmin14, eps14, rho, scale, mass;
+  std::vector<int32_t> element;
+  std::vector<int32_t> bonds, angles, dihedrals, dih_start, term_n, impropers, excl, cons;
+  std::vector<double> bond_k, bond_r0, angle_k, angle_t0, term_k, term_delta, imp_k, imp_psi0, cons_d;
+  std::vector<int8_t> excl_kind;
+};
+
+template <class T>
+std::vector<T> copy_arr(const T* p, size_t n) {
+  return (p && n) ? std::vector<T>(p, p + n) : std::vector<T>();
+}
+
+og_status copy_topology(const og_topology* t, TopoCopy* c) {
+  const int n = t->n_atoms;
+  if (n <= 0) return og_fail(OG_E_BADARG, "topology has no atoms");
+  if (!t->charge || !t->rmin_half || !t->epsilon || !t->rmin_half_14 || !t->epsilon_14 || !t->gb_rho ||
+      !t->gb_scale || !t->mass || !t->element)
+    return og_fail(OG_E_BADARG, "topology per-atom array missing");
+  c->n = n;
+  c->charge = copy_arr(t->charge, n);
+  c->rmin = copy_arr(t->rmin_half, n);
+  c->eps = copy_arr(t->epsilon, n);
+  c->rmin14 = copy_arr(t->rmin_half_14, n);
+  c->eps14 = copy_arr(t->epsilon_14, n);
+  c->rho = copy_arr(t->gb_rho, n);
+  c->scale = copy_arr(t->gb_scale, n);
+  c->mass = copy_arr(t->mass, n);
+  c->element = copy_arr(t->element, n);
+  c->bonds = copy_arr(t->bond_atoms, 2 * static_cast<size_t>(t->n_bonds));
+  c->bond_k = copy_arr(t->bond_k, t->n_bonds);
+  c->bond_r0 = copy_arr(t->bond_r0, t->n_bonds);
+  c->angles = copy_arr(t->angle_atoms, 3 * static_cast<size_t>(t->n_angles));
+  c->angle_k = copy_arr(t->angle_k, t->n_angles);
+  c->angle_t0 = copy_arr(t->angle_theta0, t->n_angles);
+  c->dihedrals = copy_arr(t->dihedral_atoms, 4 * static_cast<size_t>(t->n_dihedrals));
+  c->dih_start = copy_arr(t->dihedral_term_start, static_cast<size_t>(t->n_dihedrals) + 1);
+  c->term_k = copy_arr(t->term_k, t->n_dihedral_terms);
+  c->term_n = copy_arr(t->term_n, t->n_dihedral_terms);
+  c->term_delta = copy_arr(t->term_delta, t->n_dihedral_terms);
+  c->impropers = copy_arr(t->improper_atoms, 4 * static_cast<size_t>(t->n_impropers));
+  c->imp_k = copy_arr(t->improper_k, t->n_impropers);
+  c->imp_psi0 = copy_arr(t->improper_psi0, t->n_impropers);
+  c->excl = copy_arr(t->exclusion_atoms, 2 * static_cast<size_t>(t->n_exclusions));
+  c->excl_kind = copy_arr(t->exclusion_kind, t->n_exclusions);
+  c->cons = copy_arr(t->constraint_atoms, 2 * static_cast<size_t>(t->n_constraints));
+  c->cons_d = copy_arr(t->constraint_length, t->n_constraints);
+  if (t->n_dihedrals > 0 && c->dih_start.back() != t->n_dihedral_terms)
+    return og_fail(OG_E_BADARG, "dihedral_term_start does not end at n_dihedral_terms");
+  auto bad_idx = [n](const std::vector<int32_t>& v) {
+    for (int32_t k : v)
+      if (k < 0 || k >= n) return true;
+    return false;
+  };
+  if (bad_idx(c->bonds) || bad_idx(c->angles) || bad_idx(c->dihedrals) || bad_idx(c->impropers) ||
+      bad_idx(c->excl) || bad_idx(c->cons))
+    return og_fail(OG_E_BADARG, "topology atom index out of range");
+  return OG_OK;
+}
+
+struct SysHost {
+  TopoCopy topo;
+  std::vector<double> xyz;
+  double temperature = 310.0;
+  int atom_begin = 0, n_tiles = 0, tile_begin = 0;
+};
+
+double deg2rad(double d) { return d * M_PI / 180.0; }
+
+}  // namespace
+
+struct og_engine {
+  og_params p{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<SysHost> sys;
+  bool finalized = false;
+  bool forces_valid = false;
+  int n_padded = 0, n_tiles = 0;
+
+  // per padded atom
+  DVec<double> x, y, z, vx, vy, vz, rx, ry, rz, mass, inv_mass, q, rmin, eps, rmin14, eps14, rho, rho_tilde, srho;
+  DVec<double> born_r, born_r64, integral64, e_lj, e_coul, e_gb, e_self;
+  DVec<unsigned long long> fx, fy, fz, born_sum;
+  DVec<int32_t> atom_sys, local_idx, atom_valid, n_pairs;
+  DVec<float4> pq, lj, gb;
+  DVec<double4> origin;
+  DVec<ogk::SysState> sys_state;
+  // pair work
+  DVec<ogk::PairWork> work;
+  DVec<int32_t> jlist, mask_begin;
+  DVec<ogk::TileMaskRef> mask_refs;
+  DVec<uint32_t> mask_ex, mask_14;
+  DVec<int32_t> excl_row, excl_col;
+  DVec<int8_t> excl_kind;
+  int n_work = 0;
+  // bonded
+  DVec<int2> bond_atoms, dih_terms;
+  DVec<int4> angle_atoms, dih_atoms, imp_atoms;
+  DVec<double> bond_k, bond_r0, angle_k, angle_t0, term_k, term_delta, imp_k, imp_psi0, bonded_e;
+  DVec<int32_t> term_n;
+  int n_bonds = 0, n_angles = 0, n_dih = 0, n_imp = 0;
+  // SHAKE
+  DVec<int32_t> cl_start, cl_sys;
+  DVec<int2> cons_atoms;
+  DVec<double> cons_d2;
+  int n_clusters = 0;
+  // reductions
+  DVec<int32_t> seg_begin, seg_end;  // [atoms per sys | bonds | angles | dihedrals | impropers], 5*n_sys
+  DVec<double> seg_out;
+  DVec<int32_t> clamp_count, error_flag, sys_nonfinite;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  // profiling
+  bool profile = false;
+  std::map<std::string, std::pair<double, long long>> prof;
+  std::vector<std::string> prof_names;
+
+  ~og_engine() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+
+  ogk::AtomArrays atoms() {
+    ogk::AtomArrays a{};
+    a.n_padded = n_padded;
+    a.x = x.p; a.y = y.p; a.z = z.p;
+    a.vx = vx.p; a.vy = vy.p; a.vz = vz.p;
+    a.rx = rx.p; a.ry = ry.p; a.rz = rz.p;
+    a.fx = fx.p; a.fy = fy.p; a.fz = fz.p;
+    a.born_sum = born_sum.p;
+    a.mass = mass.p;
+    a.atom_sys = atom_sys.p;
+    a.local_idx = local_idx.p;
+    a.q = q.p;
+    a.rho = rho.p;
+    a.rho_tilde = rho_tilde.p;
+    a.srho = srho.p;
+    a.pq = pq.p;
+    a.gb = gb.p;
+    a.origin = origin.p;
+    a.born_r = born_r.p;
+    a.sys = sys_state.p;
+    a.sys_nonfinite = sys_nonfinite.p;
+    return a;
+  }
+
+  ogk::PairArgs pair_args() {
+    ogk::PairArgs a{};
+    a.pq = pq.p; a.lj = lj.p; a.gb = gb.p; a.origin = origin.p; a.atom_valid = atom_valid.p;
+    a.work = work.p; a.n_work = n_work; a.jlist = jlist.p;
+    a.mask_begin = mask_begin.p; a.mask_refs = mask_refs.p; a.mask_ex = mask_ex.p; a.mask_14 = mask_14.p;
+    a.fx = fx.p; a.fy = fy.p; a.fz = fz.p; a.born_sum = born_sum.p;
+    auto c2 = [](double c) { return no_cutoff(c) ? INFINITY : static_cast<float>(c * c); };
+    a.nb_c2 = c2(p.nb_cutoff);
+    a.gb_c2 = c2(p.gb_force_cutoff);
+    a.born_c2 = c2(p.born_cutoff);
+    a.inv_rc3 = no_cutoff(p.nb_cutoff) ? 0.0f
+                                       : static_cast<float>(1.0 / (p.nb_cutoff * p.nb_cutoff * p.nb_cutoff));
+    a.coul_kj = static_cast<float>(ogk::kCoulomb * ogk::kKcalToKj);
+    a.lj_kj12 = static_cast<float>(12.0 * ogk::kKcalToKj);
+    a.gb_pref_kj = static_cast<float>((1.0 - 1.0 / ogk::kEpsWater) * ogk::kCoulomb * ogk::kKcalToKj);
+    a.error_flag = error_flag.p;
+    a.atom_sys = atom_sys.p;
+    a.sys_nonfinite = sys_nonfinite.p;
+    return a;
+  }
+
+  ogk::BondedArgs bonded_args() {
+    ogk::BondedArgs a{};
+    a.x = x.p; a.y = y.p; a.z = z.p;
+    a.n_bonds = n_bonds; a.n_angles = n_angles; a.n_dihedrals = n_dih; a.n_impropers = n_imp;
+    a.bond_atoms = bond_atoms.p; a.bond_k = bond_k.p; a.bond_r0 = bond_r0.p;
+    a.angle_atoms = angle_atoms.p; a.angle_k = angle_k.p; a.angle_t0 = angle_t0.p;
+    a.dih_atoms = dih_atoms.p; a.dih_terms = dih_terms.p;
+    a.term_k = term_k.p; a.term_n = term_n.p; a.term_delta = term_delta.p;
+    a.imp_atoms = imp_atoms.p; a.imp_k = imp_k.p; a.imp_psi0 = imp_psi0.p;
+    a.fx = fx.p; a.fy = fy.p; a.fz = fz.p;
+    a.energy = bonded_e.p;
+    a.atom_sys = atom_sys.p;
+    a.sys_nonfinite = sys_nonfinite.p;
+    return a;
+  }
+
+  ogk::StepArgs step_args() {
+    ogk::StepArgs s{};
+    s.at = atoms();
+    s.half_dt = 0.5 * p.dt_fs;
+    s.alpha = std::exp(-p.friction_ps_inv * p.dt_fs * 1.0e-3);
+    s.seed_lo = static_cast<uint32_t>(p.seed);
+    s.seed_hi = static_cast<uint32_t>(p.seed >> 32);
+    s.use_shake = (p.constrain_h_bonds && n_clusters > 0) ? 1 : 0;
+    return s;
+  }
+
+  ogk::ShakeArgs shake_args() {
+    ogk::ShakeArgs a{};
+    a.x = x.p; a.y = y.p; a.z = z.p;
+    a.rx = rx.p; a.ry = ry.p; a.rz = rz.p;
+    a.inv_mass = inv_mass.p;
+    a.n_clusters = n_clusters;
+    a.cluster_start = cl_start.p;
+    a.cluster_sys = cl_sys.p;
+    a.cons_atoms = cons_atoms.p;
+    a.cons_d2 = cons_d2.p;
+    a.tol_sq = p.shake_tol_sq > 0.0 ? p.shake_tol_sq : 1e-6;
+    a.max_iters = p.shake_max_iters > 0 ? p.shake_max_iters : 64;
+    a.sys = sys_state.p;
+    return a;
+  }
+
+  // --- profiling helpers (used only outside graph capture)
+  struct Timer {
+    og_engine* e;
+    const char* name;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer(og_engine* eng, const char* n) : e(eng), name(n) {
+      if (!e->profile) return;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, e->stream);
+    }
+    ~Timer() {
+      if (!e->profile) return;
+      cudaEventRecord(b, e->stream);
+      cudaEventSynchronize(b);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, a, b);
+      auto& slot = e->prof[name];
+      slot.first += ms;
+      slot.second += 1;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  };
+
+  // Force evaluation on the device (positions already packed and
+  // accumulators zeroed): Born pass, radii, fused pair force, bonded terms.
+  void enqueue_forces() {
+    ogk::PairArgs pa = pair_args();
+    ogk::AtomArrays at = atoms();
+    {
+      Timer t(this, "born_pass");
+      ogk::launch_born_pass(pa, stream);
+    }
+    {
+      Timer t(this, "born_finalize");
+      ogk::launch_born_finalize(at, nullptr, born_r.p, true, nullptr, stream);
+    }
+    {
+      Timer t(this, "force_pass");
+      ogk::launch_force_pass(pa, stream);
+    }
+    {
+      Timer t(this, "bonded");
+      ogk::launch_bonded_forces(bonded_args(), stream);
+    }
+  }
+
+  void enqueue_step() {
+    ogk::StepArgs sa = step_args();
+    {
+      Timer t(this, "step_pre");
+      ogk::launch_step_pre(sa, stream);
+    }
+    if (sa.use_shake) {
+      Timer t(this, "shake");
+      ogk::launch_shake(shake_args(), stream);
+    }
+    {
+      Timer t(this, "step_mid");
+      ogk::launch_step_mid(sa, stream);
+    }
+    if (sa.use_shake) {
+      Timer t(this, "shake");
+      ogk::launch_shake(shake_args(), stream);
+    }
+    {
+      Timer t(this, "step_post");
+      ogk::launch_step_post(sa, stream);
+    }
+    enqueue_forces();
+    {
+      Timer t(this, "step_end");
+      ogk::launch_step_end(sa, stream);
+    }
+  }
+};
+
+namespace {
+
+og_status check_ready(const og_engine* e) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  if (!e->finalized) return og_fail(OG_E_STATE, "engine not finalized");
+  return OG_OK;
+}
+
+og_status check_sys(const og_engine* e, int32_t s) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (s < 0 || s >= static_cast<int32_t>(e->sys.size())) return og_fail(OG_E_BADARG, "system index out of range");
+  return OG_OK;
+}
+
+og_status launch_check(const char* what) {
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return cuda_fail(err, what);
+  return OG_OK;
+}
+
+og_status read_status(og_engine* e, std::vector<ogk::SysState>* out) {
+  out->resize(e->sys.size());
+  OG_CUDA(cudaMemcpyAsync(out->data(), e->sys_state.p, sizeof(ogk::SysState) * e->sys.size(),
+                          cudaMemcpyDeviceToHost, e->stream));
+  int32_t err_flag = 0;
+  OG_CUDA(cudaMemcpyAsync(&err_flag, e->error_flag.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  if (err_flag & ogk::kStatusTimeout) return og_fail(OG_E_TIMEOUT, "a pair-kernel pipeline wait timed out");
+  return OG_OK;
+}
+
+// xoshiro256++ / SplitMix64 / Box-Muller exactly as dynamics/src/rng.rs.
+struct Xoshiro {
+  uint64_t s[4];
+  bool has_spare = false;
+  double spare = 0.0;
+  explicit Xoshiro(uint64_t seed) {
+    uint64_t sm = seed;
+    for (int k = 0; k < 4; ++k) {
+      sm += 0x9e3779b97f4a7c15ULL;
+      uint64_t z = sm;
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+      s[k] = z ^ (z >> 31);
+    }
+  }
+  static uint64_t rotl(uint64_t v, int k) { return (v << k) | (v >> (64 - k)); }
+  uint64_t next_u64() {
+    uint64_t result = rotl(s[0] + s[3], 23) + s[0];
+    uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return result;
+  }
+  double next_f64() { return static_cast<double>(next_u64() >> 11) * (1.0 / static_cast<double>(1ULL << 53)); }
+  double gaussian() {
+    if (has_spare) {
+      has_spare = false;
+      return spare;
+    }
+    double u1 = next_f64();
+    while (u1 <= 0.0) u1 = next_f64();
+    double u2 = next_f64();
+    double r = std::sqrt(-2.0 * std::log(u1));
+    double th = 2.0 * M_PI * u2;
+    spare = r * std::sin(th);
+    has_spare = true;
+    return r * std::cos(th);
+  }
+};
+
+template <class T>
+og_status copy_sys_range(og_engine* e, const DVec<T>& v, int s, T* host) {
+  const SysHost& sh = e->sys[s];
+  OG_CUDA(cudaMemcpyAsync(host, v.p + sh.atom_begin, sizeof(T) * sh.topo.n, cudaMemcpyDeviceToHost, e->stream));
+  return OG_OK;
+}
+
+// Interleaved xyz <-> SoA device arrays of one system.
+og_status get_xyz(og_engine* e, int s, const DVec<double>& a, const DVec<double>& b, const DVec<double>& c,
+                  double* out) {
+  const int n = e->sys[s].topo.n;
+  std::vector<double> hx(n), hy(n), hz(n);
+  og_status st;
+  if ((st = copy_sys_range(e, a, s, hx.data())) != OG_OK) return st;
+  if ((st = copy_sys_range(e, b, s, hy.data())) != OG_OK) return st;
+  if ((st = copy_sys_range(e, c, s, hz.data())) != OG_OK) return st;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  for (int i = 0; i < n; ++i) {
+    out[3 * i] = hx[i];
+    out[3 * i + 1] = hy[i];
+    out[3 * i + 2] = hz[i];
+  }
+  return OG_OK;
+}
+
+og_status set_xyz(og_engine* e, int s, DVec<double>& a, DVec<double>& b, DVec<double>& c, const double* in) {
+  const SysHost& sh = e->sys[s];
+  const int n = sh.topo.n;
+  std::vector<double> hx(n), hy(n), hz(n);
+  for (int i = 0; i < n; ++i) {
+    hx[i] = in[3 * i];
+    hy[i] = in[3 * i + 1];
+    hz[i] = in[3 * i + 2];
+  }
+  OG_CUDA(cudaMemcpyAsync(a.p + sh.atom_begin, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
+  OG_CUDA(cudaMemcpyAsync(b.p + sh.atom_begin, hy.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
+  OG_CUDA(cudaMemcpyAsync(c.p + sh.atom_begin, hz.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status finalize_impl(og_engine* e) {
+  const int n_sys = static_cast<int>(e->sys.size());
+  if (n_sys == 0) return og_fail(OG_E_STATE, "no systems added");
+  cudaStream_t st = e->stream;
+
+  // ---- layout
+  int atom = 0;
+  for (auto& s : e->sys) {
+    s.atom_begin = atom;
+    s.n_tiles = (s.topo.n + kTile - 1) / kTile;
+    s.tile_begin = atom / kTile;
+    atom += s.n_tiles * kTile;
+  }
+  e->n_padded = atom;
+  e->n_tiles = atom / kTile;
+  const int np = e->n_padded;
+
+  // ---- per-atom arrays
+  std::vector<double> hx(np), hy(np), hz(np), hm(np, 1.0), him(np, 1.0), hq(np, 0.0), hrm(np, 0.0), hep(np, 0.0),
+      hrm14(np, 0.0), hep14(np, 0.0), hrho(np, 1.0), hrt(np, 1.0), hsr(np, 0.0);
+  std::vector<int32_t> hsys(np, -1), hloc(np, 0), hvalid(np, 0);
+  std::vector<float4> hlj(np, make_float4(0, 0, 0, 0));
+  for (int si = 0; si < n_sys; ++si) {
+    const SysHost& s = e->sys[si];
+    const TopoCopy& t = s.topo;
+    for (int k = 0; k < t.n; ++k) {
+      const int i = s.atom_begin + k;
+      hx[i] = s.xyz[3 * k];
+      hy[i] = s.xyz[3 * k + 1];
+      hz[i] = s.xyz[3 * k + 2];
+      hm[i] = t.mass[k];
+      him[i] = 1.0 / t.mass[k];
+      hq[i] = t.charge[k];
+      hrm[i] = t.rmin[k];
+      hep[i] = t.eps[k];
+      hrm14[i] = t.rmin14[k];
+      hep14[i] = t.eps14[k];
+      hrho[i] = t.rho[k];
+      hrt[i] = t.rho[k] - ogk::kObcOffset;
+      hsr[i] = t.scale[k] * hrt[i];
+      hsys[i] = si;
+      hloc[i] = k;
+      hvalid[i] = 1;
+      hlj[i] = make_float4(static_cast<float>(t.rmin[k]), static_cast<float>(std::sqrt(t.eps[k])),
+                           static_cast<float>(t.rmin14[k]), static_cast<float>(std::sqrt(t.eps14[k])));
+    }
+  }
+  OG_CUDA(e->x.upload(hx, st)); OG_CUDA(e->y.upload(hy, st)); OG_CUDA(e->z.upload(hz, st));
+  OG_CUDA(e->mass.upload(hm, st)); OG_CUDA(e->inv_mass.upload(him, st)); OG_CUDA(e->q.upload(hq, st));
+  OG_CUDA(e->rmin.upload(hrm, st)); OG_CUDA(e->eps.upload(hep, st));
+  OG_CUDA(e->rmin14.upload(hrm14, st)); OG_CUDA(e->eps14.upload(hep14, st));
+  OG_CUDA(e->rho.upload(hrho, st)); OG_CUDA(e->rho_tilde.upload(hrt, st)); OG_CUDA(e->srho.upload(hsr, st));
+  OG_CUDA(e->atom_sys.upload(hsys, st)); OG_CUDA(e->local_idx.upload(hloc, st));
+  OG_CUDA(e->atom_valid.upload(hvalid, st)); OG_CUDA(e->lj.upload(hlj, st));
+  std::vector<double> zeros(np, 0.0);
+  OG_CUDA(e->vx.upload(zeros, st)); OG_CUDA(e->vy.upload(zeros, st)); OG_CUDA(e->vz.upload(zeros, st));
+  OG_CUDA(e->rx.upload(zeros, st)); OG_CUDA(e->ry.upload(zeros, st)); OG_CUDA(e->rz.upload(zeros, st));
+  for (auto* v : {&e->born_r, &e->born_r64, &e->integral64, &e->e_lj, &e->e_coul, &e->e_gb, &e->e_self})
+    OG_CUDA(v->alloc(np));
+  for (auto* v : {&e->fx, &e->fy, &e->fz, &e->born_sum}) OG_CUDA(v->alloc(np));
+  OG_CUDA(e->n_pairs.alloc(np));
+  OG_CUDA(e->pq.alloc(np));
+  OG_CUDA(e->gb.alloc(np));
+  OG_CUDA(e->origin.alloc(e->n_tiles));
+
+  // ---- per-system state
+  std::vector<ogk::SysState> hs(n_sys);
+  for (int si = 0; si < n_sys; ++si) {
+    const SysHost& s = e->sys[si];
+    const int ncons = static_cast<int>(s.topo.cons_d.size());
+    const double dof = 3.0 * s.topo.n;
+    hs[si] = ogk::SysState{};
+    hs[si].temperature = s.temperature;
+    hs[si].kbt = ogk::kBoltzmann * s.temperature;
+    hs[si].dof_corr = (e->p.constrain_h_bonds && ncons > 0) ? dof / std::max(dof - ncons, 1.0) : 1.0;
+    hs[si].atom_begin = s.atom_begin;
+    hs[si].n_atoms = s.topo.n;
+  }
+  OG_CUDA(e->sys_state.upload(hs, st));
+
+  // ---- pair work: i-blocks of W tiles x all tiles of the system, split so
+  // that the grid covers the GPU several times.
+  const int W = ogk::pair_warps_per_cta();
+  int dev = 0, n_sm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  long long blocks = 0;
+  for (const auto& s : e->sys) blocks += (s.n_tiles + W - 1) / W;
+  const long long target = static_cast<long long>(n_sm) * 8;
+  std::vector<int32_t> hj;
+  std::vector<ogk::PairWork> hw;
+  for (const auto& s : e->sys) {
+    const int jb = static_cast<int>(hj.size());
+    for (int t = 0; t < s.n_tiles; ++t) hj.push_back(s.tile_begin + t);
+    const int je = static_cast<int>(hj.size());
+    int split = 1;
+    if (blocks < target) split = static_cast<int>(std::min<long long>((target + blocks - 1) / blocks, s.n_tiles / 4 + 1));
+    split = std::max(split, 1);
+    const int per = (s.n_tiles + split - 1) / split;
+    for (int t0 = 0; t0 < s.n_tiles; t0 += W)
+      for (int j0 = jb; j0 < je; j0 += per)
+        hw.push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + per)});
+  }
+  e->n_work = static_cast<int>(hw.size());
+  OG_CUDA(e->work.upload(hw, st));
+  OG_CUDA(e->jlist.upload(hj, st));
+
+  // ---- exclusion masks (per ordered tile pair) and the FP64 CSR
+  std::map<std::pair<int, int>, int> mask_of;  // (ti, tj) -> block
+  std::vector<uint32_t> mex, m14;
+  auto block = [&](int ti, int tj) {
+    auto it = mask_of.find({ti, tj});
+    if (it != mask_of.end()) return it->second;
+    int b = static_cast<int>(mask_of.size());
+    mask_of[{ti, tj}] = b;
+    mex.resize(static_cast<size_t>(b + 1) * kTile, 0u);
+    m14.resize(static_cast<size_t>(b + 1) * kTile, 0u);
+    return b;
+  };
+  std::vector<std::vector<std::pair<int, int8_t>>> rows(np);
+  for (const auto& s : e->sys) {
+    for (int t = 0; t < s.n_tiles; ++t) {  // self pairs on the diagonal
+      const int tile = s.tile_begin + t;
+      const int b = block(tile, tile);
+      for (int l = 0; l < kTile; ++l) mex[static_cast<size_t>(b) * kTile + l] |= 1u << l;
+    }
+    const auto& ex = s.topo.excl;
+    for (size_t k = 0; k < s.topo.excl_kind.size(); ++k) {
+      const int i = s.atom_begin + ex[2 * k], j = s.atom_begin + ex[2 * k + 1];
+      const int8_t kind = s.topo.excl_kind[k];
+      rows[i].push_back({j, kind});
+      rows[j].push_back({i, kind});
+      for (int dir = 0; dir < 2; ++dir) {
+        const int a = dir ? j : i, c = dir ? i : j;
+        const int b = block(a / kTile, c / kTile);
+        const size_t w = static_cast<size_t>(b) * kTile + (a % kTile);
+        if (kind == 1) mex[w] |= 1u << (c % kTile);
+        else m14[w] |= 1u << (c % kTile);
+      }
+    }
+  }
+  std::vector<int32_t> hmb(e->n_tiles + 1, 0);
+  std::vector<ogk::TileMaskRef> hmr;
+  {
+    std::vector<std::vector<ogk::TileMaskRef>> per_tile(e->n_tiles);
+    for (const auto& kv : mask_of) per_tile[kv.first.first].push_back({kv.first.second, kv.second});
+    for (int t = 0; t < e->n_tiles; ++t) {
+      std::sort(per_tile[t].begin(), per_tile[t].end(),
+                [](const ogk::TileMaskRef& a, const ogk::TileMaskRef& b) { return a.j_tile < b.j_tile; });
+      hmb[t] = static_cast<int32_t>(hmr.size());
+      hmr.insert(hmr.end(), per_tile[t].begin(), per_tile[t].end());
+    }
+    hmb[e->n_tiles] = static_cast<int32_t>(hmr.size());
+  }
+  OG_CUDA(e->mask_begin.upload(hmb, st));
+  OG_CUDA(e->mask_refs.upload(hmr, st));
+  OG_CUDA(e->mask_ex.upload(mex, st));
+  OG_CUDA(e->mask_14.upload(m14, st));
+  std::vector<int32_t> hrow(np + 1, 0), hcol;
+  std::vector<int8_t> hkind;
+  for (int i = 0; i < np; ++i) {
+    auto& r = rows[i];
+    std::sort(r.begin(), r.end());
+    hrow[i] = static_cast<int32_t>(hcol.size());
+    for (auto& pr : r) {
+      hcol.push_back(pr.first);
+      hkind.push_back(pr.second);
+    }
+  }
+  hrow[np] = static_cast<int32_t>(hcol.size());
+  OG_CUDA(e->excl_row.upload(hrow, st));
+  OG_CUDA(e->excl_col.upload(hcol, st));
+  OG_CUDA(e->excl_kind.upload(hkind, st));
+
+  // ---- bonded terms (global atom indices, angles in radians)
+  std::vector<int2> hb, hdt;
+  std::vector<int4> ha, hd, hi;
+  std::vector<double> hbk, hbr, hak, hat, htk, htd, hik, hip;
+  std::vector<int32_t> htn;
+  std::vector<int32_t> sb(5 * n_sys), se(5 * n_sys);
+  for (int si = 0; si < n_sys; ++si) {
+    const SysHost& s = e->sys[si];
+    const TopoCopy& t = s.topo;
+    const int o = s.atom_begin;
+    sb[si] = o;
+    se[si] = o + t.n;
+    sb[n_sys + si] = static_cast<int32_t>(hb.size());
+    for (size_t k = 0; k < t.bond_k.size(); ++k) {
+      hb.push_back(make_int2(o + t.bonds[2 * k], o + t.bonds[2 * k + 1]));
+      hbk.push_back(t.bond_k[k]);
+      hbr.push_back(t.bond_r0[k]);
+    }
+    se[n_sys + si] = static_cast<int32_t>(hb.size());
+    sb[2 * n_sys + si] = static_cast<int32_t>(ha.size());
+    for (size_t k = 0; k < t.angle_k.size(); ++k) {
+      ha.push_back(make_int4(o + t.angles[3 * k], o + t.angles[3 * k + 1], o + t.angles[3 * k + 2], 0));
+      hak.push_back(t.angle_k[k]);
+      hat.push_back(deg2rad(t.angle_t0[k]));
+    }
+    se[2 * n_sys + si] = static_cast<int32_t>(ha.size());
+    sb[3 * n_sys + si] = static_cast<int32_t>(hd.size());
+    const size_t ndih = t.dihedrals.size() / 4;
+    for (size_t k = 0; k < ndih; ++k) {
+      hd.push_back(make_int4(o + t.dihedrals[4 * k], o + t.dihedrals[4 * k + 1], o + t.dihedrals[4 * k + 2],
+                             o + t.dihedrals[4 * k + 3]));
+      const int base = static_cast<int>(htk.size());
+      for (int m = t.dih_start[k]; m < t.dih_start[k + 1]; ++m) {
+        htk.push_back(t.term_k[m]);
+        htn.push_back(t.term_n[m]);
+        htd.push_back(deg2rad(t.term_delta[m]));
+      }
+      hdt.push_back(make_int2(base, static_cast<int>(htk.size())));
+    }
+    se[3 * n_sys + si] = static_cast<int32_t>(hd.size());
+    sb[4 * n_sys + si] = static_cast<int32_t>(hi.size());
+    for (size_t k = 0; k < t.imp_k.size(); ++k) {
+      hi.push_back(make_int4(o + t.impropers[4 * k], o + t.impropers[4 * k + 1], o + t.impropers[4 * k + 2],
+                             o + t.impropers[4 * k + 3]));
+      hik.push_back(t.imp_k[k]);
+      hip.push_back(deg2rad(t.imp_psi0[k]));
+    }
+    se[4 * n_sys + si] = static_cast<int32_t>(hi.size());
+  }
+  e->n_bonds = static_cast<int>(hb.size());
+  e->n_angles = static_cast<int>(ha.size());
+  e->n_dih = static_cast<int>(hd.size());
+  e->n_imp = static_cast<int>(hi.size());
+  // Segments of the bonded energy array: bonds, then angles, dihedrals, impropers.
+  for (int si = 0; si < n_sys; ++si) {
+    sb[2 * n_sys + si] += e->n_bonds; se[2 * n_sys + si] += e->n_bonds;
+    sb[3 * n_sys + si] += e->n_bonds + e->n_angles; se[3 * n_sys + si] += e->n_bonds + e->n_angles;
+    sb[4 * n_sys + si] += e->n_bonds + e->n_angles + e->n_dih;
+    se[4 * n_sys + si] += e->n_bonds + e->n_angles + e->n_dih;
+  }
+  OG_CUDA(e->bond_atoms.upload(hb, st)); OG_CUDA(e->bond_k.upload(hbk, st)); OG_CUDA(e->bond_r0.upload(hbr, st));
+  OG_CUDA(e->angle_atoms.upload(ha, st)); OG_CUDA(e->angle_k.upload(hak, st)); OG_CUDA(e->angle_t0.upload(hat, st));
+  OG_CUDA(e->dih_atoms.upload(hd, st)); OG_CUDA(e->dih_terms.upload(hdt, st));
+  OG_CUDA(e->term_k.upload(htk, st)); OG_CUDA(e->term_n.upload(htn, st)); OG_CUDA(e->term_delta.upload(htd, st));
+  OG_CUDA(e->imp_atoms.upload(hi, st)); OG_CUDA(e->imp_k.upload(hik, st)); OG_CUDA(e->imp_psi0.upload(hip, st));
+  OG_CUDA(e->bonded_e.alloc(std::max(1, e->n_bonds + e->n_angles + e->n_dih + e->n_imp)));
+  OG_CUDA(e->seg_begin.upload(sb, st));
+  OG_CUDA(e->seg_end.upload(se, st));
+  OG_CUDA(e->seg_out.alloc(5 * n_sys));
+
+  // ---- SHAKE clusters: constraints grouped by their heavy atom, in
+  // constraint order inside a cluster.
+  std::vector<int32_t> hcs(1, 0), hcsys;
+  std::vector<int2> hca;
+  std::vector<double> hcd;
+  if (e->p.constrain_h_bonds) {
+    for (int si = 0; si < n_sys; ++si) {
+      const SysHost& s = e->sys[si];
+      const TopoCopy& t = s.topo;
+      std::map<int, std::vector<int>> by_heavy;
+      std::vector<int> order;
+      for (size_t k = 0; k < t.cons_d.size(); ++k) {
+        const int a = t.cons[2 * k], b = t.cons[2 * k + 1];
+        const int heavy = (t.element[a] == 0) ? b : a;
+        if (by_heavy.find(heavy) == by_heavy.end()) order.push_back(heavy);
+        by_heavy[heavy].push_back(static_cast<int>(k));
+      }
+      for (int h : order) {
+        for (int k : by_heavy[h]) {
+          hca.push_back(make_int2(s.atom_begin + t.cons[2 * k], s.atom_begin + t.cons[2 * k + 1]));
+          hcd.push_back(t.cons_d[k] * t.cons_d[k]);
+        }
+        hcs.push_back(static_cast<int32_t>(hca.size()));
+        hcsys.push_back(si);
+      }
+    }
+  }
+  e->n_clusters = static_cast<int>(hcsys.size());
+  OG_CUDA(e->cl_start.upload(hcs, st));
+  OG_CUDA(e->cl_sys.upload(hcsys, st));
+  OG_CUDA(e->cons_atoms.upload(hca, st));
+  OG_CUDA(e->cons_d2.upload(hcd, st));
+
+  OG_CUDA(e->clamp_count.alloc(n_sys));
+  OG_CUDA(e->sys_nonfinite.alloc(n_sys));
+  OG_CUDA(cudaMemsetAsync(e->sys_nonfinite.p, 0, sizeof(int32_t) * n_sys, st));
+  OG_CUDA(e->error_flag.alloc(1));
+  OG_CUDA(cudaMemsetAsync(e->error_flag.p, 0, sizeof(int32_t), st));
+
+  ogk::launch_pack(e->atoms(), true, st);
+  og_status s2 = launch_check("pack");
+  if (s2 != OG_OK) return s2;
+  OG_CUDA(cudaStreamSynchronize(st));
+  e->finalized = true;
+  e->forces_valid = false;
+  return OG_OK;
+}
+
+og_status eval_forces(og_engine* e) {
+  ogk::launch_pack(e->atoms(), true, e->stream);
+  e->enqueue_forces();
+  og_status st = launch_check("force evaluation");
+  if (st != OG_OK) return st;
+  e->forces_valid = true;
+  return OG_OK;
+}
+
+og_status build_graph(og_engine* e) {
+  if (e->graph_exec) return OG_OK;
+  cudaStream_t cap;
+  OG_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaStream_t saved = e->stream;
+  e->stream = cap;
+  cudaError_t err = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (err == cudaSuccess) {
+    e->enqueue_step();
+    err = cudaStreamEndCapture(cap, &e->graph);
+  }
+  e->stream = saved;
+  cudaStreamDestroy(cap);
+  if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+  OG_CUDA(cudaGraphInstantiate(&e->graph_exec, e->graph, 0));
+  return OG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void og_params_default(og_params* p) {
+  if (!p) return;
+  *p = og_params{};
+  p->nb_cutoff = 10.0;
+  p->born_cutoff = 20.0;
+  p->gb_force_cutoff = 10.0;
+  p->dt_fs = 1.0;
+  p->friction_ps_inv = 1.0;
+  p->constrain_h_bonds = 0;
+  p->shake_max_iters = 64;
+  p->shake_tol_sq = 1e-6;
+  p->include_sasa = 0;
+  p->sasa_gamma_scale = 1.0;
+  p->born_mode = 0;
+  p->seed = 0;
+}
+
+og_status og_engine_create(const og_params* params, og_engine** out) {
+  if (!params || !out) return og_fail(OG_E_BADARG, "null argument");
+  *out = nullptr;
+  if (!(params->dt_fs > 0.0)) return og_fail(OG_E_BADARG, "dt_fs must be positive");
+  if (params->include_sasa) return og_fail(OG_E_UNSUPPORTED, "SASA forces are not built into this engine");
+  if (params->born_mode != 0) return og_fail(OG_E_UNSUPPORTED, "learned Born radii are not built into this engine");
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
+    return og_fail(OG_E_CUDA, "no CUDA device available");
+  auto e = new (std::nothrow) og_engine();
+  if (!e) return og_fail(OG_E_NOMEM, "engine allocation failed");
+  e->p = *params;
+  cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (err != cudaSuccess) {
+    delete e;
+    return cuda_fail(err, "cudaStreamCreate");
+  }
+  e->own_stream = true;
+  *out = e;
+  return OG_OK;
+}
+
+og_status og_engine_add_system(og_engine* e, const og_topology* topo, const double* xyz, double temperature_k,
+                               int32_t* index) {
+  if (!e || !topo || !xyz) return og_fail(OG_E_BADARG, "null argument");
+  if (e->finalized) return og_fail(OG_E_STATE, "engine already finalized");
+  if (!(temperature_k >= 0.0)) return og_fail(OG_E_BADARG, "temperature must be >= 0");
+  SysHost s;
+  og_status st = copy_topology(topo, &s.topo);
+  if (st != OG_OK) return st;
+  s.xyz.assign(xyz, xyz + 3 * static_cast<size_t>(topo->n_atoms));
+  for (double v : s.xyz)
+    if (!std::isfinite(v)) return og_fail(OG_E_NONFINITE, "initial positions are not finite");
+  s.temperature = temperature_k;
+  e->sys.push_back(std::move(s));
+  if (index) *index = static_cast<int32_t>(e->sys.size()) - 1;
+  return OG_OK;
+}
+
+og_status og_engine_finalize(og_engine* e) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  if (e->finalized) return og_fail(OG_E_STATE, "engine already finalized");
+  return finalize_impl(e);
+}
+
+og_status og_engine_n_systems(const og_engine* e, int32_t* n) {
+  if (!e || !n) return og_fail(OG_E_BADARG, "null argument");
+  *n = static_cast<int32_t>(e->sys.size());
+  return OG_OK;
+}
+
+og_status og_engine_set_stream(og_engine* e, void* stream) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+  if (stream) {
+    e->stream = static_cast<cudaStream_t>(stream);
+    e->own_stream = false;
+  } else {
+    OG_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    e->own_stream = true;
+  }
+  return OG_OK;
+}
+
+og_status og_engine_synchronize(og_engine* e) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+void og_engine_destroy(og_engine* e) {
+  if (!e) return;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  delete e;
+}
+
+og_status og_set_positions(og_engine* e, int32_t s, const double* xyz) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!xyz) return og_fail(OG_E_BADARG, "null positions");
+  st = set_xyz(e, s, e->x, e->y, e->z, xyz);
+  e->forces_valid = false;
+  return st;
+}
+
+og_status og_get_positions(og_engine* e, int32_t s, double* xyz) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!xyz) return og_fail(OG_E_BADARG, "null positions");
+  return get_xyz(e, s, e->x, e->y, e->z, xyz);
+}
+
+og_status og_set_velocities(og_engine* e, int32_t s, const double* v) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!v) return og_fail(OG_E_BADARG, "null velocities");
+  return set_xyz(e, s, e->vx, e->vy, e->vz, v);
+}
+
+og_status og_get_velocities(og_engine* e, int32_t s, double* v) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!v) return og_fail(OG_E_BADARG, "null velocities");
+  return get_xyz(e, s, e->vx, e->vy, e->vz, v);
+}
+
+og_status og_init_velocities(og_engine* e, int32_t s, uint64_t seed, int32_t remove_com) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  const SysHost& sh = e->sys[s];
+  const int n = sh.topo.n;
+  const double kbt = ogk::kBoltzmann * sh.temperature;
+  Xoshiro rng(seed);
+  std::vector<double> v(3 * static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i) {
+    const double sigma = std::sqrt(kbt * ogk::kAccel / sh.topo.mass[i]);
+    v[3 * i] = sigma * rng.gaussian();
+    v[3 * i + 1] = sigma * rng.gaussian();
+    v[3 * i + 2] = sigma * rng.gaussian();
+  }
+  if (remove_com) {
+    double tm = 0.0, px = 0.0, py = 0.0, pz = 0.0;
+    for (int i = 0; i < n; ++i) {
+      px += v[3 * i] * sh.topo.mass[i];
+      py += v[3 * i + 1] * sh.topo.mass[i];
+      pz += v[3 * i + 2] * sh.topo.mass[i];
+      tm += sh.topo.mass[i];
+    }
+    if (tm > 0.0) {
+      const double cx = px / tm, cy = py / tm, cz = pz / tm;
+      for (int i = 0; i < n; ++i) {
+        v[3 * i] -= cx;
+        v[3 * i + 1] -= cy;
+        v[3 * i + 2] -= cz;
+      }
+    }
+  }
+  return set_xyz(e, s, e->vx, e->vy, e->vz, v.data());
+}
+
+og_status og_set_temperature(og_engine* e, int32_t s, double t) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!(t >= 0.0)) return og_fail(OG_E_BADARG, "temperature must be >= 0");
+  e->sys[s].temperature = t;
+  const double kbt = ogk::kBoltzmann * t;
+  OG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(e->sys_state.p + s) + offsetof(ogk::SysState, temperature), &t,
+                          sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  OG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(e->sys_state.p + s) + offsetof(ogk::SysState, kbt), &kbt,
+                          sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_compute_forces(og_engine* e, int32_t s, double* f_out) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (f_out && (s < 0 || s >= static_cast<int32_t>(e->sys.size())))
+    return og_fail(OG_E_BADARG, "system index out of range");
+  if ((st = eval_forces(e)) != OG_OK) return st;
+  if (f_out) {
+    const int n = e->sys[s].topo.n;
+    std::vector<unsigned long long> h[3];
+    const DVec<unsigned long long>* src[3] = {&e->fx, &e->fy, &e->fz};
+    for (int c = 0; c < 3; ++c) {
+      h[c].resize(n);
+      if ((st = copy_sys_range(e, *src[c], s, h[c].data())) != OG_OK) return st;
+    }
+    OG_CUDA(cudaStreamSynchronize(e->stream));
+    for (int i = 0; i < n; ++i)
+      for (int c = 0; c < 3; ++c)
+        f_out[3 * i + c] = static_cast<double>(static_cast<long long>(h[c][i])) * ogk::kForceUnscale;
+  } else {
+    OG_CUDA(cudaStreamSynchronize(e->stream));
+  }
+  return OG_OK;
+}
+
+og_status og_get_born_radii(og_engine* e, int32_t s, double* radii) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!radii) return og_fail(OG_E_BADARG, "null output");
+  if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
+  if ((st = copy_sys_range(e, e->born_r, s, radii)) != OG_OK) return st;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  const int n_sys = static_cast<int>(e->sys.size());
+  if (!out) return og_fail(OG_E_BADARG, "null output");
+  if (s < -1 || s >= n_sys) return og_fail(OG_E_BADARG, "system index out of range");
+  cudaStream_t stream = e->stream;
+  ogk::EnergyArgs a{};
+  a.x = e->x.p; a.y = e->y.p; a.z = e->z.p; a.q = e->q.p;
+  a.rmin = e->rmin.p; a.eps = e->eps.p; a.rmin14 = e->rmin14.p; a.eps14 = e->eps14.p;
+  a.rho_tilde = e->rho_tilde.p; a.srho = e->srho.p; a.born_r = e->born_r64.p;
+  a.atom_sys = e->atom_sys.p;
+  std::vector<int32_t> hb(n_sys), hc(n_sys);
+  for (int k = 0; k < n_sys; ++k) {
+    hb[k] = e->sys[k].atom_begin;
+    hc[k] = e->sys[k].topo.n;
+  }
+  DVec<int32_t> dbeg, dcnt;
+  OG_CUDA(dbeg.upload(hb, stream));
+  OG_CUDA(dcnt.upload(hc, stream));
+  a.sys_begin = dbeg.p;
+  a.sys_count = dcnt.p;
+  a.excl_row = e->excl_row.p; a.excl_col = e->excl_col.p; a.excl_kind = e->excl_kind.p;
+  a.n_atoms_padded = e->n_padded;
+  a.nb_c2 = no_cutoff(e->p.nb_cutoff) ? INFINITY : e->p.nb_cutoff * e->p.nb_cutoff;
+  a.born_c2 = no_cutoff(e->p.born_cutoff) ? INFINITY : e->p.born_cutoff * e->p.born_cutoff;
+  const double rc = e->p.nb_cutoff;
+  a.kappa = no_cutoff(rc) ? 0.0 : 1.0 / (2.0 * rc * rc * rc);
+  a.crf = no_cutoff(rc) ? 0.0 : 3.0 / (2.0 * rc);
+  a.integral = e->integral64.p;
+  a.e_lj = e->e_lj.p; a.e_coul = e->e_coul.p; a.e_gb = e->e_gb.p; a.e_self = e->e_self.p;
+  a.n_pairs = e->n_pairs.p;
+
+  OG_CUDA(cudaMemsetAsync(e->clamp_count.p, 0, sizeof(int32_t) * n_sys, stream));
+  ogk::launch_born64(a, stream);
+  ogk::launch_born_finalize(e->atoms(), e->integral64.p, e->born_r64.p, false, e->clamp_count.p, stream);
+  ogk::launch_energy64(a, stream);
+  ogk::launch_bonded_energies(e->bonded_args(), stream);
+  if ((st = launch_check("energy kernels")) != OG_OK) return st;
+
+  // Deterministic per-system sums.
+  std::vector<double> sums[5];
+  const double* per_atom[4] = {e->e_lj.p, e->e_coul.p, e->e_gb.p, e->e_self.p};
+  for (int k = 0; k < 4; ++k) {
+    ogk::launch_segment_sum(per_atom[k], e->seg_begin.p, e->seg_end.p, n_sys, e->seg_out.p + 0, stream);
+    sums[k].resize(n_sys);
+    OG_CUDA(cudaMemcpyAsync(sums[k].data(), e->seg_out.p, sizeof(double) * n_sys, cudaMemcpyDeviceToHost, stream));
+    OG_CUDA(cudaStreamSynchronize(stream));
+  }
+  std::vector<double> bonded(4 * static_cast<size_t>(n_sys));
+  ogk::launch_segment_sum(e->bonded_e.p, e->seg_begin.p + n_sys, e->seg_end.p + n_sys, 4 * n_sys, e->seg_out.p,
+                          stream);
+  OG_CUDA(cudaMemcpyAsync(bonded.data(), e->seg_out.p, sizeof(double) * 4 * n_sys, cudaMemcpyDeviceToHost, stream));
+  // Pair counts (int) summed on the host.
+  std::vector<int32_t> clamp(n_sys);
+  OG_CUDA(cudaMemcpyAsync(clamp.data(), e->clamp_count.p, sizeof(int32_t) * n_sys, cudaMemcpyDeviceToHost, stream));
+  std::vector<int32_t> pairs(e->n_padded);
+  OG_CUDA(cudaMemcpyAsync(pairs.data(), e->n_pairs.p, sizeof(int32_t) * e->n_padded, cudaMemcpyDeviceToHost,
+                          stream));
+  OG_CUDA(cudaStreamSynchronize(stream));
+  if ((st = launch_check("energy reductions")) != OG_OK) return st;
+
+  for (int k = 0; k < n_sys; ++k) {
+    if (s >= 0 && k != s) continue;
+    og_energies& o = out[s >= 0 ? 0 : k];
+    o = og_energies{};
+    o.bond = bonded[0 * n_sys + k];
+    o.angle = bonded[1 * n_sys + k];
+    o.dihedral = bonded[2 * n_sys + k];
+    o.improper = bonded[3 * n_sys + k];
+    o.lj = 0.5 * sums[0][k] * ogk::kKcalToKj;
+    o.coulomb = 0.5 * sums[1][k] * ogk::kKcalToKj;
+    o.gb_pair = 0.5 * sums[2][k] * ogk::kKcalToKj;
+    o.gb_self = sums[3][k] * ogk::kKcalToKj;
+    o.gb = o.gb_self + o.gb_pair;
+    o.sasa = 0.0;
+    o.total = o.bond + o.angle + o.dihedral + o.improper + o.lj + o.coulomb + o.gb + o.sasa;
+    o.born_clamped = clamp[k];
+    long long np = 0;
+    for (int i = e->sys[k].atom_begin; i < e->sys[k].atom_begin + e->sys[k].topo.n; ++i) np += pairs[i];
+    o.nb_pairs = static_cast<int32_t>(np / 2);
+  }
+  return OG_OK;
+}
+
+og_status og_step(og_engine* e, int32_t n_steps) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (n_steps < 0) return og_fail(OG_E_BADARG, "negative step count");
+  if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
+  if (e->profile) {
+    for (int k = 0; k < n_steps; ++k) e->enqueue_step();
+    if ((st = launch_check("step")) != OG_OK) return st;
+  } else if (n_steps > 0) {
+    if ((st = build_graph(e)) != OG_OK) return st;
+    for (int k = 0; k < n_steps; ++k) OG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
+  }
+  std::vector<ogk::SysState> hs;
+  if ((st = read_status(e, &hs)) != OG_OK) return st;
+  for (const auto& s : hs)
+    if (s.status & ogk::kStatusDiverged) return og_fail(OG_E_NONFINITE, "a system diverged (non-finite velocity)");
+  return OG_OK;
+}
+
+og_status og_system_stats(og_engine* e, int32_t s, int64_t* steps, int64_t* shake_failures, int32_t* diverged) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  std::vector<ogk::SysState> hs;
+  if ((st = read_status(e, &hs)) != OG_OK) return st;
+  if (steps) *steps = hs[s].steps;
+  if (shake_failures) *shake_failures = hs[s].shake_failures;
+  if (diverged) *diverged = (hs[s].status & ogk::kStatusDiverged) ? 1 : 0;
+  return OG_OK;
+}
+
+og_status og_kinetic(og_engine* e, int32_t s, double* ke, double* temp) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  const int n_sys = static_cast<int>(e->sys.size());
+  ogk::launch_kinetic(e->atoms(), e->seg_begin.p, e->seg_end.p, n_sys, e->seg_out.p, e->stream);
+  std::vector<double> h(n_sys);
+  OG_CUDA(cudaMemcpyAsync(h.data(), e->seg_out.p, sizeof(double) * n_sys, cudaMemcpyDeviceToHost, e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  const double dof = 3.0 * e->sys[s].topo.n;
+  if (ke) *ke = h[s];
+  if (temp) *temp = dof > 0.0 ? 2.0 * h[s] / (dof * ogk::kBoltzmann) : 0.0;
+  return OG_OK;
+}
+
+og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int32_t* accepted) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!uniforms) return og_fail(OG_E_BADARG, "null uniforms");
+  const int n_sys = static_cast<int>(e->sys.size());
+  std::vector<int> order(n_sys);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return e->sys[a].temperature < e->sys[b].temperature; });
+  std::vector<og_energies> en(n_sys);
+  if ((st = og_compute_energies(e, -1, en.data())) != OG_OK) return st;
+  std::vector<ogk::SysState> hs;
+  if ((st = read_status(e, &hs)) != OG_OK) return st;
+  const int n_pairs = n_sys - 1;
+  if (accepted)
+    for (int k = 0; k < n_pairs; ++k) accepted[k] = 0;
+  for (int pi = (parity & 1); pi < n_pairs; pi += 2) {
+    const int a = order[pi], b = order[pi + 1];
+    if ((hs[a].status | hs[b].status) & ogk::kStatusDiverged) continue;
+    if (e->sys[a].topo.n != e->sys[b].topo.n) return og_fail(OG_E_BADARG, "replica exchange between unequal systems");
+    const double ta = e->sys[a].temperature, tb = e->sys[b].temperature;
+    const double beta_a = 1.0 / (ogk::kBoltzmann * ta), beta_b = 1.0 / (ogk::kBoltzmann * tb);
+    const double delta = (beta_a - beta_b) * (en[a].total - en[b].total);
+    const double p_acc = delta >= 0.0 ? 1.0 : std::exp(delta);
+    if (uniforms[pi] < p_acc) {
+      ogk::launch_swap_systems(e->atoms(), e->sys[a].atom_begin, e->sys[b].atom_begin, e->sys[a].topo.n,
+                               std::sqrt(ta / tb), std::sqrt(tb / ta), e->stream);
+      if (accepted) accepted[pi] = 1;
+    }
+  }
+  if ((st = launch_check("replica swap")) != OG_OK) return st;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_profile_enable(og_engine* e, int32_t on) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  e->profile = on != 0;
+  e->prof.clear();
+  return OG_OK;
+}
+
+og_status og_profile_read(og_engine* e, og_kernel_time* out, int32_t cap, int32_t* n_out) {
+  if (!e || !n_out) return og_fail(OG_E_BADARG, "null argument");
+  e->prof_names.clear();
+  for (const auto& kv : e->prof) e->prof_names.push_back(kv.first);
+  int k = 0;
+  for (const auto& name : e->prof_names) {
+    if (k >= cap) break;
+    if (out) {
+      out[k].name = name.c_str();
+      out[k].ms = e->prof[name].first;
+      out[k].launches = e->prof[name].second;
+    }
+    ++k;
+  }
+  *n_out = k;
+  return OG_OK;
+}
+
+}  // extern "C"

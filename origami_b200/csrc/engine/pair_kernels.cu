@@ -1,0 +1,347 @@
+// Pair kernels of the force path and the FP64 energy path.
+//
+// Force path (FP32 pair math):
+//   born pass   -- descreening integral I_i = sum_j h(r_ij, rho~_i, s_j rho~_j)
+//                  (energy/src/gb.rs:268-324 + pairwise_descreening :347-369)
+//   force pass  -- LJ with 1-4 overrides + reaction-field Coulomb within the
+//                  nonbonded cutoff (energy/src/forces_nonbonded.rs:196-232)
+//                  fused with the frozen-radii GB pair force within the GB
+//                  cutoff (energy/src/forces_gb.rs:82-111).
+// Layout: one warp owns one 32-atom i-tile; a CTA of kWarps warps walks a
+// list of 32-atom j-tiles that thread 0 streams into shared memory with 1-D
+// TMA bulk copies (double buffered, mbarrier completion, bounded waits); each
+// j atom is then read by all 32 lanes as a shared-memory broadcast.  Every
+// ordered pair is evaluated from its i side (no Newton-3 j scatter), so each
+// i atom's sum is formed in a fixed order: FP32 per j-tile, FP64 across tiles,
+// and one 64-bit fixed-point atomic per atom per work item -- results are
+// bit-reproducible whatever the launch order.
+//
+// Positions reach the pair kernels as FP32 offsets from a per-tile FP64
+// origin; the origin difference of a tile pair is formed in FP64 once per
+// tile, which keeps |dx| accurate to ~1e-7 relative even for chains 1000 A
+// long.
+#include <cmath>
+
+#include "common.cuh"
+#include "pair_kernels.cuh"
+
+namespace ogk {
+
+namespace {
+
+constexpr int kWarps = 4;         // i-tiles per CTA
+constexpr int kStageTiles = 4;    // j-tiles per pipeline stage
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.0f, x); }
+
+// Born pass: h(r, rho_i, s_rho_j) summed over one staged j-tile.
+// Algebraically the reference's four terms with term2 + term4 folded into
+// (s^2 / 4r)(1/U^2 - 1/L^2), and ln(L/U) = log1p(-2 s / U) on the
+// non-overlapping branch, which keeps the FP32 evaluation well conditioned.
+__device__ __forceinline__ float born_tile(const float4* __restrict__ sp, const float4* __restrict__ sg, float xi,
+                                           float yi, float zi, float rho, float born_c2) {
+  float acc = 0.0f;
+#pragma unroll 4
+  for (int k = 0; k < kTile; ++k) {
+    const float4 p = sp[k];
+    const float sr = sg[k].w;
+    const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float inv_r = rsqrtf(r2);
+    const float r = r2 * inv_r;
+    const bool overlap = (r - sr) < rho;
+    const float L = overlap ? rho : r - sr;
+    const float U = r + sr;
+    const float inv_l = fast_rcp(L), inv_u = fast_rcp(U);
+    const float lg = overlap ? logf(L * inv_u) : log1pf(-2.0f * sr * inv_u);
+    const float d2 = inv_u * inv_u - inv_l * inv_l;
+    float h = 0.5f * (inv_l - inv_u) + (sr * sr) * (0.25f * inv_r) * d2 + (0.5f * inv_r) * lg;
+    const bool on = (r2 <= born_c2) && (r2 >= 1e-18f) && !(r + sr <= rho) && (U > 0.0f) && (L > 0.0f);
+    acc += on ? h : 0.0f;
+  }
+  return acc;
+}
+
+struct IAtom {
+  float x, y, z;
+  float cq;     // -coul_kj * q_i
+  float gq;     // gb_pref_kj * q_i
+  float rm, se, rm14, se14;
+  float R;      // Born radius
+  float nexp;   // -0.25 * log2(e) / R_i
+};
+
+template <bool kMasked>
+__device__ __forceinline__ void force_tile(const float4* __restrict__ sp, const float4* __restrict__ sl,
+                                           const float4* __restrict__ sg, const IAtom& ia, uint32_t ex, uint32_t m14,
+                                           const PairArgs& a, float& fx, float& fy, float& fz) {
+#pragma unroll 4
+  for (int k = 0; k < kTile; ++k) {
+    const float4 p = sp[k];
+    const float4 l = sl[k];
+    const float2 g = *reinterpret_cast<const float2*>(&sg[k]);
+    const float dx = p.x - ia.x, dy = p.y - ia.y, dz = p.z - ia.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float inv_r = rsqrtf(r2);
+    const float inv_r2 = inv_r * inv_r;
+    float rmin, se;
+    bool nb_on = r2 <= a.nb_c2;
+    if (kMasked) {
+      const bool is14 = (m14 >> k) & 1u;
+      rmin = is14 ? ia.rm14 + l.z : ia.rm + l.x;
+      se = is14 ? ia.se14 * l.w : ia.se * l.y;
+      nb_on = nb_on && !((ex >> k) & 1u);
+    } else {
+      rmin = ia.rm + l.x;
+      se = ia.se * l.y;
+    }
+    const float ratio2 = rmin * rmin * inv_r2;
+    const float r6 = ratio2 * ratio2 * ratio2;
+    const float ljc = a.lj_kj12 * se * inv_r2 * fmaf(-r6, r6, r6);
+    const float coul = ia.cq * p.w * fmaf(inv_r2, inv_r, -a.inv_rc3);
+    const float e = exp2f(r2 * ia.nexp * g.y);
+    const float f2 = fmaf(ia.R * g.x, e, r2);
+    const float inv_f = rsqrtf(f2);
+    const float gbc = ia.gq * p.w * fmaf(-0.25f, e, 1.0f) * (inv_f * inv_f * inv_f);
+    float coeff = (nb_on ? ljc + coul : 0.0f) + ((r2 <= a.gb_c2) ? gbc : 0.0f);
+    coeff = (r2 >= 1e-18f) ? coeff : 0.0f;
+    fx = fmaf(dx, coeff, fx);
+    fy = fmaf(dy, coeff, fy);
+    fz = fmaf(dz, coeff, fz);
+  }
+}
+
+// kPass 0 = Born descreening integral, 1 = force.
+template <int kPass>
+__global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
+  constexpr int kArrays = kPass == 0 ? 2 : 3;
+  constexpr uint32_t kTileBytes = kTile * sizeof(float4);
+  __shared__ __align__(128) float4 s_buf[2][kArrays][kStageTiles * kTile];
+  __shared__ __align__(8) uint64_t s_bar[2];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const PairWork w = a.work[blockIdx.x];
+  const int nj = w.j_end - w.j_begin;
+  const int n_stages = (nj + kStageTiles - 1) / kStageTiles;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int s) {
+    const int buf = s & 1;
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * kArrays);
+    for (int t = 0; t < cnt; ++t) {
+      const int jt = a.jlist[t0 + t];
+      const size_t base = static_cast<size_t>(jt) * kTile;
+      bulk_g2s(&s_buf[buf][0][t * kTile], a.pq + base, kTileBytes, &s_bar[buf]);
+      if (kPass == 0) {
+        bulk_g2s(&s_buf[buf][1][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
+      } else {
+        bulk_g2s(&s_buf[buf][1][t * kTile], a.lj + base, kTileBytes, &s_bar[buf]);
+        bulk_g2s(&s_buf[buf][2][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
+      }
+    }
+  };
+  if (threadIdx.x == 0) {
+    if (n_stages > 0) issue(0);
+    if (n_stages > 1) issue(1);
+  }
+
+  const bool active = warp < w.n_i_tiles;
+  const int it = w.i_tile0 + (active ? warp : 0);
+  const int i = it * kTile + lane;
+  const float4 pi = a.pq[i];
+  const double4 oi = a.origin[it];
+  IAtom ia;
+  float rho_i = 0.0f;
+  if (kPass == 0) {
+    rho_i = a.gb[i].z;
+  } else {
+    const float4 li = a.lj[i];
+    const float4 gi = a.gb[i];
+    ia.cq = -a.coul_kj * pi.w;
+    ia.gq = a.gb_pref_kj * pi.w;
+    ia.rm = li.x; ia.se = li.y; ia.rm14 = li.z; ia.se14 = li.w;
+    ia.R = gi.x;
+    ia.nexp = -0.25f * kLog2e * gi.y;
+  }
+  int mref = a.mask_begin[it];
+  const int mend = a.mask_begin[it + 1];
+
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  for (int s = 0; s < n_stages; ++s) {
+    const int buf = s & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[buf], static_cast<uint32_t>((s >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
+      return;
+    }
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    for (int t = 0; t < cnt; ++t) {
+      const int jt = a.jlist[t0 + t];
+      const double4 oj = a.origin[jt];
+      const float xi = pi.x - static_cast<float>(oj.x - oi.x);
+      const float yi = pi.y - static_cast<float>(oj.y - oi.y);
+      const float zi = pi.z - static_cast<float>(oj.z - oi.z);
+      const float4* sp = &s_buf[buf][0][t * kTile];
+      if (kPass == 0) {
+        acc0 += static_cast<double>(born_tile(sp, &s_buf[buf][1][t * kTile], xi, yi, zi, rho_i, a.born_c2));
+      } else {
+        while (mref < mend && a.mask_refs[mref].j_tile < jt) ++mref;
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        ia.x = xi; ia.y = yi; ia.z = zi;
+        if (mref < mend && a.mask_refs[mref].j_tile == jt) {
+          const int off = a.mask_refs[mref].offset;
+          force_tile<true>(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia,
+                           a.mask_ex[off * kTile + lane], a.mask_14[off * kTile + lane], a, fx, fy, fz);
+        } else {
+          force_tile<false>(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia, 0u, 0u, a, fx, fy, fz);
+        }
+        acc0 += static_cast<double>(fx);
+        acc1 += static_cast<double>(fy);
+        acc2 += static_cast<double>(fz);
+      }
+    }
+    __syncthreads();  // every warp is done with `buf`
+    if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
+  }
+
+  if (active && a.atom_valid[i]) {
+    if (!(isfinite(acc0) && isfinite(acc1) && isfinite(acc2))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
+    if (kPass == 0) {
+      add_fixed(a.born_sum + i, acc0, kBornScale);
+    } else {
+      // The pair coefficient multiplies d = r_j - r_i, so the i-side force is +sum.
+      add_fixed(a.fx + i, acc0, kForceScale);
+      add_fixed(a.fy + i, acc1, kForceScale);
+      add_fixed(a.fz + i, acc2, kForceScale);
+    }
+  }
+}
+
+}  // namespace
+
+void launch_born_pass(const PairArgs& a, cudaStream_t s) {
+  if (a.n_work > 0) k_pairs<0><<<a.n_work, kWarps * 32, 0, s>>>(a);
+}
+
+void launch_force_pass(const PairArgs& a, cudaStream_t s) {
+  if (a.n_work > 0) k_pairs<1><<<a.n_work, kWarps * 32, 0, s>>>(a);
+}
+
+int pair_warps_per_cta() { return kWarps; }
+
+// ----------------------------------------------------------------- FP64 path
+
+namespace {
+
+__device__ __forceinline__ double descreen64(double r, double rho_i, double s_rho_j) {
+  // energy/src/gb.rs:347-369, term for term.
+  if (r + s_rho_j <= rho_i) return 0.0;
+  const double l = (r - s_rho_j < rho_i) ? rho_i : r - s_rho_j;
+  const double u = r + s_rho_j;
+  if (u <= 0.0 || l <= 0.0) return 0.0;
+  const double inv_l = 1.0 / l, inv_u = 1.0 / u;
+  const double term1 = 0.5 * (inv_l - inv_u);
+  const double term2 = (r / 4.0) * (inv_u * inv_u - inv_l * inv_l);
+  const double term3 = (1.0 / (2.0 * r)) * log(l / u);
+  const double term4 = (s_rho_j * s_rho_j - r * r) / (4.0 * r) * (inv_u * inv_u - inv_l * inv_l);
+  return term1 + term2 + term3 + term4;
+}
+
+__global__ void k_born64(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded) return;
+  const int sys = a.atom_sys[i];
+  if (sys < 0) return;
+  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  const double xi = a.x[i], yi = a.y[i], zi = a.z[i], rho = a.rho_tilde[i];
+  double acc = 0.0;
+  for (int j = b; j < b + n; ++j) {
+    if (j == i) continue;
+    const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 > a.born_c2 || r2 < 1e-18) continue;
+    acc += descreen64(sqrt(r2), rho, a.srho[j]);
+  }
+  a.integral[i] = acc;
+}
+
+// Per i atom, over every j != i of its system: LJ + RF Coulomb within the
+// nonbonded cutoff with exclusions / 1-4 parameters (nonbonded.rs:127-169)
+// and the GB pair energy over all pairs (gb.rs:160-173).  Each unordered pair
+// is seen from both ends, so the host halves the sums.
+__global__ void k_energy64(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded) return;
+  const int sys = a.atom_sys[i];
+  if (sys < 0) {
+    a.e_lj[i] = a.e_coul[i] = a.e_gb[i] = a.e_self[i] = 0.0;
+    a.n_pairs[i] = 0;
+    return;
+  }
+  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  const double xi = a.x[i], yi = a.y[i], zi = a.z[i], qi = a.q[i], Ri = a.born_r[i];
+  const double pref = -0.5 * (1.0 - 1.0 / kEpsWater) * kCoulomb;
+  int ep = a.excl_row[i];
+  const int ee = a.excl_row[i + 1];
+  double lj = 0.0, coul = 0.0, gb = 0.0;
+  int pairs = 0;
+  for (int j = b; j < b + n; ++j) {
+    if (j == i) continue;
+    const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    int kind = 0;
+    while (ep < ee && a.excl_col[ep] < j) ++ep;
+    if (ep < ee && a.excl_col[ep] == j) kind = a.excl_kind[ep];
+    const double qq = qi * a.q[j];
+    if (qq != 0.0) {
+      const double rp = Ri * a.born_r[j];
+      const double fgb = sqrt(r2 + rp * exp(-r2 / (4.0 * rp)));
+      gb += 2.0 * pref * qq / fgb;
+    }
+    if (r2 > a.nb_c2 || kind == 1) continue;
+    const double r = sqrt(r2);
+    double rmin, eps;
+    if (kind == 2) {
+      rmin = a.rmin14[i] + a.rmin14[j];
+      eps = sqrt(a.eps14[i] * a.eps14[j]);
+    } else {
+      rmin = a.rmin[i] + a.rmin[j];
+      eps = sqrt(a.eps[i] * a.eps[j]);
+    }
+    const double x = rmin / r;
+    const double x2 = x * x;
+    const double r6 = x2 * x2 * x2;
+    lj += eps * (r6 * r6 - 2.0 * r6);
+    if (qq != 0.0) coul += kCoulomb * qq * (1.0 / r + a.kappa * r * r - a.crf);
+    ++pairs;
+  }
+  a.e_lj[i] = lj;
+  a.e_coul[i] = coul;
+  a.e_gb[i] = gb;
+  a.e_self[i] = (qi != 0.0) ? pref * (qi * qi) / Ri : 0.0;
+  a.n_pairs[i] = pairs;
+}
+
+}  // namespace
+
+void launch_born64(const EnergyArgs& a, cudaStream_t s) {
+  const int bs = 128;
+  k_born64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+}
+
+void launch_energy64(const EnergyArgs& a, cudaStream_t s) {
+  const int bs = 128;
+  k_energy64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+}
+
+}  // namespace ogk

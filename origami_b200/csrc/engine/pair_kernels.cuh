@@ -1,0 +1,88 @@
+// Tiled all-pairs / tile-list pair kernels (FP32 pair math, FP64 per-tile
+// accumulation, 64-bit fixed-point results) and the FP64 energy kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ogk {
+
+// One unit of pair work: `n_i_tiles` (<= warps per CTA) consecutive i-tiles of
+// one system against the j-tiles jlist[j_begin, j_end).
+struct PairWork {
+  int32_t i_tile0;
+  int32_t n_i_tiles;
+  int32_t j_begin;
+  int32_t j_end;
+};
+
+// Exclusion masks of one ordered (i-tile, j-tile) pair: for i-lane l, bit k
+// of ex[l] marks pair (i0+l, j0+k) as excluded (1-2, 1-3 or self), bit k of
+// m14[l] as a 1-4 pair.  Entries of one i-tile are sorted by j-tile.
+struct TileMaskRef {
+  int32_t j_tile;
+  int32_t offset;  // index of the 32-word block in the mask arrays
+};
+
+struct PairArgs {
+  // per padded atom
+  const float4* pq;   // x_rel, y_rel, z_rel (A, relative to the tile origin), charge (e)
+  const float4* lj;   // rmin_half, sqrt(eps), rmin_half_14, sqrt(eps_14)   (kcal/mol)
+  const float4* gb;   // R_born, 1/R_born, rho_tilde, s*rho_tilde
+  const double4* origin;  // per tile
+  const int32_t* atom_valid;  // 1 for real atoms
+  // work
+  const PairWork* work;
+  int32_t n_work;
+  const int32_t* jlist;
+  const int32_t* mask_begin;  // per tile: first TileMaskRef, mask_begin[t+1] = end
+  const TileMaskRef* mask_refs;
+  const uint32_t* mask_ex;
+  const uint32_t* mask_14;
+  // outputs (fixed point)
+  unsigned long long* fx;
+  unsigned long long* fy;
+  unsigned long long* fz;
+  unsigned long long* born_sum;
+  // cutoffs squared (INFINITY = none) and constants
+  float nb_c2, gb_c2, born_c2;
+  float inv_rc3;     // 1/Rc^3 of the reaction field (0 without cutoff)
+  float coul_kj;     // 332.0637 * 4.184
+  float lj_kj12;     // 12 * 4.184
+  float gb_pref_kj;  // (1 - 1/78.5) * 332.0637 * 4.184
+  int32_t* error_flag;
+  // per-system "a force or Born sum was NaN/Inf" flags (fixed point cannot
+  // carry a NaN, so it is recorded here and turned into divergence)
+  const int32_t* atom_sys;
+  int32_t* sys_nonfinite;
+};
+
+void launch_born_pass(const PairArgs& a, cudaStream_t s);
+void launch_force_pass(const PairArgs& a, cudaStream_t s);
+
+// FP64 energy evaluation, one thread per i atom over every j of its system.
+struct EnergyArgs {
+  const double* x; const double* y; const double* z;
+  const double* q;
+  const double* rmin; const double* eps; const double* rmin14; const double* eps14;
+  const double* rho_tilde; const double* srho;  // srho = scale * rho_tilde
+  const double* born_r;                          // FP64 Born radii (output of born64)
+  const int32_t* atom_sys;
+  const int32_t* sys_begin;  // per system: first padded atom
+  const int32_t* sys_count;  // real atoms
+  const int32_t* excl_row;   // CSR over padded atoms: exclusion partners (both directions)
+  const int32_t* excl_col;
+  const int8_t* excl_kind;
+  int32_t n_atoms_padded;
+  double nb_c2;    // INFINITY = all pairs
+  double born_c2;
+  double kappa, crf;  // reaction field constants (0 without cutoff)
+  // outputs, per padded atom
+  double* integral;   // born64
+  double* e_lj; double* e_coul; double* e_gb; double* e_self; int32_t* n_pairs;
+};
+
+void launch_born64(const EnergyArgs& a, cudaStream_t s);
+void launch_energy64(const EnergyArgs& a, cudaStream_t s);
+
+}  // namespace ogk

@@ -1,0 +1,133 @@
+"""Shared test fixtures.
+
+The oracle (oracle/oracle.cpp, a CPU FP64 restatement of origami's force and
+integrator code) is the checker for every parity test; it is built on demand
+with `make -C oracle`.  GPU tests are marked `gpu` and call the product only
+through the C ABI (origami_b200/liborigami_b200.so).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from origami_b200 import _ffi as F  # noqa: E402
+
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "liborigami_oracle.so")
+LIB_SO = os.path.join(ROOT, "origami_b200", "liborigami_b200.so")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def have_gpu() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        return False
+
+
+_oracle = None
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        src = os.path.join(ROOT, "oracle", "oracle.cpp")
+        if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+        o = C.CDLL(ORACLE_SO)
+        dp, ip = F.c_double_p, F.c_int32_p
+        tp = C.POINTER(F.og_topology)
+        o.orc_bonded_energy.argtypes = [tp, dp, dp]
+        o.orc_bonded_energy.restype = None
+        o.orc_nonbonded_energy.argtypes = [tp, dp, C.c_double, dp]
+        o.orc_nonbonded_energy.restype = C.c_int
+        o.orc_born_radii.argtypes = [tp, dp, C.c_double, dp]
+        o.orc_born_radii.restype = C.c_int
+        o.orc_gb_energy.argtypes = [tp, dp, C.c_double, dp]
+        o.orc_gb_energy.restype = C.c_int
+        o.orc_total_force.argtypes = [tp, dp, C.c_double, C.c_double, C.c_double, dp]
+        o.orc_total_force.restype = None
+        o.orc_bonded_forces.argtypes = [tp, dp, dp]
+        o.orc_bonded_forces.restype = None
+        o.orc_potential_energy.argtypes = [tp, dp, C.c_double, C.c_double, dp]
+        o.orc_potential_energy.restype = C.c_double
+        o.orc_exclusion_matrix.argtypes = [C.c_int, C.c_int, ip, C.POINTER(C.c_int8)]
+        o.orc_exclusion_matrix.restype = None
+        o.orc_engine_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp]
+        o.orc_engine_normals.restype = None
+        o.orc_baoab.argtypes = [tp, dp, dp, dp, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_uint64,
+                                C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double]
+        o.orc_baoab.restype = C.c_int
+        o.orc_shake.argtypes = [dp, dp, dp, C.c_int, ip, dp, C.c_double, C.c_int]
+        o.orc_shake.restype = C.c_int
+        _oracle = o
+    return _oracle
+
+
+def dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(F.c_double_p)
+
+
+INF = 1e300  # the ABI's "no cutoff"
+
+
+class Orc:
+    """Thin numpy wrappers around the oracle for one chain."""
+
+    def __init__(self, chain):
+        self.chain = chain
+        self.tp = chain.topology_ptr()
+        self.o = oracle()
+
+    def xyz(self, x=None):
+        return np.ascontiguousarray(self.chain.positions if x is None else x, dtype=np.float64)
+
+    def total_force(self, x=None, nb=10.0, born=20.0, gb=10.0):
+        x = self.xyz(x)
+        f = np.zeros_like(x)
+        self.o.orc_total_force(self.tp, dp(x), nb, born, gb, dp(f))
+        return f
+
+    def bonded_force(self, x=None):
+        x = self.xyz(x)
+        f = np.zeros_like(x)
+        self.o.orc_bonded_forces(self.tp, dp(x), dp(f))
+        return f
+
+    def energy_terms(self, x=None, nb=10.0, born=20.0):
+        x = self.xyz(x)
+        t = np.zeros(9)
+        tot = self.o.orc_potential_energy(self.tp, dp(x), nb, born, dp(t))
+        d = dict(zip(("bond", "angle", "dihedral", "improper", "lj", "coulomb", "gb", "gb_self", "gb_pair"), t))
+        d["total"] = tot
+        return d
+
+    def born_radii(self, x=None, born=20.0):
+        x = self.xyz(x)
+        r = np.zeros(x.shape[0])
+        self.o.orc_born_radii(self.tp, dp(x), born, dp(r))
+        return r
+
+
+@pytest.fixture(scope="session")
+def origami():
+    import origami_b200
+    origami_b200.lib()
+    return origami_b200
+
+
+@pytest.fixture(scope="session")
+def gpu_available():
+    return have_gpu()
