@@ -1,0 +1,319 @@
+#!/usr/bin/env python3
+"""Throughput of the batched plain-GB MD step on B200 (and the CPU oracle port).
+
+Workload (one "step" = one BAOAB + SHAKE step of every replica):
+  64 replicas of one 300-residue seeded-uniform chain (~4 900 atoms, built
+  extended by NeRF, relaxed), CHARMM36m bonded + LJ + Coulomb + GB, all-pairs
+  mode (no cutoffs), dt 2 fs, SHAKE on X-H bonds, 310 K, gamma 2 ps^-1.
+Metric: aggregate ns/day over all replicas (and GPUs).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+Timing: CUDA events on the engine's stream (torch's current stream), one
+event pair per step with a 256 MiB L2 flush before each; under torchrun the
+max over ranks.  `e2e` is the same metric through the C ABI with host
+positions/velocities copied in and positions copied out every step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+AA_ORDER = "ARNDCQEGHILKMFPSTWYV"  # AminoAcid::ALL (chem/src/amino_acid.rs:31)
+METRIC = "aggregate ns/day (64 replicas, 5k atoms, GB+SASA): learned-GB vs plain GB"
+
+
+def seeded_sequence(n_res: int, seed: int) -> str:
+    from origami_b200 import Xoshiro256pp
+    rng = Xoshiro256pp(seed)
+    return "".join(AA_ORDER[min(int(rng.next_f64() * 20), 19)] for _ in range(n_res))
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.summary = {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        if not self.proc:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k].strip() == "Active"})
+        self.summary = {"sm_mhz": statistics.median(sm) if sm else None,
+                        "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                        "samples": len(rows)}
+
+
+def build_workload(og, n_res: int, seed: int):
+    seq = seeded_sequence(n_res, seed)
+    chain = og.Chain.build(seq)
+    return seq, chain
+
+
+def relax(og, chain, all_pairs: bool, max_steps: int = 300):
+    """Untimed set-up: L-BFGS on the GPU from the extended build (origami
+    minimises before dynamics), then a short overdamped Langevin settle."""
+    from origami_b200.minimize import MinimizeOptions, lbfgs
+    mk = og.Params.all_pairs if all_pairs else og.Params
+    eng = og.Engine(mk(dt_fs=0.5, friction_ps_inv=50.0, constrain_h_bonds=False, seed=7))
+    eng.add_system(chain, chain.positions, 100.0)
+    eng.finalize()
+    res = lbfgs(eng, 0, MinimizeOptions(max_steps=max_steps, gradient_tol=5.0))
+    eng.step(200)
+    chain.positions = eng.positions(0)
+    eng.close()
+    return res
+
+
+def cpu_sample(chain, dt_fs: float, replicas: int, budget_s: float = 15.0, all_pairs: bool = True) -> dict:
+    """Oracle port (FP64, OpenMP over all host threads): BAOAB+SHAKE steps of
+    one replica; returns aggregate ns/day for `replicas` replicas run on the CPU."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from conftest import INF, Orc, dp, oracle
+    orc = Orc(chain)
+    x = np.ascontiguousarray(chain.positions)
+    v = np.zeros_like(x)
+    cut = (INF, INF, INF) if all_pairs else (10.0, 20.0, 10.0)
+    f = orc.total_force(x, *cut)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        oracle().orc_baoab(orc.tp, dp(x), dp(v), dp(f), 1, dt_fs, 2.0, 310.0, 1, 0, 0, steps, *cut)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 50:
+            break
+    per_step = el / steps  # one replica
+    agg = dt_fs * 1e-6 / (per_step * replicas) * 86400.0
+    return {"value": agg, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} BAOAB+SHAKE step(s) of 1 replica ({chain.n_atoms} atoms, all pairs, FP64 oracle, "
+                      f"OpenMP {os.cpu_count()} threads), scaled to {replicas} replicas run back to back"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import origami_b200 as og
+    seq, chain = build_workload(og, args.residues, args.seed)
+    samples = []
+    for _ in range(args.warmup):
+        pass  # the oracle has no warm-up state; warm-up steps are skipped on the CPU arm
+    t_all = time.perf_counter()
+    for _ in range(max(args.steps, 1)):
+        samples.append(cpu_sample(chain, args.dt, args.replicas, budget_s=5.0, all_pairs=not args.cutoff)["value"])
+        if time.perf_counter() - t_all > 120:
+            break
+    val = statistics.median(samples)
+    per_step_ms = args.dt * 1e-6 / val * 86400.0 * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": len(samples), "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, chain),
+        "cpu_baseline": {"value": val, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "one BAOAB+SHAKE step of one replica per timed step, FP64 oracle "
+                                   "(CPU restatement of origami's force/integrator path), OpenMP over all host "
+                                   f"threads, scaled to {args.replicas} replicas"},
+        "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def workload_config(args, chain):
+    return {"workload": f"{args.replicas} replicas x {args.residues}-residue seeded chain, "
+                        f"{'reference cutoffs 10/20/10 A' if args.cutoff else 'all pairs (no cutoff)'}, "
+                        f"dt {args.dt} fs + SHAKE, 310 K, plain GB",
+            "replicas": args.replicas, "residues": args.residues, "atoms_per_replica": chain.n_atoms,
+            "mode": "cutoff" if args.cutoff else "all_pairs", "dt_fs": args.dt, "shake": True, "sasa": False,
+            "born": "plain OBC-II pass", "l2": "flushed (256 MiB write) before every timed step",
+            "seed": args.seed}
+
+
+def run_b200(args):
+    import torch
+    import origami_b200 as og
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+
+    seq, chain = build_workload(og, args.residues, args.seed)
+    if not args.no_relax:
+        relax(og, chain, all_pairs=not args.cutoff)
+    mk = og.Params if args.cutoff else og.Params.all_pairs
+    params = mk(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1000 * rank)
+    eng = og.Engine(params)
+    x0 = chain.positions
+    for _ in range(args.replicas):
+        eng.add_system(chain, x0, 310.0)
+    eng.finalize()
+    eng.set_stream(stream.cuda_stream)
+    for r in range(args.replicas):
+        eng.init_velocities(r, (args.seed + r * 0xC0FFEE) & og.Xoshiro256pp.M, remove_com=False)
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        eng.step(1)
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            eng.step(1)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    if ws > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    atoms = chain.n_atoms
+    value = ws * args.replicas * args.dt * 1e-6 / (ms_per_step * 1e-3) * 86400.0
+
+    # ---- kernel breakdown (profile mode: CUDA events around every launch)
+    eng.profile(True)
+    prof_steps = 5
+    eng.step(prof_steps)
+    prof = eng.profile_read()
+    eng.profile(False)
+    force_ms = prof["force_pass"][0] / prof["force_pass"][1]
+    born_ms = prof["born_pass"][0] / prof["born_pass"][1]
+    pairs = args.replicas * atoms * (atoms - 1) / 2
+    peak = og.lib()
+    import ctypes as C
+    tf = C.c_double()
+    og._check(og.lib().og_measure_fp32_peak(C.byref(tf)))
+    fp32_peak = tf.value
+    force_tflops = 55 * pairs / (force_ms * 1e-3) / 1e12
+    born_tflops = 60 * pairs / (born_ms * 1e-3) / 1e12
+
+    # ---- end to end through the C ABI with host buffers
+    e2e_steps = max(3, min(args.steps, 20))
+    hx = [np.ascontiguousarray(eng.positions(r)) for r in range(args.replicas)]
+    hv = [np.ascontiguousarray(eng.velocities(r)) for r in range(args.replicas)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for r in range(args.replicas):
+            eng.set_positions(r, hx[r])
+            eng.set_velocities(r, hv[r])
+        eng.step(1)
+        for r in range(args.replicas):
+            hx[r] = eng.positions(r)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = ws * args.replicas * args.dt * 1e-6 / e2e_s * 86400.0
+
+    shake_on = 1
+    launches_per_step = 9 + 2 * shake_on
+    line = {
+        "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "precision": "FP32 pair math, FP64 tile sums, int64 fixed-point forces, FP64 integrator",
+        "data": "synthetic", "config": workload_config(args, chain),
+        "roofline": {"bound": "fp32", "kernel": "force_pass", "achieved": force_tflops, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": force_tflops / fp32_peak, "traffic": None,
+                     "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak)",
+                     "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
+        "kernels_ms_per_step": {k: v[0] / v[1] for k, v in prof.items()},
+        "born_pass_tflops": born_tflops,
+        "pair_interactions_per_s": pairs / (ms_per_step * 1e-3) * ws,
+        "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": args.replicas * atoms * 6 * 8,
+                "d2h_bytes_per_step": args.replicas * atoms * 3 * 8},
+        "gpu_launches": args.steps * launches_per_step,
+        "clocks": clk.summary,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_sample(chain, args.dt, args.replicas, budget_s=args.cpu_budget,
+                                          all_pairs=not args.cutoff)
+    if rank == 0:
+        print(json.dumps(line))
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--replicas", type=int, default=64)
+    ap.add_argument("--residues", type=int, default=300)
+    ap.add_argument("--dt", type=float, default=2.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cutoff", action="store_true", help="reference cutoffs (10/20/10 A) instead of all pairs")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-relax", action="store_true",
+                    help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -253,6 +253,11 @@ typedef struct og_kernel_time { const char* name; double ms; int64_t launches; }
 og_status og_profile_enable(og_engine* e, int32_t on);
 og_status og_profile_read(og_engine* e, og_kernel_time* out, int32_t cap, int32_t* n_out);
 
+/* Measured FP32 FMA throughput of the current device (TFLOP/s, FMA = 2 flops)
+ * from a register-resident FMA chain on every SM: the denominator of the
+ * pair kernels' FP32-pipe roofline.  No counterpart in the reference. */
+og_status og_measure_fp32_peak(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

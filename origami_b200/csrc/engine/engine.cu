@@ -162,7 +162,8 @@ struct og_engine {
   DVec<uint32_t> mask_ex, mask_14;
   DVec<int32_t> excl_row, excl_col;
   DVec<int8_t> excl_kind;
-  int n_work = 0;
+  DVec<int4> near;
+  int n_work = 0, n_near = 0;
   // bonded
   DVec<int2> bond_atoms, dih_terms;
   DVec<int4> angle_atoms, dih_atoms, imp_atoms;
@@ -234,6 +235,13 @@ struct og_engine {
     a.error_flag = error_flag.p;
     a.atom_sys = atom_sys.p;
     a.sys_nonfinite = sys_nonfinite.p;
+    a.x64 = x.p; a.y64 = y.p; a.z64 = z.p; a.q64 = q.p;
+    a.rmin64 = rmin.p; a.eps64 = eps.p; a.rmin14_64 = rmin14.p; a.eps14_64 = eps14.p;
+    a.born_r64 = born_r.p;
+    auto c2d = [](double c) { return no_cutoff(c) ? static_cast<double>(INFINITY) : c * c; };
+    a.nb_c2_64 = c2d(p.nb_cutoff);
+    a.gb_c2_64 = c2d(p.gb_force_cutoff);
+    a.inv_rc3_64 = no_cutoff(p.nb_cutoff) ? 0.0 : 1.0 / (p.nb_cutoff * p.nb_cutoff * p.nb_cutoff);
     return a;
   }
 
@@ -321,6 +329,10 @@ struct og_engine {
     {
       Timer t(this, "force_pass");
       ogk::launch_force_pass(pa, stream);
+    }
+    {
+      Timer t(this, "near_force64");
+      ogk::launch_near_force64(pa, near.p, n_near, stream);
     }
     {
       Timer t(this, "bonded");
@@ -629,6 +641,10 @@ og_status finalize_impl(og_engine* e) {
     }
     hmb[e->n_tiles] = static_cast<int32_t>(hmr.size());
   }
+  std::vector<int4> hnear;
+  for (const auto& kv : mask_of) hnear.push_back(make_int4(kv.first.first, kv.first.second, kv.second, 0));
+  e->n_near = static_cast<int>(hnear.size());
+  OG_CUDA(e->near.upload(hnear, st));
   OG_CUDA(e->mask_begin.upload(hmb, st));
   OG_CUDA(e->mask_refs.upload(hmr, st));
   OG_CUDA(e->mask_ex.upload(mex, st));

@@ -72,10 +72,10 @@ struct IAtom {
   float nexp;   // -0.25 * log2(e) / R_i
 };
 
-template <bool kMasked>
+// Far-field tile (no exclusions, no 1-4 pairs): FP32 pair math.
 __device__ __forceinline__ void force_tile(const float4* __restrict__ sp, const float4* __restrict__ sl,
-                                           const float4* __restrict__ sg, const IAtom& ia, uint32_t ex, uint32_t m14,
-                                           const PairArgs& a, float& fx, float& fy, float& fz) {
+                                           const float4* __restrict__ sg, const IAtom& ia, const PairArgs& a,
+                                           float& fx, float& fy, float& fz) {
 #pragma unroll 4
   for (int k = 0; k < kTile; ++k) {
     const float4 p = sp[k];
@@ -85,17 +85,9 @@ __device__ __forceinline__ void force_tile(const float4* __restrict__ sp, const 
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const float inv_r = rsqrtf(r2);
     const float inv_r2 = inv_r * inv_r;
-    float rmin, se;
-    bool nb_on = r2 <= a.nb_c2;
-    if (kMasked) {
-      const bool is14 = (m14 >> k) & 1u;
-      rmin = is14 ? ia.rm14 + l.z : ia.rm + l.x;
-      se = is14 ? ia.se14 * l.w : ia.se * l.y;
-      nb_on = nb_on && !((ex >> k) & 1u);
-    } else {
-      rmin = ia.rm + l.x;
-      se = ia.se * l.y;
-    }
+    const float rmin = ia.rm + l.x;
+    const float se = ia.se * l.y;
+    const bool nb_on = r2 <= a.nb_c2;
     const float ratio2 = rmin * rmin * inv_r2;
     const float r6 = ratio2 * ratio2 * ratio2;
     const float ljc = a.lj_kj12 * se * inv_r2 * fmaf(-r6, r6, r6);
@@ -198,13 +190,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
         while (mref < mend && a.mask_refs[mref].j_tile < jt) ++mref;
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         ia.x = xi; ia.y = yi; ia.z = zi;
-        if (mref < mend && a.mask_refs[mref].j_tile == jt) {
-          const int off = a.mask_refs[mref].offset;
-          force_tile<true>(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia,
-                           a.mask_ex[off * kTile + lane], a.mask_14[off * kTile + lane], a, fx, fy, fz);
-        } else {
-          force_tile<false>(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia, 0u, 0u, a, fx, fy, fz);
-        }
+        // Near-field tiles (exclusion / 1-4 masks) belong to the FP64 kernel.
+        if (mref < mend && a.mask_refs[mref].j_tile == jt) continue;
+        force_tile(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia, a, fx, fy, fz);
         acc0 += static_cast<double>(fx);
         acc1 += static_cast<double>(fy);
         acc2 += static_cast<double>(fz);
@@ -238,6 +226,72 @@ void launch_force_pass(const PairArgs& a, cudaStream_t s) {
 }
 
 int pair_warps_per_cta() { return kWarps; }
+
+// ------------------------------------------------------- FP64 near field
+// One warp per near-field (i-tile, j-tile) pair -- the tiles that carry
+// exclusion / 1-4 masks, i.e. the bonded neighbourhood where the large LJ and
+// Coulomb pair forces cancel against the bonded terms.  FP64 throughout, term
+// for term as forces_nonbonded.rs:196-232 + forces_gb.rs:82-111; the j atoms
+// are warp-uniform broadcast loads.
+namespace {
+
+__global__ void __launch_bounds__(128) k_near64(PairArgs a, const int4* __restrict__ near, int n_near) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= n_near) return;
+  const int4 w = near[wid];  // i_tile, j_tile, mask offset
+  const int i = w.x * kTile + lane;
+  const uint32_t ex = a.mask_ex[w.z * kTile + lane];
+  const uint32_t m14 = a.mask_14[w.z * kTile + lane];
+  const double xi = a.x64[i], yi = a.y64[i], zi = a.z64[i], qi = a.q64[i], Ri = a.born_r64[i];
+  const double rmi = a.rmin64[i], epi = a.eps64[i], rm14i = a.rmin14_64[i], ep14i = a.eps14_64[i];
+  const double coul_kj = kCoulomb * kKcalToKj;
+  const double gb_pref = (1.0 - 1.0 / kEpsWater) * kCoulomb * kKcalToKj;
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  const int j0 = w.y * kTile;
+  for (int k = 0; k < kTile; ++k) {
+    const int j = j0 + k;
+    if (!a.atom_valid[j]) continue;
+    const double dx = a.x64[j] - xi, dy = a.y64[j] - yi, dz = a.z64[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < 1e-18) continue;
+    const double qq = qi * a.q64[j];
+    double coeff = 0.0;
+    if (!((ex >> k) & 1u) && r2 <= a.nb_c2_64) {
+      const bool is14 = (m14 >> k) & 1u;
+      const double rmin = is14 ? rm14i + a.rmin14_64[j] : rmi + a.rmin64[j];
+      const double eps = sqrt(is14 ? ep14i * a.eps14_64[j] : epi * a.eps64[j]);
+      const double inv_r2 = 1.0 / r2;
+      const double ratio2 = rmin * rmin * inv_r2;
+      const double r6 = ratio2 * ratio2 * ratio2;
+      coeff += 12.0 * eps * inv_r2 * (r6 - r6 * r6) * kKcalToKj;
+      if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 / sqrt(r2) - a.inv_rc3_64);
+    }
+    if (qq != 0.0 && r2 <= a.gb_c2_64) {
+      const double r = sqrt(r2);
+      const double rp = Ri * a.born_r64[j];
+      const double e = exp(-r2 / (4.0 * rp));
+      const double f2 = r2 + rp * e;
+      const double f = sqrt(f2);
+      coeff += gb_pref * qq / f2 * ((2.0 * r - 0.5 * r * e) / (2.0 * f)) / r;
+    }
+    ax += dx * coeff;
+    ay += dy * coeff;
+    az += dz * coeff;
+  }
+  if (a.atom_valid[i]) {
+    if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
+    add_fixed(a.fx + i, ax, kForceScale);
+    add_fixed(a.fy + i, ay, kForceScale);
+    add_fixed(a.fz + i, az, kForceScale);
+  }
+}
+
+}  // namespace
+
+void launch_near_force64(const PairArgs& a, const int4* near, int n_near, cudaStream_t s) {
+  if (n_near > 0) k_near64<<<(n_near * 32 + 127) / 128, 128, 0, s>>>(a, near, n_near);
+}
 
 // ----------------------------------------------------------------- FP64 path
 

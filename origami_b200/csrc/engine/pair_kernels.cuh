@@ -55,10 +55,22 @@ struct PairArgs {
   // carry a NaN, so it is recorded here and turned into divergence)
   const int32_t* atom_sys;
   int32_t* sys_nonfinite;
+  // Near-field tiles (those carrying exclusion / 1-4 masks: the bonded
+  // neighbourhood, where large pair forces cancel against the bonded terms)
+  // are evaluated in FP64 from these arrays.
+  const double* x64; const double* y64; const double* z64;
+  const double* q64;
+  const double* rmin64; const double* eps64; const double* rmin14_64; const double* eps14_64;
+  const double* born_r64;
+  double nb_c2_64, gb_c2_64, inv_rc3_64;
 };
 
 void launch_born_pass(const PairArgs& a, cudaStream_t s);
+// Far field (tiles without exclusion masks), FP32.
 void launch_force_pass(const PairArgs& a, cudaStream_t s);
+// Near field: near[k] = (i_tile, j_tile, mask block, 0) for every ordered tile
+// pair that carries masks, FP64.
+void launch_near_force64(const PairArgs& a, const int4* near, int n_near, cudaStream_t s);
 
 // FP64 energy evaluation, one thread per i atom over every j of its system.
 struct EnergyArgs {

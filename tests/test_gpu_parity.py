@@ -37,6 +37,25 @@ def jitter(x, scale=0.05, seed=0):
     return x + np.random.default_rng(seed).normal(scale=scale, size=x.shape)
 
 
+_MIN_CACHE = {}
+
+
+def minimized(origami, seq, helical=False):
+    """Chain relaxed by L-BFGS on the CPU oracle (deterministic start for MD tests;
+    origami likewise minimises before dynamics)."""
+    key = (seq, helical)
+    if key not in _MIN_CACHE:
+        from test_minimize import OracleEngine
+        from origami_b200.minimize import MinimizeOptions, lbfgs
+        ch = helix(origami, seq) if helical else origami.Chain.build(seq)
+        eng = OracleEngine(ch)
+        lbfgs(eng, 0, MinimizeOptions(max_steps=300, gradient_tol=5.0))
+        _MIN_CACHE[key] = eng.x.copy()
+    ch = helix(origami, seq) if helical else origami.Chain.build(seq)
+    ch.positions = _MIN_CACHE[key]
+    return ch
+
+
 def make_engine(origami, chain, xyz=None, params=None, temperature=310.0):
     eng = origami.Engine(params or origami.Params())
     eng.add_system(chain, chain.positions if xyz is None else xyz, temperature)
@@ -100,8 +119,8 @@ def test_batched_uneven_systems_match_single(origami):
 
 @pytest.mark.parametrize("shake", [False, True])
 def test_baoab_steps_match_oracle(origami, shake):
-    ch = helix(origami, "AKEWL")
-    x0 = jitter(ch.positions, 0.01, 4)
+    ch = minimized(origami, "AKEWL", helical=True)
+    x0 = ch.positions
     dt = 2.0 if shake else 1.0
     params = origami.Params(dt_fs=dt, friction_ps_inv=2.0, constrain_h_bonds=shake, seed=1234)
     eng = make_engine(origami, ch, x0, params, temperature=310.0)
@@ -130,7 +149,7 @@ def test_baoab_steps_match_oracle(origami, shake):
 
 
 def test_deterministic_rerun(origami):
-    ch = helix(origami, TRP)
+    ch = minimized(origami, TRP)
     runs = []
     for _ in range(2):
         eng = make_engine(origami, ch, None, origami.Params(dt_fs=2.0, constrain_h_bonds=True, seed=5))
@@ -156,7 +175,7 @@ def test_initial_velocities_follow_reference_stream(origami):
 
 def test_thermostat_reaches_target(origami):
     # dynamics/tests/langevin_thermostat.rs: Ala3, 310 K, 2000 steps -> mean T within 60 K
-    ch = origami.Chain.build("AAA")
+    ch = minimized(origami, "AAA")
     res = origami.run_langevin(ch, origami.LangevinOptions(steps=2000, save_every=10, seed=3, friction_ps_inv=5.0))
     assert not res["diverged"]
     assert abs(res["temperature_mean_k"] - 310.0) < 60.0
@@ -164,7 +183,7 @@ def test_thermostat_reaches_target(origami):
 
 def test_shake_dt2_no_failures(origami):
     # dynamics/tests/shake_dt2.rs: Trp-cage at dt 2 fs + SHAKE, 0 failures, T within 80 K
-    ch = origami.Chain.build(TRP)
+    ch = minimized(origami, TRP)
     res = origami.run_langevin(ch, origami.LangevinOptions(steps=1000, dt_fs=2.0, constrain_h_bonds=True,
                                                            save_every=20, seed=11, friction_ps_inv=5.0))
     assert res["shake_failures"] == 0 and not res["diverged"]
@@ -196,7 +215,7 @@ def test_remd_swap_exchanges_configurations(origami):
 
 def test_remd_driver_accepts(origami):
     # dynamics/tests/remd_acceptance.rs: Ala3, 4 replicas, best acceptance > 0.1
-    ch = origami.Chain.build("AAA")
+    ch = minimized(origami, "AAA")
     res = origami.run_remd(ch, origami.RemdOptions(temperatures_k=[300, 330, 360, 400], total_time_fs=4000.0,
                                                    swap_interval_fs=100.0, seed=9))
     assert max(res["acceptance_ratios"]) > 0.1
