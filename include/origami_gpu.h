@@ -227,6 +227,9 @@ og_status og_compute_energies(og_engine* e, int32_t sys, og_energies* out);
 /* Effective Born radii of system `sys` (gb.rs:203 compute_born_radii_into_scratch);
  * out receives n_atoms doubles. */
 og_status og_get_born_radii(og_engine* e, int32_t sys, double* radii);
+/* The descreening integrals behind those radii (ForceScratch::gb_integral,
+ * scratch.rs:95), n_atoms doubles in 1/A, from the last force evaluation. */
+og_status og_get_born_integrals(og_engine* e, int32_t sys, double* integrals);
 
 /* Advance every system by n_steps BAOAB(+SHAKE) steps (the loop body of
  * run_langevin, langevin.rs:223-342).  Per-system status words record

@@ -294,6 +294,25 @@ int orc_nonbonded_energy(const og_topology* t, const double* xyz, double cutoff,
   return static_cast<int>(pairs);
 }
 
+// Descreening integrals I_i (energy/src/gb.rs:268-324), before the OBC map.
+void orc_born_integrals(const og_topology* t, const double* xyz, double born_cutoff, double* out) {
+  const int n = t->n_atoms;
+  const bool all = no_cutoff(born_cutoff);
+  const double c2 = born_cutoff * born_cutoff;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n; ++i) {
+    double acc = 0.0;
+    const double rti = t->gb_rho[i] - kObcOffset;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      double r2 = norm2(P(xyz, j) - P(xyz, i));
+      if ((!all && r2 > c2) || r2 < 1e-18) continue;
+      acc += pairwise_descreening(std::sqrt(r2), rti, t->gb_scale[j] * (t->gb_rho[j] - kObcOffset));
+    }
+    out[i] = acc;
+  }
+}
+
 // energy/src/gb.rs:100-144.  Returns the clamp count.
 int orc_born_radii(const og_topology* t, const double* xyz, double born_cutoff, double* radii) {
   return born_radii(t, xyz, born_cutoff, radii);

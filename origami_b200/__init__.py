@@ -371,6 +371,12 @@ class Engine:
         _check(lib().og_get_born_radii(self._h, sys, _dptr(r)))
         return r
 
+    def born_integrals(self, sys: int = 0) -> np.ndarray:
+        """Descreening integrals of the last force evaluation (1/A)."""
+        r = np.empty(self._n_atoms[sys])
+        _check(lib().og_get_born_integrals(self._h, sys, _dptr(r)))
+        return r
+
     def energies(self, sys: int = 0) -> dict:
         e = F.og_energies()
         _check(lib().og_compute_energies(self._h, sys, C.byref(e)))

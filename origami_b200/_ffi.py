@@ -93,6 +93,7 @@ SIGNATURES = [
     ("og_compute_forces", C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
     ("og_compute_energies", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(og_energies)]),
     ("og_get_born_radii", C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
+    ("og_get_born_integrals", C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
     ("og_step", C.c_int, [C.c_void_p, C.c_int32]),
     ("og_system_stats", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), c_int32_p]),
     ("og_kinetic", C.c_int, [C.c_void_p, C.c_int32, c_double_p, c_double_p]),

@@ -24,6 +24,9 @@ CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "liborigami_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# FP32 pair kernels flush denormals (no subnormal fix-up paths around the
+# MUFU rsqrt / ex2); every FP64 path is unaffected by -ftz.
+PER_FILE_FLAGS = {"pair_kernels.cu": ["-ftz=true"]}
 
 
 def nvcc() -> str:
@@ -69,7 +72,8 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
         obj = os.path.join(BUILD, rel + ".o")
         objs.append(obj)
         if force or _stale(obj, src, hdr_mtime):
-            jobs.append([*common, *opt, "-c", src, "-o", obj])
+            extra = PER_FILE_FLAGS.get(os.path.basename(src), [])
+            jobs.append([*common, *opt, *extra, "-c", src, "-o", obj])
 
     def run(cmd: list[str]) -> tuple[int, str, list[str]]:
         p = subprocess.run(cmd, capture_output=True, text=True)

@@ -25,6 +25,7 @@
 
 namespace ogk {
 int pair_warps_per_cta();
+int force_warps_per_cta();
 }
 
 namespace {
@@ -163,7 +164,9 @@ struct og_engine {
   DVec<int32_t> excl_row, excl_col;
   DVec<int8_t> excl_kind;
   DVec<int4> near;
-  int n_work = 0, n_near = 0;
+  DVec<ogk::PairWork> work_f;   // far-field force: upper-triangle tile pairs
+  DVec<int32_t> jlist_f;
+  int n_work = 0, n_near = 0, n_work_f = 0;
   // bonded
   DVec<int2> bond_atoms, dih_terms;
   DVec<int4> angle_atoms, dih_atoms, imp_atoms;
@@ -328,7 +331,11 @@ struct og_engine {
     }
     {
       Timer t(this, "force_pass");
-      ogk::launch_force_pass(pa, stream);
+      ogk::PairArgs pf = pa;
+      pf.work = work_f.p;
+      pf.n_work = n_work_f;
+      pf.jlist = jlist_f.p;
+      ogk::launch_force_pass(pf, stream);
     }
     {
       Timer t(this, "near_force64");
@@ -593,6 +600,30 @@ og_status finalize_impl(og_engine* e) {
   e->n_work = static_cast<int>(hw.size());
   OG_CUDA(e->work.upload(hw, st));
   OG_CUDA(e->jlist.upload(hj, st));
+
+  // Far-field force work (Newton-3): i-blocks of WF tiles against the tiles
+  // after the block's first tile, cut into chunks of at most 16 j-tiles.
+  {
+    const int WF = ogk::force_warps_per_cta();
+    const int chunk = 16;
+    std::vector<int32_t> hjf;
+    std::vector<ogk::PairWork> hwf;
+    for (const auto& s : e->sys) {
+      for (int t0 = 0; t0 < s.n_tiles; t0 += WF) {
+        const int jb = static_cast<int>(hjf.size());
+        for (int t = t0 + 1; t < s.n_tiles; ++t) hjf.push_back(s.tile_begin + t);
+        const int je = static_cast<int>(hjf.size());
+        for (int j0 = jb; j0 < je; j0 += chunk)
+          hwf.push_back(ogk::PairWork{s.tile_begin + t0, std::min(WF, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
+      }
+    }
+    std::stable_sort(hwf.begin(), hwf.end(), [](const ogk::PairWork& a, const ogk::PairWork& b) {
+      return (a.j_end - a.j_begin) > (b.j_end - b.j_begin);
+    });
+    e->n_work_f = static_cast<int>(hwf.size());
+    OG_CUDA(e->work_f.upload(hwf, st));
+    OG_CUDA(e->jlist_f.upload(hjf, st));
+  }
 
   // ---- exclusion masks (per ordered tile pair) and the FP64 CSR
   std::map<std::pair<int, int>, int> mask_of;  // (ti, tj) -> block
@@ -1017,6 +1048,19 @@ og_status og_get_born_radii(og_engine* e, int32_t s, double* radii) {
   if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
   if ((st = copy_sys_range(e, e->born_r, s, radii)) != OG_OK) return st;
   OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_get_born_integrals(og_engine* e, int32_t s, double* out) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!out) return og_fail(OG_E_BADARG, "null output");
+  if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
+  const int n = e->sys[s].topo.n;
+  std::vector<unsigned long long> h(n);
+  if ((st = copy_sys_range(e, e->born_sum, s, h.data())) != OG_OK) return st;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  for (int i = 0; i < n; ++i) out[i] = static_cast<double>(static_cast<long long>(h[i])) * ogk::kBornUnscale;
   return OG_OK;
 }
 

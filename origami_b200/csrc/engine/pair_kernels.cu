@@ -7,14 +7,15 @@
 //                  nonbonded cutoff (energy/src/forces_nonbonded.rs:196-232)
 //                  fused with the frozen-radii GB pair force within the GB
 //                  cutoff (energy/src/forces_gb.rs:82-111).
-// Layout: one warp owns one 32-atom i-tile; a CTA of kWarps warps walks a
-// list of 32-atom j-tiles that thread 0 streams into shared memory with 1-D
-// TMA bulk copies (double buffered, mbarrier completion, bounded waits); each
-// j atom is then read by all 32 lanes as a shared-memory broadcast.  Every
-// ordered pair is evaluated from its i side (no Newton-3 j scatter), so each
-// i atom's sum is formed in a fixed order: FP32 per j-tile, FP64 across tiles,
-// and one 64-bit fixed-point atomic per atom per work item -- results are
-// bit-reproducible whatever the launch order.
+// Layout: one warp owns one 32-atom i-tile; a CTA of warps walks a list of
+// 32-atom j-tiles that thread 0 streams into shared memory with 1-D TMA bulk
+// copies (double buffered, mbarrier completion, bounded waits); each j atom
+// is then read by all 32 lanes as a shared-memory broadcast.  The Born pass
+// evaluates every ordered pair from its i side (h_ij and h_ji are different
+// functions); the force pass evaluates each unordered far-field pair once and
+// reduces the j-side force across the warp.  Every sum is formed in a fixed
+// order (FP32 per j-tile, FP64 across tiles, 64-bit fixed point across work
+// items), so results are bit-reproducible whatever the launch order.
 //
 // Positions reach the pair kernels as FP32 offsets from a per-tile FP64
 // origin; the origin difference of a tile pair is formed in FP64 once per
@@ -36,9 +37,35 @@ constexpr float kLog2e = 1.4426950408889634f;
 __device__ __forceinline__ float fast_rcp(float x) { return __fdividef(1.0f, x); }
 
 // Born pass: h(r, rho_i, s_rho_j) summed over one staged j-tile.
-// Algebraically the reference's four terms with term2 + term4 folded into
-// (s^2 / 4r)(1/U^2 - 1/L^2), and ln(L/U) = log1p(-2 s / U) on the
-// non-overlapping branch, which keeps the FP32 evaluation well conditioned.
+//
+// origami's pairwise_descreening (gb.rs:347-369) is
+//   h = 1/2 (1/L - 1/U) + (r/4)(1/U^2 - 1/L^2) + ln(L/U)/(2r)
+//       + (s^2 - r^2)/(4r) (1/U^2 - 1/L^2),      L = max(rho_i, r - s), U = r + s.
+// Its terms cancel to O(s^3/r^4) for distant pairs, so FP32 evaluation of the
+// closed form loses most digits there.  On the non-overlapping branch
+// (L = r - s) the expression is, exactly, the series in x = s/r
+//   h = -(x^3 / r) * sum_{k>=1} k(2k-1)/(2k+1) x^(2(k-1))
+// (expand 1/(1-x^2), 1/(1-x^2)^2 and atanh x = -ln((1-x)/(1+x))/2 and collect
+// powers).  For x < 1/4 eight terms leave a truncation error below 1e-8
+// relative, under FP32 rounding.  A j atom takes that path when every lane's
+// pair is distant (warp vote); otherwise all lanes use the closed form with
+// term2 + term4 folded into (s^2 / 4r)(1/U^2 - 1/L^2) and
+// ln(L/U) = log1p((L - U)/U).
+constexpr float kSeriesMaxX = 0.25f;
+
+__device__ __forceinline__ float descreen_series(float x, float inv_r) {
+  const float x2 = x * x;
+  float p = 120.0f / 17.0f;                 // k = 8
+  p = fmaf(p, x2, 91.0f / 15.0f);           // k = 7
+  p = fmaf(p, x2, 66.0f / 13.0f);           // k = 6
+  p = fmaf(p, x2, 45.0f / 11.0f);           // k = 5
+  p = fmaf(p, x2, 28.0f / 9.0f);            // k = 4
+  p = fmaf(p, x2, 15.0f / 7.0f);            // k = 3
+  p = fmaf(p, x2, 6.0f / 5.0f);             // k = 2
+  p = fmaf(p, x2, 1.0f / 3.0f);             // k = 1
+  return -(x2 * x * inv_r) * p;
+}
+
 __device__ __forceinline__ float born_tile(const float4* __restrict__ sp, const float4* __restrict__ sg, float xi,
                                            float yi, float zi, float rho, float born_c2) {
   float acc = 0.0f;
@@ -50,15 +77,22 @@ __device__ __forceinline__ float born_tile(const float4* __restrict__ sp, const 
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     const float inv_r = rsqrtf(r2);
     const float r = r2 * inv_r;
-    const bool overlap = (r - sr) < rho;
-    const float L = overlap ? rho : r - sr;
-    const float U = r + sr;
-    const float inv_l = fast_rcp(L), inv_u = fast_rcp(U);
-    const float lg = overlap ? logf(L * inv_u) : log1pf(-2.0f * sr * inv_u);
-    const float d2 = inv_u * inv_u - inv_l * inv_l;
-    float h = 0.5f * (inv_l - inv_u) + (sr * sr) * (0.25f * inv_r) * d2 + (0.5f * inv_r) * lg;
-    const bool on = (r2 <= born_c2) && (r2 >= 1e-18f) && !(r + sr <= rho) && (U > 0.0f) && (L > 0.0f);
-    acc += on ? h : 0.0f;
+    const float x = sr * inv_r;
+    const bool far = (x < kSeriesMaxX) && (r - sr >= rho);
+    float h;
+    if (__all_sync(0xffffffffu, far)) {
+      h = descreen_series(x, inv_r);
+    } else {
+      const bool overlap = (r - sr) < rho;
+      const float L = overlap ? rho : r - sr;
+      const float U = r + sr;
+      const float inv_l = fast_rcp(L), inv_u = fast_rcp(U);
+      const float lg = log1pf((overlap ? rho - U : -2.0f * sr) * inv_u);
+      const float d2 = inv_u * inv_u - inv_l * inv_l;
+      h = 0.5f * (inv_l - inv_u) + (sr * sr) * (0.25f * inv_r) * d2 + (0.5f * inv_r) * lg;
+      h = (!(r + sr <= rho) && (U > 0.0f) && (L > 0.0f)) ? h : 0.0f;
+    }
+    acc += ((r2 <= born_c2) && (r2 >= 1e-18f)) ? h : 0.0f;
   }
   return acc;
 }
@@ -67,55 +101,21 @@ struct IAtom {
   float x, y, z;
   float cq;     // -coul_kj * q_i
   float gq;     // gb_pref_kj * q_i
-  float rm, se, rm14, se14;
+  float rm;     // Rmin/2
+  float se;     // 12 * 4.184 * sqrt(eps)
   float R;      // Born radius
   float nexp;   // -0.25 * log2(e) / R_i
 };
 
-// Far-field tile (no exclusions, no 1-4 pairs): FP32 pair math.
-__device__ __forceinline__ void force_tile(const float4* __restrict__ sp, const float4* __restrict__ sl,
-                                           const float4* __restrict__ sg, const IAtom& ia, const PairArgs& a,
-                                           float& fx, float& fy, float& fz) {
-#pragma unroll 4
-  for (int k = 0; k < kTile; ++k) {
-    const float4 p = sp[k];
-    const float4 l = sl[k];
-    const float2 g = *reinterpret_cast<const float2*>(&sg[k]);
-    const float dx = p.x - ia.x, dy = p.y - ia.y, dz = p.z - ia.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float inv_r = rsqrtf(r2);
-    const float inv_r2 = inv_r * inv_r;
-    const float rmin = ia.rm + l.x;
-    const float se = ia.se * l.y;
-    const bool nb_on = r2 <= a.nb_c2;
-    const float ratio2 = rmin * rmin * inv_r2;
-    const float r6 = ratio2 * ratio2 * ratio2;
-    const float ljc = a.lj_kj12 * se * inv_r2 * fmaf(-r6, r6, r6);
-    const float coul = ia.cq * p.w * fmaf(inv_r2, inv_r, -a.inv_rc3);
-    const float e = exp2f(r2 * ia.nexp * g.y);
-    const float f2 = fmaf(ia.R * g.x, e, r2);
-    const float inv_f = rsqrtf(f2);
-    const float gbc = ia.gq * p.w * fmaf(-0.25f, e, 1.0f) * (inv_f * inv_f * inv_f);
-    float coeff = (nb_on ? ljc + coul : 0.0f) + ((r2 <= a.gb_c2) ? gbc : 0.0f);
-    coeff = (r2 >= 1e-18f) ? coeff : 0.0f;
-    fx = fmaf(dx, coeff, fx);
-    fy = fmaf(dy, coeff, fy);
-    fz = fmaf(dz, coeff, fz);
-  }
-}
-
-// kPass 0 = Born descreening integral, 1 = force.
-template <int kPass>
-__global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
-  constexpr int kArrays = kPass == 0 ? 2 : 3;
+// Born descreening integral I_i over every j of the i-tile's j list.
+__global__ void __launch_bounds__(kWarps * 32) k_born(PairArgs a) {
   constexpr uint32_t kTileBytes = kTile * sizeof(float4);
-  __shared__ __align__(128) float4 s_buf[2][kArrays][kStageTiles * kTile];
+  __shared__ __align__(128) float4 s_buf[2][2][kStageTiles * kTile];
   __shared__ __align__(8) uint64_t s_bar[2];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const PairWork w = a.work[blockIdx.x];
-  const int nj = w.j_end - w.j_begin;
-  const int n_stages = (nj + kStageTiles - 1) / kStageTiles;
+  const int n_stages = (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles;
 
   if (threadIdx.x == 0) {
     mbar_init(&s_bar[0], 1);
@@ -123,22 +123,125 @@ __global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
     fence_mbar_init();
   }
   __syncthreads();
-
   auto issue = [&](int s) {
     const int buf = s & 1;
     const int t0 = w.j_begin + s * kStageTiles;
     const int cnt = min(kStageTiles, w.j_end - t0);
-    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * kArrays);
+    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * 2);
     for (int t = 0; t < cnt; ++t) {
-      const int jt = a.jlist[t0 + t];
-      const size_t base = static_cast<size_t>(jt) * kTile;
+      const size_t base = static_cast<size_t>(a.jlist[t0 + t]) * kTile;
       bulk_g2s(&s_buf[buf][0][t * kTile], a.pq + base, kTileBytes, &s_bar[buf]);
-      if (kPass == 0) {
-        bulk_g2s(&s_buf[buf][1][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
-      } else {
-        bulk_g2s(&s_buf[buf][1][t * kTile], a.lj + base, kTileBytes, &s_bar[buf]);
-        bulk_g2s(&s_buf[buf][2][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
-      }
+      bulk_g2s(&s_buf[buf][1][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    if (n_stages > 0) issue(0);
+    if (n_stages > 1) issue(1);
+  }
+
+  const bool active = warp < w.n_i_tiles;
+  const int it = w.i_tile0 + (active ? warp : 0);
+  const int i = it * kTile + lane;
+  const float4 pi = a.pq[i];
+  const double4 oi = a.origin[it];
+  const float rho_i = a.gb[i].z;
+  double acc = 0.0;
+  for (int s = 0; s < n_stages; ++s) {
+    const int buf = s & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[buf], static_cast<uint32_t>((s >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
+      return;
+    }
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    for (int t = 0; t < cnt; ++t) {
+      const double4 oj = a.origin[a.jlist[t0 + t]];
+      const float xi = pi.x - static_cast<float>(oj.x - oi.x);
+      const float yi = pi.y - static_cast<float>(oj.y - oi.y);
+      const float zi = pi.z - static_cast<float>(oj.z - oi.z);
+      acc += static_cast<double>(
+          born_tile(&s_buf[buf][0][t * kTile], &s_buf[buf][1][t * kTile], xi, yi, zi, rho_i, a.born_c2));
+    }
+    __syncthreads();  // every warp is done with `buf`
+    if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
+  }
+  if (active && a.atom_valid[i]) {
+    if (!isfinite(acc)) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
+    add_fixed(a.born_sum + i, acc, kBornScale);
+  }
+}
+
+}  // namespace
+
+void launch_born_pass(const PairArgs& a, cudaStream_t s) {
+  if (a.n_work > 0) k_born<<<a.n_work, kWarps * 32, 0, s>>>(a);
+}
+
+// ------------------------------------------------- far-field force, Newton-3
+// Each unordered far-field tile pair (ti < tj, no masks) is evaluated once:
+// the warp owning i-tile ti walks j-tile tj, every lane accumulates its i
+// force in registers, and the force on each j atom (minus the sum over the
+// 32 lanes) is formed by a butterfly reduction and kept by lane k for j = k.
+// Per stage the W warps' j partials are summed in shared memory in a fixed
+// order and added to the 64-bit fixed-point accumulators with one atomic per
+// j atom and component, so results stay bit-reproducible.
+namespace {
+
+constexpr int kN3Warps = 8;
+
+template <bool kAllPairs>
+__device__ __forceinline__ float pair_coeff(const float4 p, const float4 l, const float2 g, const IAtom& ia,
+                                            const PairArgs& a, float dx, float dy, float dz) {
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const float inv_r = rsqrtf(r2);
+  const float inv_r2 = inv_r * inv_r;
+  const float rmin = ia.rm + l.x;
+  const float ratio2 = rmin * rmin * inv_r2;
+  const float r6 = ratio2 * ratio2 * ratio2;
+  const float ljc = (ia.se * l.y) * inv_r2 * fmaf(-r6, r6, r6);       // ia.se carries 12 * 4.184
+  const float coul = ia.cq * p.w * fmaf(inv_r2, inv_r, -a.inv_rc3);
+  const float e = exp2f(r2 * ia.nexp * g.y);
+  const float f2 = fmaf(ia.R * g.x, e, r2);
+  const float inv_f = rsqrtf(f2);
+  const float gbc = ia.gq * p.w * fmaf(-0.25f, e, 1.0f) * (inv_f * inv_f * inv_f);
+  float coeff;
+  if (kAllPairs) {
+    coeff = ljc + coul + gbc;
+  } else {
+    coeff = ((r2 <= a.nb_c2) ? ljc + coul : 0.0f) + ((r2 <= a.gb_c2) ? gbc : 0.0f);
+  }
+  return (r2 >= 1e-18f) ? coeff : 0.0f;
+}
+
+template <bool kAllPairs>
+__global__ void __launch_bounds__(kN3Warps * 32) k_force_n3(PairArgs a) {
+  constexpr uint32_t kTileBytes = kTile * sizeof(float4);
+  constexpr int kStageAtoms = kStageTiles * kTile;
+  __shared__ __align__(128) float4 s_buf[2][3][kStageAtoms];
+  __shared__ float s_jf[kN3Warps][3][kStageAtoms];
+  __shared__ __align__(8) uint64_t s_bar[2];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const PairWork w = a.work[blockIdx.x];
+  const int n_stages = (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int s) {
+    const int buf = s & 1;
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * 3);
+    for (int t = 0; t < cnt; ++t) {
+      const size_t base = static_cast<size_t>(a.jlist[t0 + t]) * kTile;
+      bulk_g2s(&s_buf[buf][0][t * kTile], a.pq + base, kTileBytes, &s_bar[buf]);
+      bulk_g2s(&s_buf[buf][1][t * kTile], a.lj + base, kTileBytes, &s_bar[buf]);
+      bulk_g2s(&s_buf[buf][2][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
     }
   };
   if (threadIdx.x == 0) {
@@ -152,22 +255,20 @@ __global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
   const float4 pi = a.pq[i];
   const double4 oi = a.origin[it];
   IAtom ia;
-  float rho_i = 0.0f;
-  if (kPass == 0) {
-    rho_i = a.gb[i].z;
-  } else {
+  {
     const float4 li = a.lj[i];
     const float4 gi = a.gb[i];
     ia.cq = -a.coul_kj * pi.w;
     ia.gq = a.gb_pref_kj * pi.w;
-    ia.rm = li.x; ia.se = li.y; ia.rm14 = li.z; ia.se14 = li.w;
+    ia.rm = li.x;
+    ia.se = a.lj_kj12 * li.y;
     ia.R = gi.x;
     ia.nexp = -0.25f * kLog2e * gi.y;
   }
   int mref = a.mask_begin[it];
   const int mend = a.mask_begin[it + 1];
-
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+
   for (int s = 0; s < n_stages; ++s) {
     const int buf = s & 1;
     const bool ok = mbar_wait_bounded(&s_bar[buf], static_cast<uint32_t>((s >> 1) & 1));
@@ -179,50 +280,87 @@ __global__ void __launch_bounds__(kWarps * 32) k_pairs(PairArgs a) {
     const int cnt = min(kStageTiles, w.j_end - t0);
     for (int t = 0; t < cnt; ++t) {
       const int jt = a.jlist[t0 + t];
-      const double4 oj = a.origin[jt];
-      const float xi = pi.x - static_cast<float>(oj.x - oi.x);
-      const float yi = pi.y - static_cast<float>(oj.y - oi.y);
-      const float zi = pi.z - static_cast<float>(oj.z - oi.z);
-      const float4* sp = &s_buf[buf][0][t * kTile];
-      if (kPass == 0) {
-        acc0 += static_cast<double>(born_tile(sp, &s_buf[buf][1][t * kTile], xi, yi, zi, rho_i, a.born_c2));
-      } else {
-        while (mref < mend && a.mask_refs[mref].j_tile < jt) ++mref;
+      while (mref < mend && a.mask_refs[mref].j_tile < jt) ++mref;
+      const bool masked = mref < mend && a.mask_refs[mref].j_tile == jt;
+      float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+      if (active && jt > it && !masked) {
+        const double4 oj = a.origin[jt];
+        ia.x = pi.x - static_cast<float>(oj.x - oi.x);
+        ia.y = pi.y - static_cast<float>(oj.y - oi.y);
+        ia.z = pi.z - static_cast<float>(oj.z - oi.z);
+        const float4* sp = &s_buf[buf][0][t * kTile];
+        const float4* sl = &s_buf[buf][1][t * kTile];
+        const float4* sg = &s_buf[buf][2][t * kTile];
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        ia.x = xi; ia.y = yi; ia.z = zi;
-        // Near-field tiles (exclusion / 1-4 masks) belong to the FP64 kernel.
-        if (mref < mend && a.mask_refs[mref].j_tile == jt) continue;
-        force_tile(sp, &s_buf[buf][1][t * kTile], &s_buf[buf][2][t * kTile], ia, a, fx, fy, fz);
+#pragma unroll 8
+        for (int k = 0; k < kTile; ++k) {
+          const float4 p = sp[k];
+          const float4 l = sl[k];
+          const float2 g = *reinterpret_cast<const float2*>(&sg[k]);
+          const float dx = p.x - ia.x, dy = p.y - ia.y, dz = p.z - ia.z;
+          const float c = pair_coeff<kAllPairs>(p, l, g, ia, a, dx, dy, dz);
+          float ux = dx * c, uy = dy * c, uz = dz * c;
+          fx += ux;
+          fy += uy;
+          fz += uz;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            ux += __shfl_xor_sync(0xffffffffu, ux, o);
+            uy += __shfl_xor_sync(0xffffffffu, uy, o);
+            uz += __shfl_xor_sync(0xffffffffu, uz, o);
+          }
+          if (lane == k) {
+            jx = -ux;
+            jy = -uy;
+            jz = -uz;
+          }
+        }
         acc0 += static_cast<double>(fx);
         acc1 += static_cast<double>(fy);
         acc2 += static_cast<double>(fz);
       }
+      s_jf[warp][0][t * kTile + lane] = jx;
+      s_jf[warp][1][t * kTile + lane] = jy;
+      s_jf[warp][2][t * kTile + lane] = jz;
     }
-    __syncthreads();  // every warp is done with `buf`
+    __syncthreads();  // every warp is done with `buf` and has written its j partials
     if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
+    for (int q = threadIdx.x; q < cnt * kTile; q += blockDim.x) {
+      const int j = a.jlist[t0 + q / kTile] * kTile + (q % kTile);
+      if (!a.atom_valid[j]) continue;
+      float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+#pragma unroll
+      for (int ww = 0; ww < kN3Warps; ++ww) {
+        sx += s_jf[ww][0][q];
+        sy += s_jf[ww][1][q];
+        sz += s_jf[ww][2][q];
+      }
+      if (sx != 0.0f || sy != 0.0f || sz != 0.0f) {
+        if (!(isfinite(sx) && isfinite(sy) && isfinite(sz))) atomicOr(a.sys_nonfinite + a.atom_sys[j], 1);
+        add_fixed(a.fx + j, sx, kForceScale);
+        add_fixed(a.fy + j, sy, kForceScale);
+        add_fixed(a.fz + j, sz, kForceScale);
+      }
+    }
   }
-
   if (active && a.atom_valid[i]) {
     if (!(isfinite(acc0) && isfinite(acc1) && isfinite(acc2))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
-    if (kPass == 0) {
-      add_fixed(a.born_sum + i, acc0, kBornScale);
-    } else {
-      // The pair coefficient multiplies d = r_j - r_i, so the i-side force is +sum.
-      add_fixed(a.fx + i, acc0, kForceScale);
-      add_fixed(a.fy + i, acc1, kForceScale);
-      add_fixed(a.fz + i, acc2, kForceScale);
-    }
+    add_fixed(a.fx + i, acc0, kForceScale);
+    add_fixed(a.fy + i, acc1, kForceScale);
+    add_fixed(a.fz + i, acc2, kForceScale);
   }
 }
 
 }  // namespace
 
-void launch_born_pass(const PairArgs& a, cudaStream_t s) {
-  if (a.n_work > 0) k_pairs<0><<<a.n_work, kWarps * 32, 0, s>>>(a);
-}
+int force_warps_per_cta() { return kN3Warps; }
 
 void launch_force_pass(const PairArgs& a, cudaStream_t s) {
-  if (a.n_work > 0) k_pairs<1><<<a.n_work, kWarps * 32, 0, s>>>(a);
+  if (a.n_work <= 0) return;
+  if (a.nb_c2 == INFINITY && a.gb_c2 == INFINITY)
+    k_force_n3<true><<<a.n_work, kN3Warps * 32, 0, s>>>(a);
+  else
+    k_force_n3<false><<<a.n_work, kN3Warps * 32, 0, s>>>(a);
 }
 
 int pair_warps_per_cta() { return kWarps; }

@@ -52,6 +52,8 @@ def oracle() -> C.CDLL:
         o.orc_bonded_energy.restype = None
         o.orc_nonbonded_energy.argtypes = [tp, dp, C.c_double, dp]
         o.orc_nonbonded_energy.restype = C.c_int
+        o.orc_born_integrals.argtypes = [tp, dp, C.c_double, dp]
+        o.orc_born_integrals.restype = None
         o.orc_born_radii.argtypes = [tp, dp, C.c_double, dp]
         o.orc_born_radii.restype = C.c_int
         o.orc_gb_energy.argtypes = [tp, dp, C.c_double, dp]
@@ -113,6 +115,12 @@ class Orc:
         d = dict(zip(("bond", "angle", "dihedral", "improper", "lj", "coulomb", "gb", "gb_self", "gb_pair"), t))
         d["total"] = tot
         return d
+
+    def born_integrals(self, x=None, born=20.0):
+        x = self.xyz(x)
+        r = np.zeros(x.shape[0])
+        self.o.orc_born_integrals(self.tp, dp(x), born, dp(r))
+        return r
 
     def born_radii(self, x=None, born=20.0):
         x = self.xyz(x)

@@ -88,6 +88,22 @@ def test_born_radii_match_oracle(origami):
 
 
 @pytest.mark.parametrize("mode", ["cutoff", "all_pairs"])
+@pytest.mark.parametrize("build", ["extended", "helix"])
+def test_born_integrals_match_oracle(origami, mode, build):
+    # The radii all floor to rho - 0.09 (origami's descreening terms are
+    # negative), so the integral itself is what checks the Born pass.
+    # FP32 pair math: per-atom absolute error below 1e-6 of the largest |I|.
+    ch = origami.Chain.build(TRP) if build == "extended" else helix(origami, TRP)
+    x = jitter(ch.positions, 0.03, 5)
+    params = origami.Params() if mode == "cutoff" else origami.Params.all_pairs()
+    eng = make_engine(origami, ch, x, params)
+    eng.total_force(0)
+    got = eng.born_integrals(0)
+    ref = Orc(ch).born_integrals(x, 20.0 if mode == "cutoff" else INF)
+    assert np.max(np.abs(got - ref)) < 1e-6 * np.max(np.abs(ref)), np.max(np.abs(got - ref))
+
+
+@pytest.mark.parametrize("mode", ["cutoff", "all_pairs"])
 def test_energies_match_oracle(origami, mode):
     ch = helix(origami, TRP)
     x = jitter(ch.positions, 0.03, 3)
