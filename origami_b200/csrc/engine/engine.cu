@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <numeric>
@@ -58,7 +59,15 @@ struct DVec {
     release();
     n = count;
     if (count == 0) return cudaSuccess;
-    return cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    // OG_DEBUG_POISON=1 fills new buffers with 0xFF bytes (NaN as float or
+    // double) so a read before the first write shows up as a non-finite result.
+    if (e == cudaSuccess && poison_enabled()) e = cudaMemset(p, 0xFF, count * sizeof(T));
+    return e;
+  }
+  static bool poison_enabled() {
+    const char* v = std::getenv("OG_DEBUG_POISON");
+    return v && v[0] == '1';
   }
   cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
     cudaError_t e = alloc(h.size());
@@ -556,7 +565,14 @@ og_status finalize_impl(og_engine* e) {
   for (auto* v : {&e->fx, &e->fy, &e->fz, &e->born_sum}) OG_CUDA(v->alloc(np));
   OG_CUDA(e->n_pairs.alloc(np));
   OG_CUDA(e->pq.alloc(np));
-  OG_CUDA(e->gb.alloc(np));
+  // The Born pass reads rho~ and s*rho~ from these float4s before the first
+  // radii exist, so they start out fully defined (R = rho~ until then).
+  std::vector<float4> hgb(np, make_float4(1.0f, 1.0f, 1.0f, 0.0f));
+  for (int i = 0; i < np; ++i)
+    if (hsys[i] >= 0)
+      hgb[i] = make_float4(static_cast<float>(hrt[i]), static_cast<float>(1.0 / hrt[i]), static_cast<float>(hrt[i]),
+                           static_cast<float>(hsr[i]));
+  OG_CUDA(e->gb.upload(hgb, st));
   OG_CUDA(e->origin.alloc(e->n_tiles));
 
   // ---- per-system state
@@ -574,52 +590,34 @@ og_status finalize_impl(og_engine* e) {
   }
   OG_CUDA(e->sys_state.upload(hs, st));
 
-  // ---- pair work: i-blocks of W tiles x all tiles of the system, split so
-  // that the grid covers the GPU several times.
-  const int W = ogk::pair_warps_per_cta();
-  int dev = 0, n_sm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-  long long blocks = 0;
-  for (const auto& s : e->sys) blocks += (s.n_tiles + W - 1) / W;
-  const long long target = static_cast<long long>(n_sm) * 8;
-  std::vector<int32_t> hj;
-  std::vector<ogk::PairWork> hw;
-  for (const auto& s : e->sys) {
-    const int jb = static_cast<int>(hj.size());
-    for (int t = 0; t < s.n_tiles; ++t) hj.push_back(s.tile_begin + t);
-    const int je = static_cast<int>(hj.size());
-    int split = 1;
-    if (blocks < target) split = static_cast<int>(std::min<long long>((target + blocks - 1) / blocks, s.n_tiles / 4 + 1));
-    split = std::max(split, 1);
-    const int per = (s.n_tiles + split - 1) / split;
-    for (int t0 = 0; t0 < s.n_tiles; t0 += W)
-      for (int j0 = jb; j0 < je; j0 += per)
-        hw.push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + per)});
-  }
-  e->n_work = static_cast<int>(hw.size());
-  OG_CUDA(e->work.upload(hw, st));
-  OG_CUDA(e->jlist.upload(hj, st));
-
-  // Far-field force work (Newton-3): i-blocks of WF tiles against the tiles
-  // after the block's first tile, cut into chunks of at most 16 j-tiles.
+  // ---- pair work (Newton-3 layout): i-blocks of W consecutive tiles against
+  // the tiles from the block's first tile on (Born pass: the block's own
+  // diagonal included) or after it (far-field force pass), cut into chunks of
+  // at most 16 j-tiles and ordered longest first.
   {
-    const int WF = ogk::force_warps_per_cta();
+    const int W = ogk::force_warps_per_cta();
     const int chunk = 16;
-    std::vector<int32_t> hjf;
-    std::vector<ogk::PairWork> hwf;
-    for (const auto& s : e->sys) {
-      for (int t0 = 0; t0 < s.n_tiles; t0 += WF) {
-        const int jb = static_cast<int>(hjf.size());
-        for (int t = t0 + 1; t < s.n_tiles; ++t) hjf.push_back(s.tile_begin + t);
-        const int je = static_cast<int>(hjf.size());
-        for (int j0 = jb; j0 < je; j0 += chunk)
-          hwf.push_back(ogk::PairWork{s.tile_begin + t0, std::min(WF, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
+    auto build_list = [&](int first_offset, std::vector<ogk::PairWork>* hw, std::vector<int32_t>* hj) {
+      for (const auto& s : e->sys) {
+        for (int t0 = 0; t0 < s.n_tiles; t0 += W) {
+          const int jb = static_cast<int>(hj->size());
+          for (int t = t0 + first_offset; t < s.n_tiles; ++t) hj->push_back(s.tile_begin + t);
+          const int je = static_cast<int>(hj->size());
+          for (int j0 = jb; j0 < je; j0 += chunk)
+            hw->push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
+        }
       }
-    }
-    std::stable_sort(hwf.begin(), hwf.end(), [](const ogk::PairWork& a, const ogk::PairWork& b) {
-      return (a.j_end - a.j_begin) > (b.j_end - b.j_begin);
-    });
+      std::stable_sort(hw->begin(), hw->end(), [](const ogk::PairWork& a, const ogk::PairWork& b) {
+        return (a.j_end - a.j_begin) > (b.j_end - b.j_begin);
+      });
+    };
+    std::vector<int32_t> hj, hjf;
+    std::vector<ogk::PairWork> hw, hwf;
+    build_list(0, &hw, &hj);
+    build_list(1, &hwf, &hjf);
+    e->n_work = static_cast<int>(hw.size());
+    OG_CUDA(e->work.upload(hw, st));
+    OG_CUDA(e->jlist.upload(hj, st));
     e->n_work_f = static_cast<int>(hwf.size());
     OG_CUDA(e->work_f.upload(hwf, st));
     OG_CUDA(e->jlist_f.upload(hjf, st));

@@ -66,35 +66,16 @@ __device__ __forceinline__ float descreen_series(float x, float inv_r) {
   return -(x2 * x * inv_r) * p;
 }
 
-__device__ __forceinline__ float born_tile(const float4* __restrict__ sp, const float4* __restrict__ sg, float xi,
-                                           float yi, float zi, float rho, float born_c2) {
-  float acc = 0.0f;
-#pragma unroll 4
-  for (int k = 0; k < kTile; ++k) {
-    const float4 p = sp[k];
-    const float sr = sg[k].w;
-    const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float inv_r = rsqrtf(r2);
-    const float r = r2 * inv_r;
-    const float x = sr * inv_r;
-    const bool far = (x < kSeriesMaxX) && (r - sr >= rho);
-    float h;
-    if (__all_sync(0xffffffffu, far)) {
-      h = descreen_series(x, inv_r);
-    } else {
-      const bool overlap = (r - sr) < rho;
-      const float L = overlap ? rho : r - sr;
-      const float U = r + sr;
-      const float inv_l = fast_rcp(L), inv_u = fast_rcp(U);
-      const float lg = log1pf((overlap ? rho - U : -2.0f * sr) * inv_u);
-      const float d2 = inv_u * inv_u - inv_l * inv_l;
-      h = 0.5f * (inv_l - inv_u) + (sr * sr) * (0.25f * inv_r) * d2 + (0.5f * inv_r) * lg;
-      h = (!(r + sr <= rho) && (U > 0.0f) && (L > 0.0f)) ? h : 0.0f;
-    }
-    acc += ((r2 <= born_c2) && (r2 >= 1e-18f)) ? h : 0.0f;
-  }
-  return acc;
+// Closed form, valid on both branches.
+__device__ __forceinline__ float descreen_closed(float r, float inv_r, float rho, float sr) {
+  const bool overlap = (r - sr) < rho;
+  const float L = overlap ? rho : r - sr;
+  const float U = r + sr;
+  const float inv_l = fast_rcp(L), inv_u = fast_rcp(U);
+  const float lg = log1pf((overlap ? rho - U : -2.0f * sr) * inv_u);
+  const float d2 = inv_u * inv_u - inv_l * inv_l;
+  const float h = 0.5f * (inv_l - inv_u) + (sr * sr) * (0.25f * inv_r) * d2 + (0.5f * inv_r) * lg;
+  return (!(r + sr <= rho) && (U > 0.0f) && (L > 0.0f)) ? h : 0.0f;
 }
 
 struct IAtom {
@@ -107,76 +88,8 @@ struct IAtom {
   float nexp;   // -0.25 * log2(e) / R_i
 };
 
-// Born descreening integral I_i over every j of the i-tile's j list.
-__global__ void __launch_bounds__(kWarps * 32) k_born(PairArgs a) {
-  constexpr uint32_t kTileBytes = kTile * sizeof(float4);
-  __shared__ __align__(128) float4 s_buf[2][2][kStageTiles * kTile];
-  __shared__ __align__(8) uint64_t s_bar[2];
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const PairWork w = a.work[blockIdx.x];
-  const int n_stages = (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles;
-
-  if (threadIdx.x == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  auto issue = [&](int s) {
-    const int buf = s & 1;
-    const int t0 = w.j_begin + s * kStageTiles;
-    const int cnt = min(kStageTiles, w.j_end - t0);
-    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * 2);
-    for (int t = 0; t < cnt; ++t) {
-      const size_t base = static_cast<size_t>(a.jlist[t0 + t]) * kTile;
-      bulk_g2s(&s_buf[buf][0][t * kTile], a.pq + base, kTileBytes, &s_bar[buf]);
-      bulk_g2s(&s_buf[buf][1][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
-    }
-  };
-  if (threadIdx.x == 0) {
-    if (n_stages > 0) issue(0);
-    if (n_stages > 1) issue(1);
-  }
-
-  const bool active = warp < w.n_i_tiles;
-  const int it = w.i_tile0 + (active ? warp : 0);
-  const int i = it * kTile + lane;
-  const float4 pi = a.pq[i];
-  const double4 oi = a.origin[it];
-  const float rho_i = a.gb[i].z;
-  double acc = 0.0;
-  for (int s = 0; s < n_stages; ++s) {
-    const int buf = s & 1;
-    const bool ok = mbar_wait_bounded(&s_bar[buf], static_cast<uint32_t>((s >> 1) & 1));
-    if (__syncthreads_or(!ok)) {
-      if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
-      return;
-    }
-    const int t0 = w.j_begin + s * kStageTiles;
-    const int cnt = min(kStageTiles, w.j_end - t0);
-    for (int t = 0; t < cnt; ++t) {
-      const double4 oj = a.origin[a.jlist[t0 + t]];
-      const float xi = pi.x - static_cast<float>(oj.x - oi.x);
-      const float yi = pi.y - static_cast<float>(oj.y - oi.y);
-      const float zi = pi.z - static_cast<float>(oj.z - oi.z);
-      acc += static_cast<double>(
-          born_tile(&s_buf[buf][0][t * kTile], &s_buf[buf][1][t * kTile], xi, yi, zi, rho_i, a.born_c2));
-    }
-    __syncthreads();  // every warp is done with `buf`
-    if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
-  }
-  if (active && a.atom_valid[i]) {
-    if (!isfinite(acc)) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
-    add_fixed(a.born_sum + i, acc, kBornScale);
-  }
-}
-
 }  // namespace
 
-void launch_born_pass(const PairArgs& a, cudaStream_t s) {
-  if (a.n_work > 0) k_born<<<a.n_work, kWarps * 32, 0, s>>>(a);
-}
 
 // ------------------------------------------------- far-field force, Newton-3
 // Each unordered far-field tile pair (ti < tj, no masks) is evaluated once:
@@ -189,6 +102,26 @@ void launch_born_pass(const PairArgs& a, cudaStream_t s) {
 namespace {
 
 constexpr int kN3Warps = 8;
+
+// Reduce-scatter over the warp of four per-lane values v0..v3 (the
+// contributions to four consecutive j atoms): afterwards every lane of the
+// 8-lane group g = lane >> 3 holds the warp total of v_g.  Six shuffles
+// instead of the twenty of four separate butterflies; fixed order, so the
+// result does not depend on scheduling.
+__device__ __forceinline__ float reduce_scatter4(float v0, float v1, float v2, float v3, int lane) {
+  const bool hi16 = (lane & 16) != 0;
+  float k0 = hi16 ? v2 : v0, k1 = hi16 ? v3 : v1;   // kept: j = 2*hi16 + {0, 1}
+  const float s0 = hi16 ? v0 : v2, s1 = hi16 ? v1 : v3;
+  k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+  k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+  const bool hi8 = (lane & 8) != 0;
+  float k = hi8 ? k1 : k0;                           // kept: j = 2*hi16 + hi8 = lane >> 3
+  k += __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
+  k += __shfl_xor_sync(0xffffffffu, k, 4);
+  k += __shfl_xor_sync(0xffffffffu, k, 2);
+  k += __shfl_xor_sync(0xffffffffu, k, 1);
+  return k;
+}
 
 template <bool kAllPairs>
 __device__ __forceinline__ float pair_coeff(const float4 p, const float4 l, const float2 g, const IAtom& ia,
@@ -215,7 +148,7 @@ __device__ __forceinline__ float pair_coeff(const float4 p, const float4 l, cons
 }
 
 template <bool kAllPairs>
-__global__ void __launch_bounds__(kN3Warps * 32) k_force_n3(PairArgs a) {
+__global__ void __launch_bounds__(kN3Warps * 32, 2) k_force_n3(PairArgs a) {
   constexpr uint32_t kTileBytes = kTile * sizeof(float4);
   constexpr int kStageAtoms = kStageTiles * kTile;
   __shared__ __align__(128) float4 s_buf[2][3][kStageAtoms];
@@ -282,7 +215,9 @@ __global__ void __launch_bounds__(kN3Warps * 32) k_force_n3(PairArgs a) {
       const int jt = a.jlist[t0 + t];
       while (mref < mend && a.mask_refs[mref].j_tile < jt) ++mref;
       const bool masked = mref < mend && a.mask_refs[mref].j_tile == jt;
-      float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+      float* jfx = &s_jf[warp][0][t * kTile];
+      float* jfy = &s_jf[warp][1][t * kTile];
+      float* jfz = &s_jf[warp][2][t * kTile];
       if (active && jt > it && !masked) {
         const double4 oj = a.origin[jt];
         ia.x = pi.x - static_cast<float>(oj.x - oi.x);
@@ -292,36 +227,41 @@ __global__ void __launch_bounds__(kN3Warps * 32) k_force_n3(PairArgs a) {
         const float4* sl = &s_buf[buf][1][t * kTile];
         const float4* sg = &s_buf[buf][2][t * kTile];
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-#pragma unroll 8
-        for (int k = 0; k < kTile; ++k) {
-          const float4 p = sp[k];
-          const float4 l = sl[k];
-          const float2 g = *reinterpret_cast<const float2*>(&sg[k]);
-          const float dx = p.x - ia.x, dy = p.y - ia.y, dz = p.z - ia.z;
-          const float c = pair_coeff<kAllPairs>(p, l, g, ia, a, dx, dy, dz);
-          float ux = dx * c, uy = dy * c, uz = dz * c;
-          fx += ux;
-          fy += uy;
-          fz += uz;
+#pragma unroll 2
+        for (int k0 = 0; k0 < kTile; k0 += 4) {
+          float ux[4], uy[4], uz[4];
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            ux += __shfl_xor_sync(0xffffffffu, ux, o);
-            uy += __shfl_xor_sync(0xffffffffu, uy, o);
-            uz += __shfl_xor_sync(0xffffffffu, uz, o);
+          for (int g = 0; g < 4; ++g) {
+            const int k = k0 + g;
+            const float4 p = sp[k];
+            const float4 l = sl[k];
+            const float2 gg = *reinterpret_cast<const float2*>(&sg[k]);
+            const float dx = p.x - ia.x, dy = p.y - ia.y, dz = p.z - ia.z;
+            const float c = pair_coeff<kAllPairs>(p, l, gg, ia, a, dx, dy, dz);
+            ux[g] = dx * c;
+            uy[g] = dy * c;
+            uz[g] = dz * c;
+            fx += ux[g];
+            fy += uy[g];
+            fz += uz[g];
           }
-          if (lane == k) {
-            jx = -ux;
-            jy = -uy;
-            jz = -uz;
+          const float tx = reduce_scatter4(ux[0], ux[1], ux[2], ux[3], lane);
+          const float ty = reduce_scatter4(uy[0], uy[1], uy[2], uy[3], lane);
+          const float tz = reduce_scatter4(uz[0], uz[1], uz[2], uz[3], lane);
+          if ((lane & 7) == 0) {
+            jfx[k0 + (lane >> 3)] = -tx;
+            jfy[k0 + (lane >> 3)] = -ty;
+            jfz[k0 + (lane >> 3)] = -tz;
           }
         }
         acc0 += static_cast<double>(fx);
         acc1 += static_cast<double>(fy);
         acc2 += static_cast<double>(fz);
+      } else {
+        jfx[lane] = 0.0f;
+        jfy[lane] = 0.0f;
+        jfz[lane] = 0.0f;
       }
-      s_jf[warp][0][t * kTile + lane] = jx;
-      s_jf[warp][1][t * kTile + lane] = jy;
-      s_jf[warp][2][t * kTile + lane] = jz;
     }
     __syncthreads();  // every warp is done with `buf` and has written its j partials
     if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
@@ -351,9 +291,149 @@ __global__ void __launch_bounds__(kN3Warps * 32) k_force_n3(PairArgs a) {
   }
 }
 
+
+// ------------------------------------------------------ Born pass, Newton-3
+// Each unordered tile pair (ti <= tj) is visited once: h_ij feeds atom i
+// (lane registers) and h_ji feeds atom j (reduce-scatter across the warp,
+// then a fixed-order sum over warps in shared memory).  The distance is
+// shared by both directions.  The diagonal tile is evaluated from the i
+// side only, over all ordered pairs.
+__device__ __forceinline__ float born_pair(float r, float inv_r, float rho, float sr, bool series) {
+  return series ? descreen_series(sr * inv_r, inv_r) : descreen_closed(r, inv_r, rho, sr);
+}
+
+__global__ void __launch_bounds__(kN3Warps * 32) k_born_n3(PairArgs a) {
+  constexpr uint32_t kTileBytes = kTile * sizeof(float4);
+  constexpr int kStageAtoms = kStageTiles * kTile;
+  __shared__ __align__(128) float4 s_buf[2][2][kStageAtoms];
+  __shared__ float s_jh[kN3Warps][kStageAtoms];
+  __shared__ __align__(8) uint64_t s_bar[2];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const PairWork w = a.work[blockIdx.x];
+  const int n_stages = (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int s) {
+    const int buf = s & 1;
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    mbar_arrive_expect_tx(&s_bar[buf], static_cast<uint32_t>(cnt) * kTileBytes * 2);
+    for (int t = 0; t < cnt; ++t) {
+      const size_t base = static_cast<size_t>(a.jlist[t0 + t]) * kTile;
+      bulk_g2s(&s_buf[buf][0][t * kTile], a.pq + base, kTileBytes, &s_bar[buf]);
+      bulk_g2s(&s_buf[buf][1][t * kTile], a.gb + base, kTileBytes, &s_bar[buf]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    if (n_stages > 0) issue(0);
+    if (n_stages > 1) issue(1);
+  }
+
+  const bool active = warp < w.n_i_tiles;
+  const int it = w.i_tile0 + (active ? warp : 0);
+  const int i = it * kTile + lane;
+  const float4 pi = a.pq[i];
+  const double4 oi = a.origin[it];
+  const float rho_i = a.gb[i].z, s_i = a.gb[i].w;
+  const float c2 = a.born_c2;
+  double acc = 0.0;
+  for (int s = 0; s < n_stages; ++s) {
+    const int buf = s & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[buf], static_cast<uint32_t>((s >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
+      return;
+    }
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    for (int t = 0; t < cnt; ++t) {
+      const int jt = a.jlist[t0 + t];
+      float* jh = &s_jh[warp][t * kTile];
+      if (!active || jt < it) {
+        jh[lane] = 0.0f;
+        continue;
+      }
+      const double4 oj = a.origin[jt];
+      const float xi = pi.x - static_cast<float>(oj.x - oi.x);
+      const float yi = pi.y - static_cast<float>(oj.y - oi.y);
+      const float zi = pi.z - static_cast<float>(oj.z - oi.z);
+      const float4* sp = &s_buf[buf][0][t * kTile];
+      const float4* sg = &s_buf[buf][1][t * kTile];
+      float hi_acc = 0.0f;
+      if (jt == it) {
+#pragma unroll 4
+        for (int k = 0; k < kTile; ++k) {
+          const float4 p = sp[k];
+          const float sr = sg[k].w;
+          const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
+          const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+          const float inv_r = rsqrtf(r2);
+          const float r = r2 * inv_r;
+          const bool far = (sr * inv_r < kSeriesMaxX) && (r - sr >= rho_i);
+          const float h = born_pair(r, inv_r, rho_i, sr, __all_sync(0xffffffffu, far));
+          hi_acc += ((r2 <= c2) && (r2 >= 1e-18f)) ? h : 0.0f;
+        }
+        jh[lane] = 0.0f;
+      } else {
+#pragma unroll 2
+        for (int k0 = 0; k0 < kTile; k0 += 4) {
+          float u[4];
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            const int k = k0 + g;
+            const float4 p = sp[k];
+            const float4 gj = sg[k];  // rho~_j in z, s_j rho~_j in w
+            const float dx = p.x - xi, dy = p.y - yi, dz = p.z - zi;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float inv_r = rsqrtf(r2);
+            const float r = r2 * inv_r;
+            const bool far = (gj.w * inv_r < kSeriesMaxX) && (s_i * inv_r < kSeriesMaxX) && (r - gj.w >= rho_i) &&
+                             (r - s_i >= gj.z);
+            const bool series = __all_sync(0xffffffffu, far);
+            const bool on = (r2 <= c2) && (r2 >= 1e-18f);
+            const float hij = born_pair(r, inv_r, rho_i, gj.w, series);
+            const float hji = born_pair(r, inv_r, gj.z, s_i, series);
+            hi_acc += on ? hij : 0.0f;
+            u[g] = on ? hji : 0.0f;
+          }
+          const float tot = reduce_scatter4(u[0], u[1], u[2], u[3], lane);
+          if ((lane & 7) == 0) jh[k0 + (lane >> 3)] = tot;
+        }
+      }
+      acc += static_cast<double>(hi_acc);
+    }
+    __syncthreads();  // every warp is done with `buf` and has written its j partials
+    if (threadIdx.x == 0 && s + 2 < n_stages) issue(s + 2);
+    for (int q = threadIdx.x; q < cnt * kTile; q += blockDim.x) {
+      const int j = a.jlist[t0 + q / kTile] * kTile + (q % kTile);
+      if (!a.atom_valid[j]) continue;
+      float sum = 0.0f;
+#pragma unroll
+      for (int ww = 0; ww < kN3Warps; ++ww) sum += s_jh[ww][q];
+      if (sum != 0.0f) {
+        if (!isfinite(sum)) atomicOr(a.sys_nonfinite + a.atom_sys[j], 1);
+        add_fixed(a.born_sum + j, static_cast<double>(sum), kBornScale);
+      }
+    }
+  }
+  if (active && a.atom_valid[i]) {
+    if (!isfinite(acc)) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
+    add_fixed(a.born_sum + i, acc, kBornScale);
+  }
+}
+
 }  // namespace
 
 int force_warps_per_cta() { return kN3Warps; }
+
+void launch_born_pass(const PairArgs& a, cudaStream_t s) {
+  if (a.n_work > 0) k_born_n3<<<a.n_work, kN3Warps * 32, 0, s>>>(a);
+}
 
 void launch_force_pass(const PairArgs& a, cudaStream_t s) {
   if (a.n_work <= 0) return;

@@ -17,6 +17,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
+# Every device buffer starts as NaN in the tests, so a kernel that reads a
+# buffer before writing it fails a parity test instead of passing by luck.
+os.environ.setdefault("OG_DEBUG_POISON", "1")
 
 from origami_b200 import _ffi as F  # noqa: E402
 
