@@ -29,6 +29,14 @@ constexpr double kBornUnscale = 1.0 / 1099511627776.0;
 // Tile geometry: 32 atoms per tile (one warp lane per atom).
 constexpr int kTile = 32;
 
+// Tile-SoA layout of the FP32 per-atom arrays the pair kernels stream: tile
+// t occupies 128 consecutive floats, four 32-float columns c = 0..3, so one
+// 512-byte bulk copy moves a whole tile and a 16-byte shared-memory load
+// yields one column for four consecutive atoms.
+__host__ __device__ __forceinline__ int soa_index(int atom, int col) {
+  return ((atom >> 5) << 7) + (col << 5) + (atom & 31);
+}
+
 // Status bits of a system (og_system_stats / og_step).
 constexpr int kStatusDiverged = 1;
 constexpr int kStatusShakeFail = 2;

@@ -25,7 +25,6 @@
 #include "step_kernels.cuh"
 
 namespace ogk {
-int pair_warps_per_cta();
 int force_warps_per_cta();
 }
 
@@ -162,7 +161,7 @@ struct og_engine {
   DVec<double> born_r, born_r64, integral64, e_lj, e_coul, e_gb, e_self;
   DVec<unsigned long long> fx, fy, fz, born_sum;
   DVec<int32_t> atom_sys, local_idx, atom_valid, n_pairs;
-  DVec<float4> pq, lj, gb;
+  DVec<float> pq, lj, gb;  // tile-SoA, 4 columns per 32-atom tile
   DVec<double4> origin;
   DVec<ogk::SysState> sys_state;
   // pair work
@@ -524,7 +523,7 @@ og_status finalize_impl(og_engine* e) {
   std::vector<double> hx(np), hy(np), hz(np), hm(np, 1.0), him(np, 1.0), hq(np, 0.0), hrm(np, 0.0), hep(np, 0.0),
       hrm14(np, 0.0), hep14(np, 0.0), hrho(np, 1.0), hrt(np, 1.0), hsr(np, 0.0);
   std::vector<int32_t> hsys(np, -1), hloc(np, 0), hvalid(np, 0);
-  std::vector<float4> hlj(np, make_float4(0, 0, 0, 0));
+  std::vector<float> hlj(4 * static_cast<size_t>(np), 0.0f);  // tile-SoA: rmin, sqrt eps, rmin14, sqrt eps14
   for (int si = 0; si < n_sys; ++si) {
     const SysHost& s = e->sys[si];
     const TopoCopy& t = s.topo;
@@ -546,8 +545,10 @@ og_status finalize_impl(og_engine* e) {
       hsys[i] = si;
       hloc[i] = k;
       hvalid[i] = 1;
-      hlj[i] = make_float4(static_cast<float>(t.rmin[k]), static_cast<float>(std::sqrt(t.eps[k])),
-                           static_cast<float>(t.rmin14[k]), static_cast<float>(std::sqrt(t.eps14[k])));
+      hlj[ogk::soa_index(i, 0)] = static_cast<float>(t.rmin[k]);
+      hlj[ogk::soa_index(i, 1)] = static_cast<float>(std::sqrt(t.eps[k]));
+      hlj[ogk::soa_index(i, 2)] = static_cast<float>(t.rmin14[k]);
+      hlj[ogk::soa_index(i, 3)] = static_cast<float>(std::sqrt(t.eps14[k]));
     }
   }
   OG_CUDA(e->x.upload(hx, st)); OG_CUDA(e->y.upload(hy, st)); OG_CUDA(e->z.upload(hz, st));
@@ -564,14 +565,17 @@ og_status finalize_impl(og_engine* e) {
     OG_CUDA(v->alloc(np));
   for (auto* v : {&e->fx, &e->fy, &e->fz, &e->born_sum}) OG_CUDA(v->alloc(np));
   OG_CUDA(e->n_pairs.alloc(np));
-  OG_CUDA(e->pq.alloc(np));
-  // The Born pass reads rho~ and s*rho~ from these float4s before the first
-  // radii exist, so they start out fully defined (R = rho~ until then).
-  std::vector<float4> hgb(np, make_float4(1.0f, 1.0f, 1.0f, 0.0f));
-  for (int i = 0; i < np; ++i)
-    if (hsys[i] >= 0)
-      hgb[i] = make_float4(static_cast<float>(hrt[i]), static_cast<float>(1.0 / hrt[i]), static_cast<float>(hrt[i]),
-                           static_cast<float>(hsr[i]));
+  OG_CUDA(e->pq.alloc(4 * static_cast<size_t>(np)));
+  // The Born pass reads rho~ and s*rho~ before the first radii exist, so the
+  // gb columns start out fully defined (R = rho~ until then).
+  std::vector<float> hgb(4 * static_cast<size_t>(np));
+  for (int i = 0; i < np; ++i) {
+    const bool real = hsys[i] >= 0;
+    hgb[ogk::soa_index(i, 0)] = real ? static_cast<float>(hrt[i]) : 1.0f;
+    hgb[ogk::soa_index(i, 1)] = real ? static_cast<float>(1.0 / hrt[i]) : 1.0f;
+    hgb[ogk::soa_index(i, 2)] = real ? static_cast<float>(hrt[i]) : 1.0f;
+    hgb[ogk::soa_index(i, 3)] = real ? static_cast<float>(hsr[i]) : 0.0f;
+  }
   OG_CUDA(e->gb.upload(hgb, st));
   OG_CUDA(e->origin.alloc(e->n_tiles));
 

@@ -1,0 +1,181 @@
+// FP64 pair kernels: the near-field force tiles of the force path and the
+// energy path (Born radii and LJ / Coulomb / GB pair energies).
+#include <cmath>
+
+#include "common.cuh"
+#include "pair_kernels.cuh"
+
+namespace ogk {
+
+// ------------------------------------------------------- FP64 near field
+// One warp per near-field (i-tile, j-tile) pair -- the tiles that carry
+// exclusion / 1-4 masks, i.e. the bonded neighbourhood where the large LJ and
+// Coulomb pair forces cancel against the bonded terms.  FP64 throughout, term
+// for term as forces_nonbonded.rs:196-232 + forces_gb.rs:82-111; the j atoms
+// are warp-uniform broadcast loads.
+namespace {
+
+__global__ void __launch_bounds__(128) k_near64(PairArgs a, const int4* __restrict__ near, int n_near) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= n_near) return;
+  const int4 w = near[wid];  // i_tile, j_tile, mask offset
+  const int i = w.x * kTile + lane;
+  const uint32_t ex = a.mask_ex[w.z * kTile + lane];
+  const uint32_t m14 = a.mask_14[w.z * kTile + lane];
+  const double xi = a.x64[i], yi = a.y64[i], zi = a.z64[i], qi = a.q64[i], Ri = a.born_r64[i];
+  const double rmi = a.rmin64[i], epi = a.eps64[i], rm14i = a.rmin14_64[i], ep14i = a.eps14_64[i];
+  const double coul_kj = kCoulomb * kKcalToKj;
+  const double gb_pref = (1.0 - 1.0 / kEpsWater) * kCoulomb * kKcalToKj;
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  const int j0 = w.y * kTile;
+  for (int k = 0; k < kTile; ++k) {
+    const int j = j0 + k;
+    if (!a.atom_valid[j]) continue;
+    const double dx = a.x64[j] - xi, dy = a.y64[j] - yi, dz = a.z64[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < 1e-18) continue;
+    const double qq = qi * a.q64[j];
+    double coeff = 0.0;
+    if (!((ex >> k) & 1u) && r2 <= a.nb_c2_64) {
+      const bool is14 = (m14 >> k) & 1u;
+      const double rmin = is14 ? rm14i + a.rmin14_64[j] : rmi + a.rmin64[j];
+      const double eps = sqrt(is14 ? ep14i * a.eps14_64[j] : epi * a.eps64[j]);
+      const double inv_r2 = 1.0 / r2;
+      const double ratio2 = rmin * rmin * inv_r2;
+      const double r6 = ratio2 * ratio2 * ratio2;
+      coeff += 12.0 * eps * inv_r2 * (r6 - r6 * r6) * kKcalToKj;
+      if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 / sqrt(r2) - a.inv_rc3_64);
+    }
+    if (qq != 0.0 && r2 <= a.gb_c2_64) {
+      const double r = sqrt(r2);
+      const double rp = Ri * a.born_r64[j];
+      const double e = exp(-r2 / (4.0 * rp));
+      const double f2 = r2 + rp * e;
+      const double f = sqrt(f2);
+      coeff += gb_pref * qq / f2 * ((2.0 * r - 0.5 * r * e) / (2.0 * f)) / r;
+    }
+    ax += dx * coeff;
+    ay += dy * coeff;
+    az += dz * coeff;
+  }
+  if (a.atom_valid[i]) {
+    if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
+    add_fixed(a.fx + i, ax, kForceScale);
+    add_fixed(a.fy + i, ay, kForceScale);
+    add_fixed(a.fz + i, az, kForceScale);
+  }
+}
+
+}  // namespace
+
+void launch_near_force64(const PairArgs& a, const int4* near, int n_near, cudaStream_t s) {
+  if (n_near > 0) k_near64<<<(n_near * 32 + 127) / 128, 128, 0, s>>>(a, near, n_near);
+}
+
+// ----------------------------------------------------------------- FP64 path
+
+namespace {
+
+__device__ __forceinline__ double descreen64(double r, double rho_i, double s_rho_j) {
+  // energy/src/gb.rs:347-369, term for term.
+  if (r + s_rho_j <= rho_i) return 0.0;
+  const double l = (r - s_rho_j < rho_i) ? rho_i : r - s_rho_j;
+  const double u = r + s_rho_j;
+  if (u <= 0.0 || l <= 0.0) return 0.0;
+  const double inv_l = 1.0 / l, inv_u = 1.0 / u;
+  const double term1 = 0.5 * (inv_l - inv_u);
+  const double term2 = (r / 4.0) * (inv_u * inv_u - inv_l * inv_l);
+  const double term3 = (1.0 / (2.0 * r)) * log(l / u);
+  const double term4 = (s_rho_j * s_rho_j - r * r) / (4.0 * r) * (inv_u * inv_u - inv_l * inv_l);
+  return term1 + term2 + term3 + term4;
+}
+
+__global__ void k_born64(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded) return;
+  const int sys = a.atom_sys[i];
+  if (sys < 0) return;
+  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  const double xi = a.x[i], yi = a.y[i], zi = a.z[i], rho = a.rho_tilde[i];
+  double acc = 0.0;
+  for (int j = b; j < b + n; ++j) {
+    if (j == i) continue;
+    const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 > a.born_c2 || r2 < 1e-18) continue;
+    acc += descreen64(sqrt(r2), rho, a.srho[j]);
+  }
+  a.integral[i] = acc;
+}
+
+// Per i atom, over every j != i of its system: LJ + RF Coulomb within the
+// nonbonded cutoff with exclusions / 1-4 parameters (nonbonded.rs:127-169)
+// and the GB pair energy over all pairs (gb.rs:160-173).  Each unordered pair
+// is seen from both ends, so the host halves the sums.
+__global__ void k_energy64(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded) return;
+  const int sys = a.atom_sys[i];
+  if (sys < 0) {
+    a.e_lj[i] = a.e_coul[i] = a.e_gb[i] = a.e_self[i] = 0.0;
+    a.n_pairs[i] = 0;
+    return;
+  }
+  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  const double xi = a.x[i], yi = a.y[i], zi = a.z[i], qi = a.q[i], Ri = a.born_r[i];
+  const double pref = -0.5 * (1.0 - 1.0 / kEpsWater) * kCoulomb;
+  int ep = a.excl_row[i];
+  const int ee = a.excl_row[i + 1];
+  double lj = 0.0, coul = 0.0, gb = 0.0;
+  int pairs = 0;
+  for (int j = b; j < b + n; ++j) {
+    if (j == i) continue;
+    const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    int kind = 0;
+    while (ep < ee && a.excl_col[ep] < j) ++ep;
+    if (ep < ee && a.excl_col[ep] == j) kind = a.excl_kind[ep];
+    const double qq = qi * a.q[j];
+    if (qq != 0.0) {
+      const double rp = Ri * a.born_r[j];
+      const double fgb = sqrt(r2 + rp * exp(-r2 / (4.0 * rp)));
+      gb += 2.0 * pref * qq / fgb;
+    }
+    if (r2 > a.nb_c2 || kind == 1) continue;
+    const double r = sqrt(r2);
+    double rmin, eps;
+    if (kind == 2) {
+      rmin = a.rmin14[i] + a.rmin14[j];
+      eps = sqrt(a.eps14[i] * a.eps14[j]);
+    } else {
+      rmin = a.rmin[i] + a.rmin[j];
+      eps = sqrt(a.eps[i] * a.eps[j]);
+    }
+    const double x = rmin / r;
+    const double x2 = x * x;
+    const double r6 = x2 * x2 * x2;
+    lj += eps * (r6 * r6 - 2.0 * r6);
+    if (qq != 0.0) coul += kCoulomb * qq * (1.0 / r + a.kappa * r * r - a.crf);
+    ++pairs;
+  }
+  a.e_lj[i] = lj;
+  a.e_coul[i] = coul;
+  a.e_gb[i] = gb;
+  a.e_self[i] = (qi != 0.0) ? pref * (qi * qi) / Ri : 0.0;
+  a.n_pairs[i] = pairs;
+}
+
+}  // namespace
+
+void launch_born64(const EnergyArgs& a, cudaStream_t s) {
+  const int bs = 128;
+  k_born64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+}
+
+void launch_energy64(const EnergyArgs& a, cudaStream_t s) {
+  const int bs = 128;
+  k_energy64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+}
+
+}  // namespace ogk

@@ -26,9 +26,10 @@ struct TileMaskRef {
 
 struct PairArgs {
   // per padded atom
-  const float4* pq;   // x_rel, y_rel, z_rel (A, relative to the tile origin), charge (e)
-  const float4* lj;   // rmin_half, sqrt(eps), rmin_half_14, sqrt(eps_14)   (kcal/mol)
-  const float4* gb;   // R_born, 1/R_born, rho_tilde, s*rho_tilde
+  // FP32 per-atom data in tile-SoA layout (see soa_index in common.cuh):
+  const float* pq;    // columns x_rel, y_rel, z_rel (A, from the tile origin), charge (e)
+  const float* lj;    // columns rmin_half, sqrt(eps), rmin_half_14, sqrt(eps_14)   (kcal/mol)
+  const float* gb;    // columns R_born, 1/R_born, rho_tilde, s*rho_tilde
   const double4* origin;  // per tile
   const int32_t* atom_valid;  // 1 for real atoms
   // work

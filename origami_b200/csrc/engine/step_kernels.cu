@@ -30,12 +30,24 @@ __device__ __forceinline__ void pack_atom(const AtomArrays& a, int i) {
   const double oz = first_real ? a.z[first] : 0.0;
   if ((i & 31) == 0) a.origin[tile] = make_double4(ox, oy, oz, 0.0);
   if (a.atom_sys[i] >= 0) {
-    a.pq[i] = make_float4(static_cast<float>(a.x[i] - ox), static_cast<float>(a.y[i] - oy),
-                          static_cast<float>(a.z[i] - oz), static_cast<float>(a.q[i]));
+    a.pq[soa_index(i, 0)] = static_cast<float>(a.x[i] - ox);
+    a.pq[soa_index(i, 1)] = static_cast<float>(a.y[i] - oy);
+    a.pq[soa_index(i, 2)] = static_cast<float>(a.z[i] - oz);
+    a.pq[soa_index(i, 3)] = static_cast<float>(a.q[i]);
   } else {
     // Padding: far from everything, no charge, no LJ (params are zero).
-    a.pq[i] = make_float4(1.0e6f + 16.0f * static_cast<float>(i & 31), 1.0e6f, 1.0e6f, 0.0f);
+    a.pq[soa_index(i, 0)] = 1.0e6f + 16.0f * static_cast<float>(i & 31);
+    a.pq[soa_index(i, 1)] = 1.0e6f;
+    a.pq[soa_index(i, 2)] = 1.0e6f;
+    a.pq[soa_index(i, 3)] = 0.0f;
   }
+}
+
+__device__ __forceinline__ void store_gb(const AtomArrays& a, int i, float r, float inv_r, float rt, float srho) {
+  a.gb[soa_index(i, 0)] = r;
+  a.gb[soa_index(i, 1)] = inv_r;
+  a.gb[soa_index(i, 2)] = rt;
+  a.gb[soa_index(i, 3)] = srho;
 }
 
 __global__ void k_pack(AtomArrays a, bool zero_acc) {
@@ -57,7 +69,7 @@ __global__ void k_born_finalize(AtomArrays a, const double* integral64, double* 
   if (i >= a.n_padded) return;
   const int sys = a.atom_sys[i];
   if (sys < 0) {
-    if (write_gb) a.gb[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    if (write_gb) store_gb(a, i, 1.0f, 1.0f, 1.0f, 0.0f);
     out_r[i] = 1.0;
     return;
   }
@@ -78,8 +90,9 @@ __global__ void k_born_finalize(AtomArrays a, const double* integral64, double* 
     r = r > floor_r ? r : floor_r;
   }
   out_r[i] = r;
-  if (write_gb) a.gb[i] = make_float4(static_cast<float>(r), static_cast<float>(1.0 / r), static_cast<float>(rt),
-                                      static_cast<float>(a.srho[i]));
+  if (write_gb)
+    store_gb(a, i, static_cast<float>(r), static_cast<float>(1.0 / r), static_cast<float>(rt),
+                  static_cast<float>(a.srho[i]));
 }
 
 // ----------------------------------------------------------------- bonded

@@ -34,8 +34,8 @@ struct AtomArrays {
   const double* rho;          // intrinsic radius
   const double* rho_tilde;
   const double* srho;         // HCT scale * rho_tilde
-  float4* pq;                 // packed FP32 positions + charge
-  float4* gb;                 // R, 1/R, rho_tilde, s*rho_tilde
+  float* pq;                  // tile-SoA FP32 positions + charge
+  float* gb;                  // tile-SoA R, 1/R, rho_tilde, s*rho_tilde
   double4* origin;            // per tile
   double* born_r;             // FP64 Born radii (force path)
   SysState* sys;
