@@ -31,7 +31,8 @@ __all__ = [
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "liborigami_b200.so")
+# ORIGAMI_B200_LIB selects another build of the library (tuning sweeps).
+LIB_PATH = os.environ.get("ORIGAMI_B200_LIB") or os.path.join(_PKG, "liborigami_b200.so")
 DATA_DIR = os.path.join(_PKG, "data")
 
 BOLTZMANN_KJ_PER_MOL_K = 8.314_462_618e-3   # dynamics/src/langevin.rs:44

@@ -1,12 +1,14 @@
 """Builds origami_b200/liborigami_b200.so (host C++ + sm_100a CUDA) in-tree.
 
-    python -m origami_b200.build [--force] [--debug]
+    python -m origami_b200.build [--force] [--debug] [-D NAME=VALUE ...] [--out DIR]
 
 Every translation unit is compiled by nvcc (host .cpp files go to the host
 compiler through nvcc) with ``-gencode arch=compute_100a,code=sm_100a``; the
 CUDA runtime is linked statically so the library needs only the driver.
 Objects are cached under origami_b200/_build/ and rebuilt when a source or
-header is newer than the object.
+header is newer than the object.  ``-D`` passes tuning macros (for example
+OG_PAIR_MIN_BLOCKS) and ``--out`` writes that variant's objects and library
+to another directory, leaving the default build untouched.
 """
 from __future__ import annotations
 
@@ -58,18 +60,22 @@ def _stale(obj: str, src: str, hdr_mtime: float) -> bool:
     return m < os.path.getmtime(src) or m < hdr_mtime
 
 
-def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, debug: bool = False, verbose: bool = False, defines: list[str] | None = None,
+          out_dir: str | None = None) -> str:
+    build_dir = os.path.join(out_dir, "_build") if out_dir else BUILD
+    lib = os.path.join(out_dir, "liborigami_b200.so") if out_dir else LIB
+    os.makedirs(build_dir, exist_ok=True)
     nv = nvcc()
     hdr_mtime = max((os.path.getmtime(h) for h in headers()), default=0.0)
     opt = ["-O0", "-g", "-G"] if debug else ["-O3", "-lineinfo"]
     common = [nv, *ARCH, *host_compiler(), "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-              "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
+              "-I", os.path.join(ROOT, "include"), "--expt-relaxed-constexpr",
+              *[f"-D{d}" for d in (defines or [])]]
     jobs = []
     objs = []
     for src in sources():
         rel = os.path.relpath(src, CSRC).replace(os.sep, "_")
-        obj = os.path.join(BUILD, rel + ".o")
+        obj = os.path.join(build_dir, rel + ".o")
         objs.append(obj)
         if force or _stale(obj, src, hdr_mtime):
             extra = PER_FILE_FLAGS.get(os.path.basename(src), [])
@@ -85,14 +91,18 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
                 sys.stderr.write(" ".join(cmd) + "\n" + out)
             if rc != 0:
                 raise RuntimeError(f"compile failed: {cmd[-3]}")
-    if force or jobs or not os.path.exists(LIB):
-        link = [nv, *ARCH, *host_compiler(), "-shared", "-o", LIB, *objs, "-ldl", "-lpthread"]
+    if force or jobs or not os.path.exists(lib):
+        link = [nv, *ARCH, *host_compiler(), "-shared", "-o", lib, *objs, "-ldl", "-lpthread"]
         rc, out, _ = run(link)
         if verbose or rc != 0:
             sys.stderr.write(" ".join(link) + "\n" + out)
         if rc != 0:
             raise RuntimeError("link failed")
-    return LIB
+    if out_dir:  # a variant library finds the data tables next to itself
+        data = os.path.join(out_dir, "data")
+        if not os.path.exists(data):
+            os.symlink(os.path.join(PKG, "data"), data)
+    return lib
 
 
 def main() -> int:
@@ -100,8 +110,10 @@ def main() -> int:
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--debug", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
+    ap.add_argument("-D", dest="defines", action="append", default=[], help="NAME=VALUE tuning macro")
+    ap.add_argument("--out", default=None, help="directory for a variant build")
     args = ap.parse_args()
-    print(build(force=args.force, debug=args.debug, verbose=args.verbose))
+    print(build(force=args.force, debug=args.debug, verbose=args.verbose, defines=args.defines, out_dir=args.out))
     return 0
 
 
