@@ -256,6 +256,28 @@ typedef struct og_kernel_time { const char* name; double ms; int64_t launches; }
 og_status og_profile_enable(og_engine* e, int32_t on);
 og_status og_profile_read(og_engine* e, og_kernel_time* out, int32_t cap, int32_t* n_out);
 
+/* GB solvation energy of one system with no device allocation.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need the energy: a host whose GPU memory is reserved up front by
+ * another framework's caching allocator, or a latency-critical loop that
+ * forbids allocation (and the device synchronisation it implies) after
+ * start-up.  Computes what gb_energy returns (Born radii with descreening
+ * pairs within born_cutoff, self term, pair sum over ALL pairs; FP64) into
+ * energy_out[0..2] = {gb, self, pair} in kJ/mol.  Every pointer is a device
+ * pointer the caller owns: xyz (3 * n_atoms, interleaved), charge, gb_rho,
+ * gb_scale (n_atoms each), energy_out (3); work is queued on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and the call does not wait.
+ * Scratch is a fixed device array inside the library, sized for at most
+ * OG_NOALLOC_MAX_ATOMS atoms (~129 KiB held on every GPU that loads the
+ * library until exit); larger systems are rejected with OG_E_BADARG.  The
+ * first call on a device looks up that array's address (do it before any
+ * stream capture).  All calls share the array, so calls that overlap on the
+ * GPU race: order them. */
+#define OG_NOALLOC_MAX_ATOMS 16384
+og_status og_gb_energy_noalloc(const double* xyz, const double* charge, const double* gb_rho,
+                               const double* gb_scale, int32_t n_atoms, double born_cutoff,
+                               double* energy_out, void* stream);
+
 /* Measured FP32 FMA throughput of the current device (TFLOP/s, FMA = 2 flops)
  * from a register-resident FMA chain on every SM: the denominator of the
  * pair kernels' FP32-pipe roofline.  No counterpart in the reference. */

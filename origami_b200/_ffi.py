@@ -101,6 +101,8 @@ SIGNATURES = [
     ("og_profile_enable", C.c_int, [C.c_void_p, C.c_int32]),
     ("og_profile_read", C.c_int, [C.c_void_p, C.POINTER(og_kernel_time), C.c_int32, c_int32_p]),
     ("og_measure_fp32_peak", C.c_int, [c_double_p]),
+    ("og_gb_energy_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double,
+                                       C.c_void_p, C.c_void_p]),
 ]
 
 
