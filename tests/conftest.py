@@ -45,8 +45,8 @@ _oracle = None
 def oracle() -> C.CDLL:
     global _oracle
     if _oracle is None:
-        src = os.path.join(ROOT, "oracle", "oracle.cpp")
-        if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+        srcs = [os.path.join(ROOT, "oracle", s) for s in ("oracle.cpp", "powersasa.cpp")]
+        if not os.path.exists(ORACLE_SO) or any(os.path.getmtime(ORACLE_SO) < os.path.getmtime(s) for s in srcs):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
         o = C.CDLL(ORACLE_SO)
         dp, ip = F.c_double_p, F.c_int32_p
@@ -76,6 +76,16 @@ def oracle() -> C.CDLL:
         o.orc_baoab.restype = C.c_int
         o.orc_shake.argtypes = [dp, dp, dp, C.c_int, ip, dp, C.c_double, C.c_int]
         o.orc_shake.restype = C.c_int
+        o.orc_sasa_radius.argtypes = [C.c_int]
+        o.orc_sasa_radius.restype = C.c_double
+        o.orc_sasa_gamma.argtypes = [C.c_int, C.c_double]
+        o.orc_sasa_gamma.restype = C.c_double
+        o.orc_sasa_areas.argtypes = [C.c_int, dp, dp, dp]
+        o.orc_sasa_areas.restype = None
+        o.orc_sasa_forces.argtypes = [C.c_int, dp, dp, dp, dp]
+        o.orc_sasa_forces.restype = None
+        o.orc_shrake_rupley_areas.argtypes = [C.c_int, dp, dp, C.c_int, dp]
+        o.orc_shrake_rupley_areas.restype = None
         _oracle = o
     return _oracle
 

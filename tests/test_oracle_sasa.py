@@ -1,0 +1,176 @@
+"""Pins the PowerSasa / Shrake-Rupley oracle (oracle/powersasa.cpp) to the
+reference's own test cases, all on the CPU:
+
+* isolated carbon = 4 pi (1.7 + 1.4)^2 (crates/energy/src/powersasa/mod.rs:120-137)
+* one cap: A = 2 pi R^2 (1 + cos alpha) (powersasa/area.rs:418-429)
+* analytical gradient vs central differences: two atoms, 1e-3
+  (powersasa/analytical.rs:999-1061); Ala3, 1e-2 per affected atom
+  (analytical.rs:888-997); Ala-Val total energy, 0.5 (analytical.rs:822-868)
+* PowerSasa within 2 % of Shrake-Rupley (4096 dots) on one Ala and on the
+  extended Trp-cage (powersasa/mod.rs:161-172, 459-474)
+* Shrake-Rupley: isolated atom, far-apart atoms, extended 20-mer range
+  (crates/energy/src/sasa.rs:205-277)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import dp, oracle
+
+TRP = "NLYIQWLKDGGPSSGRPPPS"
+
+
+def radii_gamma(chain, scale=1.0):
+    o = oracle()
+    el = np.array(chain.topology().element)
+    r = np.array([o.orc_sasa_radius(int(e)) for e in el])
+    g = np.array([o.orc_sasa_gamma(int(e), scale) for e in el])
+    return r, g
+
+
+def areas(x, r):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    a = np.zeros(x.shape[0])
+    oracle().orc_sasa_areas(x.shape[0], dp(x), dp(np.ascontiguousarray(r)), dp(a))
+    return a
+
+
+def sr_areas(x, r, n_dots):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    a = np.zeros(x.shape[0])
+    oracle().orc_shrake_rupley_areas(x.shape[0], dp(x), dp(np.ascontiguousarray(r)), n_dots, dp(a))
+    return a
+
+
+def sasa_forces(x, r, g):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    f = np.zeros_like(x)
+    oracle().orc_sasa_forces(x.shape[0], dp(x), dp(np.ascontiguousarray(r)), dp(np.ascontiguousarray(g)), dp(f))
+    return f
+
+
+def area_gradient(x, r, i):
+    """dA_i/dr_x for every atom x, from the force routine with gamma one-hot at i."""
+    g = np.zeros(x.shape[0])
+    g[i] = 1.0
+    return -sasa_forces(x, r, g)
+
+
+def test_isolated_carbon_full_sphere():
+    a = areas(np.zeros((1, 3)), np.array([1.7 + 1.4]))
+    assert abs(a[0] - 4 * math.pi * 3.1**2) < 1e-6
+
+
+def test_single_cap_closed_form():
+    R, d = 3.1, 2.5
+    a = areas(np.array([[0.0, 0, 0], [d, 0, 0]]), np.array([R, R]))
+    cos_a = d / (2 * R)
+    np.testing.assert_allclose(a, 2 * math.pi * R * R * (1 + cos_a), rtol=1e-12)
+
+
+def test_gradient_two_atoms_matches_central_difference():
+    x = np.array([[0.0, 0, 0], [3.0, 0, 0]])
+    r = np.array([3.0, 3.0])
+    grad = area_gradient(x, r, 0)
+    eps = 1e-5
+    for k in range(2):
+        for ax in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[k, ax] += eps
+            xm[k, ax] -= eps
+            num = (areas(xp, r)[0] - areas(xm, r)[0]) / (2 * eps)
+            assert abs(grad[k, ax] - num) < 1e-3, (k, ax, grad[k, ax], num)
+
+
+def test_gradient_ala3_matches_central_difference(origami):
+    chain = origami.Chain.build("AAA")
+    x = chain.positions
+    r, _ = radii_gamma(chain)
+    n = x.shape[0]
+    eps = 1e-5
+    checked = 0
+    for i in range(min(n, 12)):
+        grad = area_gradient(x, r, i)
+        d = np.linalg.norm(x - x[i], axis=1)
+        affected = [i] + [j for j in range(n) if j != i and d[j] < r[i] + r[j]]
+        for k in affected:
+            for ax in range(3):
+                xp, xm = x.copy(), x.copy()
+                xp[k, ax] += eps
+                xm[k, ax] -= eps
+                num = (areas(xp, r)[i] - areas(xm, r)[i]) / (2 * eps)
+                assert abs(grad[k, ax] - num) < 1e-2, (i, k, ax, grad[k, ax], num)
+                checked += 1
+    assert checked > 100
+
+
+def test_forces_ala_val_match_total_energy_difference(origami):
+    chain = origami.Chain.build("AV")
+    x = chain.positions
+    r, g = radii_gamma(chain)
+    f = sasa_forces(x, r, g)
+    eps = 1e-4
+    for k in range(8):
+        for ax in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[k, ax] += eps
+            xm[k, ax] -= eps
+            num = -((g * areas(xp, r)).sum() - (g * areas(xm, r)).sum()) / (2 * eps)
+            assert abs(f[k, ax] - num) < 0.5
+
+
+def test_gradient_helix_trp_cage_mostly_smooth(origami):
+    """On the helical Trp-cage most sampled coordinates agree with central
+    differences to 1e-6; the rest are atoms whose area the reference clamps
+    at zero or whose component count is not smooth, where the analytical
+    gradient (like the reference's) is the Gauss-Bonnet formula's."""
+    chain = origami.Chain.build(TRP, math.radians(-57), math.radians(-47), math.pi)
+    x = chain.positions
+    r, g = radii_gamma(chain)
+    f = sasa_forces(x, r, g)
+    rng = np.random.default_rng(0)
+    good = total = 0
+    h = 1e-5
+    for k in rng.choice(x.shape[0], 12, replace=False):
+        for ax in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[k, ax] += h
+            xm[k, ax] -= h
+            num = -((g * areas(xp, r)).sum() - (g * areas(xm, r)).sum()) / (2 * h)
+            total += 1
+            good += abs(f[k, ax] - num) < 1e-6
+    assert good >= 0.75 * total, (good, total)
+
+
+def test_powersasa_matches_shrake_rupley(origami):
+    for seq in ("A", TRP):
+        chain = origami.Chain.build(seq)
+        x = chain.positions
+        r, _ = radii_gamma(chain)
+        ps = areas(x, r).sum()
+        sr = sr_areas(x, r, 4096).sum()
+        assert abs(ps - sr) / sr < 0.02, (seq, ps, sr)
+
+
+def test_shrake_rupley_reference_cases(origami):
+    single = 4 * math.pi * 3.1**2
+    a = sr_areas(np.zeros((1, 3)), np.array([3.1]), 960)
+    assert abs(a[0] - single) < 1e-9
+    a = sr_areas(np.array([[0.0, 0, 0], [50.0, 0, 0]]), np.array([3.1, 3.1]), 960)
+    assert abs(a.sum() - 2 * single) <= 0.005 * 2 * single
+    chain = origami.Chain.build("ARNDCQEGHILKMFPSTWYV")
+    r, g = radii_gamma(chain)
+    a = sr_areas(chain.positions, r, 960)
+    assert 1500.0 < a.sum() < 10000.0
+    assert (g * a).sum() > 0.0
+
+
+def test_gamma_is_carbon_and_sulfur_only():
+    o = oracle()
+    assert o.orc_sasa_gamma(1, 1.0) == pytest.approx(0.005 * 4.184)
+    assert o.orc_sasa_gamma(5, 0.25) == pytest.approx(0.25 * 0.005 * 4.184)
+    for e in (0, 2, 3, 4):
+        assert o.orc_sasa_gamma(e, 1.0) == 0.0
