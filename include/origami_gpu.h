@@ -158,8 +158,13 @@ typedef struct og_params {
   int32_t constrain_h_bonds;  /* SHAKE X-H bonds, tol 1e-6 A^2, 64 iterations */
   int32_t shake_max_iters;    /* 0 -> 64 */
   double shake_tol_sq;        /* 0 -> 1e-6 */
-  /* Analytical PowerSasa hydrophobic force (analytical.rs:451); gamma scale as
-   * ORIGAMI_SASA_GAMMA_SCALE. */
+  /* Analytical PowerSasa hydrophobic term: forces as
+   * add_sasa_forces_analytical_with_scratch (powersasa/analytical.rs:451),
+   * energy sum gamma_i A_i as powersasa_energy (powersasa/mod.rs:55).  gamma =
+   * 0.005 kcal/mol/A^2 on C and S times sasa_gamma_scale (the reference's
+   * ORIGAMI_SASA_GAMMA_SCALE, analytical.rs:607), applied to the energy as
+   * well as the force so the two stay consistent (the reference scales the
+   * force only). */
   int32_t include_sasa;
   double sasa_gamma_scale;
   /* Born radii: 0 = plain OBC-II descreening pass, 1 = learned radii. */
@@ -175,7 +180,7 @@ typedef struct og_energies {
   double bond, angle, dihedral, improper;  /* bonded.rs BondedBreakdown */
   double lj, coulomb;                      /* nonbonded.rs NonbondedBreakdown */
   double gb, gb_self, gb_pair;             /* gb.rs GbBreakdown */
-  double sasa;
+  double sasa;                             /* sum gamma_i A_i (include_sasa) */
   double total;
   int32_t born_clamped;                    /* gb.rs GbBreakdown::clamped_count */
   int32_t nb_pairs;                        /* pairs inside the LJ/Coulomb cutoff */
@@ -247,8 +252,18 @@ og_status og_kinetic(og_engine* e, int32_t sys, double* ke_kj_mol, double* tempe
  * a = parity, parity+2, ... of the temperature-sorted systems, Metropolis on
  * delta = (beta_a - beta_b)(E_a - E_b) with uniforms u[pair]; on acceptance
  * positions, velocities and forces are exchanged and velocities rescaled by
- * sqrt(T_a/T_b).  accepted[pair] (optional) receives 0/1. */
+ * sqrt(T_a/T_b).  accepted[pair] (optional) receives 0/1.  With include_sasa
+ * the surface term of E is the 960-point Shrake-Rupley energy with the
+ * unscaled tension, as remd.rs:529-537 potential_energy uses. */
 og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int32_t* accepted);
+
+/* Per-atom solvent-accessible area (A^2, radius vdW + 1.4 A) of system `sys`
+ * at its current positions; area_out receives n_atoms doubles.
+ * method 0: analytical PowerSasa (powersasa/mod.rs:55 powersasa_energy's
+ * per_atom_area); method 1: Shrake-Rupley with n_dots Fibonacci points
+ * (sasa.rs:65 sasa_per_atom_with_dots; n_dots <= 0 means the reference's
+ * 960).  FP64 on the device; works whether or not include_sasa is set. */
+og_status og_compute_sasa(og_engine* e, int32_t sys, int32_t method, int32_t n_dots, double* area_out);
 
 /* CUDA-event timing of the kernels the last og_step launched: fills up to
  * `cap` entries of (kernel id, milliseconds) summed over the call. */

@@ -634,6 +634,42 @@ void orc_sasa_areas(int n, const double* xyz, const double* radii, double* area)
   }
 }
 
+// Directional derivatives of single Gauss-Bonnet terms (the pieces
+// directional_area_derivative sums, analytical.rs:337-421), one tangent per
+// (role, axis).  p holds the centres of (i, k, l, m) or (i, k, l), r their
+// radii; g receives 12 or 9 values, role-major.  The roles' atoms are taken
+// distinct.
+void orc_arc_term_jvps(const double* p, const double* r, int ss, int se, double theta, int vertexed, double* g) {
+  const V3 pi = P(p, 0), pk = P(p, 1), pl = P(p, 2), pm = P(p, 3);
+  for (int role = 0; role < 4; ++role) {
+    for (int axis = 0; axis < 3; ++axis) {
+      V3 t[4] = {};
+      (axis == 0 ? t[role].x : axis == 1 ? t[role].y : t[role].z) = 1.0;
+      const double dcos = cos_alpha_directional(pi, pk, r[0], r[1], t[0], t[1]);
+      double term = theta * dcos;
+      if (vertexed) {
+        double dth = 0.0;
+        if (!arc_theta_jvp(pi, pk, pl, pm, r[0], r[1], r[2], r[3], ss, se, t[0], t[1], t[2], t[3], &dth)) dth = 0.0;
+        term += cap_cos(pi, pk, r[0], r[1]) * dth;
+      }
+      g[3 * role + axis] = term;
+    }
+  }
+}
+
+void orc_vertex_term_jvps(const double* p, const double* r, int sign, double* g) {
+  const V3 pi = P(p, 0), pk = P(p, 1), pl = P(p, 2);
+  for (int role = 0; role < 3; ++role) {
+    for (int axis = 0; axis < 3; ++axis) {
+      V3 t[3] = {};
+      (axis == 0 ? t[role].x : axis == 1 ? t[role].y : t[role].z) = 1.0;
+      double de = 0.0;
+      if (!vertex_epsilon_jvp(pi, pk, pl, r[0], r[1], r[2], sign, t[0], t[1], t[2], &de)) de = 0.0;
+      g[3 * role + axis] = de;
+    }
+  }
+}
+
 // Shrake-Rupley per-atom area (A^2) with n_dots Fibonacci test points per
 // atom (crates/energy/src/sasa.rs:65-110, points :182-197): a point is
 // buried when strictly inside another expanded sphere.

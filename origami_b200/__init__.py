@@ -378,6 +378,17 @@ class Engine:
         _check(lib().og_get_born_integrals(self._h, sys, _dptr(r)))
         return r
 
+    def sasa_areas(self, sys: int = 0, method: str = "powersasa", n_dots: int = 960) -> np.ndarray:
+        """Per-atom accessible area (A^2): "powersasa" (analytical, as
+        powersasa_energy) or "shrake_rupley" with n_dots test points (as
+        sasa_per_atom_with_dots)."""
+        codes = {"powersasa": 0, "shrake_rupley": 1}
+        if method not in codes:
+            raise ValueError(f"unknown SASA method {method!r}")
+        r = np.empty(self._n_atoms[sys])
+        _check(lib().og_compute_sasa(self._h, sys, codes[method], n_dots, _dptr(r)))
+        return r
+
     def energies(self, sys: int = 0) -> dict:
         e = F.og_energies()
         _check(lib().og_compute_energies(self._h, sys, C.byref(e)))

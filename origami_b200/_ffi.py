@@ -98,6 +98,7 @@ SIGNATURES = [
     ("og_system_stats", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64), c_int32_p]),
     ("og_kinetic", C.c_int, [C.c_void_p, C.c_int32, c_double_p, c_double_p]),
     ("og_remd_swap", C.c_int, [C.c_void_p, C.c_int32, c_double_p, c_int32_p]),
+    ("og_compute_sasa", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, c_double_p]),
     ("og_profile_enable", C.c_int, [C.c_void_p, C.c_int32]),
     ("og_profile_read", C.c_int, [C.c_void_p, C.POINTER(og_kernel_time), C.c_int32, c_int32_p]),
     ("og_measure_fp32_peak", C.c_int, [c_double_p]),

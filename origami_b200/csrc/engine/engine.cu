@@ -22,6 +22,7 @@
 #include "../host/status.h"
 #include "common.cuh"
 #include "pair_kernels.cuh"
+#include "sasa.cuh"
 #include "step_kernels.cuh"
 
 namespace ogk {
@@ -190,6 +191,15 @@ struct og_engine {
   DVec<int32_t> seg_begin, seg_end;  // [atoms per sys | bonds | angles | dihedrals | impropers], 5*n_sys
   DVec<double> seg_out;
   DVec<int32_t> clamp_count, error_flag, sys_nonfinite;
+  // SASA: per padded atom radius (vdW + probe) and surface tension, the
+  // atoms with non-zero tension (force / energy tasks) and all real atoms
+  // (area queries), per-system tile ranges, component probes, test points.
+  DVec<double> sasa_r, sasa_gamma, sasa_area, sasa_energy, sasa_probes, sr_dots;
+  DVec<int32_t> sasa_tasks, sasa_all, probe_begin;
+  DVec<int16_t> probe_adj;
+  DVec<int2> sys_tiles;
+  int n_sasa_tasks = 0, n_sasa_all = 0, n_sr_dots = 0;
+  double sasa_rmax = 0.0;
   // graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -269,6 +279,27 @@ struct og_engine {
     a.energy = bonded_e.p;
     a.atom_sys = atom_sys.p;
     a.sys_nonfinite = sys_nonfinite.p;
+    return a;
+  }
+
+  ogk::SasaArgs sasa_args(bool all_atoms) {
+    ogk::SasaArgs a{};
+    a.x = x.p; a.y = y.p; a.z = z.p;
+    a.radius = sasa_r.p;
+    a.gamma = sasa_gamma.p;
+    a.tasks = all_atoms ? sasa_all.p : sasa_tasks.p;
+    a.n_tasks = all_atoms ? n_sasa_all : n_sasa_tasks;
+    a.atom_sys = atom_sys.p;
+    a.sys_tiles = sys_tiles.p;
+    a.origin = origin.p;
+    a.r_max = sasa_rmax;
+    a.fx = fx.p; a.fy = fy.p; a.fz = fz.p;
+    a.area = sasa_area.p;
+    a.energy = sasa_energy.p;
+    a.probes = sasa_probes.p;
+    a.probe_adj_begin = probe_begin.p;
+    a.probe_adj = probe_adj.p;
+    a.sys = sys_state.p;
     return a;
   }
 
@@ -353,6 +384,10 @@ struct og_engine {
       Timer t(this, "bonded");
       ogk::launch_bonded_forces(bonded_args(), stream);
     }
+    if (p.include_sasa) {
+      Timer t(this, "sasa");
+      ogk::launch_sasa_forces(sasa_args(false), stream);
+    }
   }
 
   void enqueue_step() {
@@ -414,7 +449,40 @@ og_status read_status(og_engine* e, std::vector<ogk::SysState>* out) {
   OG_CUDA(cudaMemcpyAsync(&err_flag, e->error_flag.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
   OG_CUDA(cudaStreamSynchronize(e->stream));
   if (err_flag & ogk::kStatusTimeout) return og_fail(OG_E_TIMEOUT, "a pair-kernel pipeline wait timed out");
+  for (const auto& s : *out)
+    if (s.status & ogk::kStatusSasaOverflow)
+      return og_fail(OG_E_UNSUPPORTED, "an atom's SASA arrangement exceeds the kernel's capacity (caps, "
+                                       "transitions per cap or arcs); its surface term was not evaluated");
   return OG_OK;
+}
+
+// Fibonacci test points of the Shrake-Rupley sampler (sasa.rs:182-197).
+std::vector<double> sr_dot_table(int n) {
+  std::vector<double> d(3 * static_cast<size_t>(n));
+  const double phi = M_PI * (std::sqrt(3.0) + 1.0);
+  for (int k = 0; k < n; ++k) {
+    const double yy = 1.0 - 2.0 * k / (n - 1.0);
+    const double rr = std::sqrt(1.0 - yy * yy);
+    d[3 * k] = std::cos(phi * k) * rr;
+    d[3 * k + 1] = yy;
+    d[3 * k + 2] = std::sin(phi * k) * rr;
+  }
+  return d;
+}
+
+// Per-atom areas of every real atom into e->sasa_area (method 0 PowerSasa,
+// 1 Shrake-Rupley with `dots`), from the current positions.
+og_status sasa_areas_all(og_engine* e, int method, const double* dots, int n_dots) {
+  cudaStream_t st = e->stream;
+  OG_CUDA(cudaMemsetAsync(e->sasa_area.p, 0, sizeof(double) * e->n_padded, st));
+  OG_CUDA(cudaMemsetAsync(e->sasa_energy.p, 0, sizeof(double) * e->n_padded, st));
+  ogk::launch_pack(e->atoms(), false, st);
+  if (method == 0) ogk::launch_sasa_areas(e->sasa_args(true), st);
+  else ogk::launch_shrake_rupley(e->sasa_args(true), dots, n_dots, st);
+  og_status s = launch_check("SASA area kernel");
+  if (s != OG_OK) return s;
+  std::vector<ogk::SysState> hs;
+  return read_status(e, &hs);
 }
 
 // xoshiro256++ / SplitMix64 / Box-Muller exactly as dynamics/src/rng.rs.
@@ -578,6 +646,74 @@ og_status finalize_impl(og_engine* e) {
   }
   OG_CUDA(e->gb.upload(hgb, st));
   OG_CUDA(e->origin.alloc(e->n_tiles));
+
+  // ---- SASA tables: radius = Bondi vdW + 1.4 A probe, surface tension
+  // 0.005 kcal/mol/A^2 on C and S (powersasa/mod.rs:27-52), times
+  // sasa_gamma_scale (analytical.rs:607-614).
+  {
+    static const double kVdw[6] = {1.20, 1.70, 1.55, 1.52, 1.80, 1.80};
+    const double g_cs = 0.005 * ogk::kKcalToKj * e->p.sasa_gamma_scale;
+    std::vector<double> hr(np, 0.0), hg(np, 0.0);
+    std::vector<int32_t> htask, hall;
+    std::vector<int2> hst(n_sys);
+    double rmax = 0.0;
+    for (int si = 0; si < n_sys; ++si) {
+      const SysHost& s = e->sys[si];
+      hst[si] = make_int2(s.tile_begin, s.n_tiles);
+      for (int k = 0; k < s.topo.n; ++k) {
+        const int el = s.topo.element[k];
+        if (el < 0 || el > 5) return og_fail(OG_E_BADARG, "element code out of range");
+        const int i = s.atom_begin + k;
+        hr[i] = kVdw[el] + 1.4;
+        hg[i] = (el == 1 || el == 5) ? g_cs : 0.0;
+        rmax = std::max(rmax, hr[i]);
+        hall.push_back(i);
+        if (hg[i] != 0.0) htask.push_back(i);
+      }
+    }
+    e->sasa_rmax = rmax;
+    e->n_sasa_tasks = static_cast<int>(htask.size());
+    e->n_sasa_all = static_cast<int>(hall.size());
+    OG_CUDA(e->sasa_r.upload(hr, st));
+    OG_CUDA(e->sasa_gamma.upload(hg, st));
+    OG_CUDA(e->sasa_tasks.upload(htask, st));
+    OG_CUDA(e->sasa_all.upload(hall, st));
+    OG_CUDA(e->sys_tiles.upload(hst, st));
+    OG_CUDA(e->sasa_area.alloc(np));
+    OG_CUDA(e->sasa_energy.alloc(np));
+    // Component probes: Fibonacci points, golden angle pi (3 - sqrt 5),
+    // joined when their dot product exceeds cos(2.5 sqrt(4 pi / N))
+    // (arrangement.rs:327-391).
+    const int np_ = ogk::kSasaProbes;
+    std::vector<double> hp(3 * np_);
+    const double golden = M_PI * (3.0 - std::sqrt(5.0));
+    for (int k = 0; k < np_; ++k) {
+      const double zz = 1.0 - (2.0 * k + 1.0) / np_;
+      const double rr = std::sqrt(std::max(1.0 - zz * zz, 0.0));
+      const double th = golden * k;
+      hp[3 * k] = rr * std::cos(th);
+      hp[3 * k + 1] = rr * std::sin(th);
+      hp[3 * k + 2] = zz;
+    }
+    const double cos_thresh = std::cos(std::min(2.5 * std::sqrt(4.0 * M_PI / np_), M_PI));
+    std::vector<int32_t> hpb(1, 0);
+    std::vector<int16_t> hadj;
+    for (int a = 0; a < np_; ++a) {
+      for (int b = 0; b < np_; ++b) {
+        if (a == b) continue;
+        const double d = hp[3 * a] * hp[3 * b] + hp[3 * a + 1] * hp[3 * b + 1] + hp[3 * a + 2] * hp[3 * b + 2];
+        if (d > cos_thresh) hadj.push_back(static_cast<int16_t>(b));
+      }
+      hpb.push_back(static_cast<int32_t>(hadj.size()));
+    }
+    OG_CUDA(e->sasa_probes.upload(hp, st));
+    OG_CUDA(e->probe_begin.upload(hpb, st));
+    OG_CUDA(e->probe_adj.upload(hadj, st));
+    // Shrake-Rupley test points, the reference's 960 (sasa.rs:26).
+    e->n_sr_dots = 960;
+    OG_CUDA(e->sr_dots.upload(sr_dot_table(e->n_sr_dots), st));
+    OG_CUDA(ogk::sasa_prepare());
+  }
 
   // ---- per-system state
   std::vector<ogk::SysState> hs(n_sys);
@@ -868,7 +1004,6 @@ og_status og_engine_create(const og_params* params, og_engine** out) {
   if (!params || !out) return og_fail(OG_E_BADARG, "null argument");
   *out = nullptr;
   if (!(params->dt_fs > 0.0)) return og_fail(OG_E_BADARG, "dt_fs must be positive");
-  if (params->include_sasa) return og_fail(OG_E_UNSUPPORTED, "SASA forces are not built into this engine");
   if (params->born_mode != 0) return og_fail(OG_E_UNSUPPORTED, "learned Born radii are not built into this engine");
   int n_dev = 0;
   if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
@@ -1025,6 +1160,10 @@ og_status og_compute_forces(og_engine* e, int32_t s, double* f_out) {
   if (f_out && (s < 0 || s >= static_cast<int32_t>(e->sys.size())))
     return og_fail(OG_E_BADARG, "system index out of range");
   if ((st = eval_forces(e)) != OG_OK) return st;
+  if (e->p.include_sasa) {
+    std::vector<ogk::SysState> hs;
+    if ((st = read_status(e, &hs)) != OG_OK) return st;
+  }
   if (f_out) {
     const int n = e->sys[s].topo.n;
     std::vector<unsigned long long> h[3];
@@ -1104,12 +1243,19 @@ og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
   ogk::launch_born_finalize(e->atoms(), e->integral64.p, e->born_r64.p, false, e->clamp_count.p, stream);
   ogk::launch_energy64(a, stream);
   ogk::launch_bonded_energies(e->bonded_args(), stream);
+  if (e->p.include_sasa) {
+    OG_CUDA(cudaMemsetAsync(e->sasa_area.p, 0, sizeof(double) * e->n_padded, stream));
+    OG_CUDA(cudaMemsetAsync(e->sasa_energy.p, 0, sizeof(double) * e->n_padded, stream));
+    ogk::launch_pack(e->atoms(), false, stream);
+    ogk::launch_sasa_areas(e->sasa_args(false), stream);
+  }
   if ((st = launch_check("energy kernels")) != OG_OK) return st;
 
   // Deterministic per-system sums.
   std::vector<double> sums[5];
-  const double* per_atom[4] = {e->e_lj.p, e->e_coul.p, e->e_gb.p, e->e_self.p};
-  for (int k = 0; k < 4; ++k) {
+  const double* per_atom[5] = {e->e_lj.p, e->e_coul.p, e->e_gb.p, e->e_self.p, e->sasa_energy.p};
+  const int n_terms = e->p.include_sasa ? 5 : 4;
+  for (int k = 0; k < n_terms; ++k) {
     ogk::launch_segment_sum(per_atom[k], e->seg_begin.p, e->seg_end.p, n_sys, e->seg_out.p + 0, stream);
     sums[k].resize(n_sys);
     OG_CUDA(cudaMemcpyAsync(sums[k].data(), e->seg_out.p, sizeof(double) * n_sys, cudaMemcpyDeviceToHost, stream));
@@ -1127,6 +1273,10 @@ og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
                           stream));
   OG_CUDA(cudaStreamSynchronize(stream));
   if ((st = launch_check("energy reductions")) != OG_OK) return st;
+  if (e->p.include_sasa) {
+    std::vector<ogk::SysState> hs;
+    if ((st = read_status(e, &hs)) != OG_OK) return st;
+  }
 
   for (int k = 0; k < n_sys; ++k) {
     if (s >= 0 && k != s) continue;
@@ -1141,7 +1291,7 @@ og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
     o.gb_pair = 0.5 * sums[2][k] * ogk::kKcalToKj;
     o.gb_self = sums[3][k] * ogk::kKcalToKj;
     o.gb = o.gb_self + o.gb_pair;
-    o.sasa = 0.0;
+    o.sasa = e->p.include_sasa ? sums[4][k] : 0.0;
     o.total = o.bond + o.angle + o.dihedral + o.improper + o.lj + o.coulomb + o.gb + o.sasa;
     o.born_clamped = clamp[k];
     long long np = 0;
@@ -1206,6 +1356,25 @@ og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int
                    [&](int a, int b) { return e->sys[a].temperature < e->sys[b].temperature; });
   std::vector<og_energies> en(n_sys);
   if ((st = og_compute_energies(e, -1, en.data())) != OG_OK) return st;
+  if (e->p.include_sasa) {
+    // remd.rs:529-537: the swap energy's surface term is the Shrake-Rupley
+    // energy (960 points, unscaled tension on C and S), summed in atom order.
+    if ((st = sasa_areas_all(e, 1, e->sr_dots.p, e->n_sr_dots)) != OG_OK) return st;
+    std::vector<double> area(e->n_padded);
+    OG_CUDA(cudaMemcpyAsync(area.data(), e->sasa_area.p, sizeof(double) * e->n_padded, cudaMemcpyDeviceToHost,
+                            e->stream));
+    OG_CUDA(cudaStreamSynchronize(e->stream));
+    const double g = 0.005 * ogk::kKcalToKj;
+    for (int k = 0; k < n_sys; ++k) {
+      const SysHost& sh = e->sys[k];
+      double esr = 0.0;
+      for (int a = 0; a < sh.topo.n; ++a) {
+        const int el = sh.topo.element[a];
+        if (el == 1 || el == 5) esr += g * area[sh.atom_begin + a];
+      }
+      en[k].total += esr - en[k].sasa;
+    }
+  }
   std::vector<ogk::SysState> hs;
   if ((st = read_status(e, &hs)) != OG_OK) return st;
   const int n_pairs = n_sys - 1;
@@ -1226,6 +1395,26 @@ og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int
     }
   }
   if ((st = launch_check("replica swap")) != OG_OK) return st;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_compute_sasa(og_engine* e, int32_t s, int32_t method, int32_t n_dots, double* area_out) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!area_out) return og_fail(OG_E_BADARG, "null output");
+  if (method != 0 && method != 1) return og_fail(OG_E_BADARG, "method must be 0 (PowerSasa) or 1 (Shrake-Rupley)");
+  DVec<double> dots;
+  const double* dp = e->sr_dots.p;
+  int nd = e->n_sr_dots;
+  if (method == 1 && n_dots > 0 && n_dots != e->n_sr_dots) {
+    if (n_dots < 2) return og_fail(OG_E_BADARG, "n_dots must be >= 2");
+    OG_CUDA(dots.upload(sr_dot_table(n_dots), e->stream));
+    dp = dots.p;
+    nd = n_dots;
+  }
+  if ((st = sasa_areas_all(e, method, dp, nd)) != OG_OK) return st;
+  if ((st = copy_sys_range(e, e->sasa_area, s, area_out)) != OG_OK) return st;
   OG_CUDA(cudaStreamSynchronize(e->stream));
   return OG_OK;
 }

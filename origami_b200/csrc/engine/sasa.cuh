@@ -1,0 +1,64 @@
+// Analytical PowerSasa surface term on the GPU: per-atom accessible area
+// (spherical Gauss-Bonnet over the exposed boundary arcs) and its exact
+// analytical gradient, restating crates/energy/src/powersasa/ (see sasa.cu
+// for the per-function citations).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "step_kernels.cuh"
+
+namespace ogk {
+
+// Per-atom capacities of the on-chip boundary arrangement.  An atom that
+// exceeds one marks its system with kStatusSasaOverflow (the host reports
+// OG_E_UNSUPPORTED) instead of producing a wrong force.
+constexpr int kSasaMaxCaps = 128;
+constexpr int kSasaMaxTrans = 128;
+constexpr int kSasaMaxArcs = 96;
+constexpr int kStatusSasaOverflow = 8;
+
+// Probes of the accessible-component count (arrangement.rs:327-391).
+constexpr int kSasaProbes = 500;
+
+struct SasaArgs {
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* radius;       // per padded atom: vdW + 1.4 A probe
+  const double* gamma;        // per padded atom: surface tension, kJ/mol/A^2
+  const int32_t* tasks;       // padded atom indices to evaluate
+  int32_t n_tasks;
+  const int32_t* atom_sys;    // -1 for padding
+  const int2* sys_tiles;      // per system: (first tile, tile count)
+  const double4* origin;      // per tile: first atom, w = bounding radius
+  double r_max;               // largest SASA radius of any atom
+  unsigned long long* fx;     // fixed-point forces (kForceScale)
+  unsigned long long* fy;
+  unsigned long long* fz;
+  double* area;               // per padded atom (area kernels)
+  double* energy;             // per padded atom gamma * area (area kernels)
+  const double* probes;       // kSasaProbes x 3 unit vectors
+  const int32_t* probe_adj_begin;  // CSR adjacency of the probe graph
+  const int16_t* probe_adj;
+  SysState* sys;
+};
+
+// F_x += gamma_i R_i^2 (sum_arcs [theta dcos + cos_alpha dtheta] + sum_vertices
+// d epsilon) over every task atom i with a bounded boundary.
+void launch_sasa_forces(const SasaArgs& a, cudaStream_t s);
+
+// area[i] and energy[i] = gamma_i area[i] for every task atom i (0 buried,
+// 4 pi R^2 exposed).
+void launch_sasa_areas(const SasaArgs& a, cudaStream_t s);
+
+// Shrake-Rupley area (crates/energy/src/sasa.rs:65-110) with n_dots
+// Fibonacci test points per task atom; same outputs as launch_sasa_areas.
+void launch_shrake_rupley(const SasaArgs& a, const double* dots, int n_dots, cudaStream_t s);
+
+// Sets the kernels' shared-memory limits; call once before the first launch
+// (outside stream capture).
+cudaError_t sasa_prepare();
+
+}  // namespace ogk

@@ -28,7 +28,16 @@ __device__ __forceinline__ void pack_atom(const AtomArrays& a, int i) {
   const double ox = first_real ? a.x[first] : 0.0;
   const double oy = first_real ? a.y[first] : 0.0;
   const double oz = first_real ? a.z[first] : 0.0;
-  if ((i & 31) == 0) a.origin[tile] = make_double4(ox, oy, oz, 0.0);
+  // origin.w = radius of the tile's bounding sphere about its first atom
+  // (the SASA neighbour search culls tiles with it).  The whole warp is one
+  // tile: n_padded is a multiple of 32 and launches use whole warps.
+  double rad = 0.0;
+  if (a.atom_sys[i] >= 0) {
+    const double dx = a.x[i] - ox, dy = a.y[i] - oy, dz = a.z[i] - oz;
+    rad = sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  for (int o = 16; o > 0; o >>= 1) rad = fmax(rad, __shfl_xor_sync(0xffffffffu, rad, o));
+  if ((i & 31) == 0) a.origin[tile] = make_double4(ox, oy, oz, rad);
   if (a.atom_sys[i] >= 0) {
     a.pq[soa_index(i, 0)] = static_cast<float>(a.x[i] - ox);
     a.pq[soa_index(i, 1)] = static_cast<float>(a.y[i] - oy);
