@@ -62,7 +62,13 @@ struct DVec {
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
     // OG_DEBUG_POISON=1 fills new buffers with 0xFF bytes (NaN as float or
     // double) so a read before the first write shows up as a non-finite result.
-    if (e == cudaSuccess && poison_enabled()) e = cudaMemset(p, 0xFF, count * sizeof(T));
+    // The fill runs on the legacy default stream, which does not order against
+    // the engine's non-blocking stream, so it is waited for before the buffer
+    // is handed out (else it could land after the buffer's first write).
+    if (e == cudaSuccess && poison_enabled()) {
+      e = cudaMemset(p, 0xFF, count * sizeof(T));
+      if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
     return e;
   }
   static bool poison_enabled() {
@@ -198,6 +204,10 @@ struct og_engine {
   DVec<int32_t> sasa_tasks, sasa_all, probe_begin;
   DVec<int16_t> probe_adj;
   DVec<int2> sys_tiles;
+  DVec<ogk::SasaArcTerm> sasa_arc_terms;
+  DVec<ogk::SasaVertexTerm> sasa_vertex_terms;
+  DVec<int32_t> sasa_counts;
+  int sasa_term_cap = 0;
   int n_sasa_tasks = 0, n_sasa_all = 0, n_sr_dots = 0;
   double sasa_rmax = 0.0;
   // graph
@@ -300,6 +310,10 @@ struct og_engine {
     a.probe_adj_begin = probe_begin.p;
     a.probe_adj = probe_adj.p;
     a.sys = sys_state.p;
+    a.arc_terms = sasa_arc_terms.p;
+    a.vertex_terms = sasa_vertex_terms.p;
+    a.counts = sasa_counts.p;
+    a.term_cap = sasa_term_cap;
     return a;
   }
 
@@ -681,6 +695,15 @@ og_status finalize_impl(og_engine* e) {
     OG_CUDA(e->sys_tiles.upload(hst, st));
     OG_CUDA(e->sasa_area.alloc(np));
     OG_CUDA(e->sasa_energy.alloc(np));
+    if (e->p.include_sasa) {
+      // Term records of one force evaluation: proteins average a few exposed
+      // arcs per C/S atom and reach 19; 16 per atom on average is the limit
+      // (exceeding it is reported as a capacity overflow).
+      e->sasa_term_cap = 16 * e->n_sasa_tasks + 1024;
+      OG_CUDA(e->sasa_arc_terms.alloc(e->sasa_term_cap));
+      OG_CUDA(e->sasa_vertex_terms.alloc(e->sasa_term_cap));
+      OG_CUDA(e->sasa_counts.alloc(2));
+    }
     // Component probes: Fibonacci points, golden angle pi (3 - sqrt 5),
     // joined when their dot product exceeds cos(2.5 sqrt(4 pi / N))
     // (arrangement.rs:327-391).

@@ -59,13 +59,15 @@ __device__ __forceinline__ bool contains_strict(Cap c, D3 p) { return dot(p, c.a
 
 enum { kTwo = 0, kTangent = 1, kDisjoint = 2, kCoincident = 3 };
 
-// geometry.rs:70-102
+// geometry.rs:70-102 (one reciprocal for the shared denominator and one
+// reciprocal square root for the normal's length; same values to rounding).
 __device__ int intersect(Cap c1, Cap c2, D3* p, D3* q) {
   const double sigma = dot(c1.axis, c2.axis);
   const double denom = 1.0 - sigma * sigma;
   if (fabs(denom) < 1e-12) return fabs(c1.c - sigma * c2.c) < 1e-9 ? kCoincident : kDisjoint;
-  const double a = (c1.c - sigma * c2.c) / denom;
-  const double b = (c2.c - sigma * c1.c) / denom;
+  const double inv = 1.0 / denom;
+  const double a = (c1.c - sigma * c2.c) * inv;
+  const double b = (c2.c - sigma * c1.c) * inv;
   const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * sigma;
   if (c_sq < -1e-9) return kDisjoint;
   const D3 base = c1.axis * a + c2.axis * b;
@@ -73,9 +75,8 @@ __device__ int intersect(Cap c1, Cap c2, D3* p, D3* q) {
     *p = base;
     return kTangent;
   }
-  const double c = sqrt(c_sq);
   const D3 nc = cross(c1.axis, c2.axis);
-  const D3 off = (nc / norm(nc)) * c;
+  const D3 off = nc * (sqrt(c_sq) * rsqrt(norm2(nc)));
   *p = base + off;
   *q = base - off;
   return kTwo;
@@ -114,7 +115,7 @@ __device__ int identify_root_sign(Cap c1, Cap c2, D3 ref) {
 // ------------------------------------------------------ per-warp storage
 struct WarpSmem {
   // caps (indices in neighbour order, i.e. ascending atom index)
-  double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps], cs[kSasaMaxCaps];
+  double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps];
   int32_t owner[kSasaMaxCaps];
   uint8_t live[kSasaMaxCaps];
   // transitions of the cap being processed
@@ -244,7 +245,6 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
           w.cy[slot] = ay;
           w.cz[slot] = az;
           w.cc[slot] = ca;
-          w.cs[slot] = sqrt(fmax(1.0 - ca * ca, 0.0));
           w.owner[slot] = j;
         }
       }
@@ -256,19 +256,21 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
   if (n_caps == 0) return kExposed;
   __syncwarp();
 
-  // ---- drop caps whose circle lies inside another cap
+  // ---- drop caps whose circle lies inside another cap: alpha_k < alpha_m
+  // and angle(axis_k, axis_m) < alpha_m - alpha_k, i.e. sigma - c_k c_m -
+  // margin > s_k s_m, compared squared (both sides positive)
   int n_live = 0;
   for (int k0 = 0; k0 < n_caps; k0 += 32) {
     const int k = k0 + lane;
     bool live = k < n_caps;
     if (live) {
-      const double ck = w.cc[k], sk = w.cs[k];
+      const double ck = w.cc[k], sk2 = 1.0 - ck * ck;
       const D3 ak = {w.cx[k], w.cy[k], w.cz[k]};
       for (int m = 0; m < n_caps; ++m) {
         const double cm = w.cc[m];
         if (m == k || !(ck > cm)) continue;
-        const double sig = ak.x * w.cx[m] + ak.y * w.cy[m] + ak.z * w.cz[m];
-        if (sig > cm * ck + w.cs[m] * sk + 1e-6) {
+        const double lhs = ak.x * w.cx[m] + ak.y * w.cy[m] + ak.z * w.cz[m] - cm * ck - 1e-6;
+        if (lhs > 0.0 && lhs * lhs > sk2 * (1.0 - cm * cm)) {
           live = false;
           break;
         }
@@ -408,13 +410,13 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
         sb = w.torder[(r + 1) % n_kept];
         D3 mid;
         if (segment_midpoint(tpoint(w, sa), tpoint(w, sb), ck, n_kept == 1, &mid, &cos_ccw, &sin_ccw)) {
-          exposed = true;
-          for (int lm = 0; lm < n_live; ++lm) {
+          // A buried segment usually lies in one of the two caps whose
+          // circles bound it; testing those first ends most searches early
+          // (the answer -- inside any other cap -- does not depend on order).
+          exposed = !contains_strict(cap_at(w, w.tother[sa]), mid) && !contains_strict(cap_at(w, w.tother[sb]), mid);
+          for (int lm = 0; lm < n_live && exposed; ++lm) {
             const int m = w.live[lm];
-            if (m != k && contains_strict(cap_at(w, m), mid)) {
-              exposed = false;
-              break;
-            }
+            if (m != k && contains_strict(cap_at(w, m), mid)) exposed = false;
           }
         }
       }
@@ -484,7 +486,9 @@ __device__ __forceinline__ void scatter(const SasaArgs& a, int x, D3 g, double s
   if (g.z != 0.0) add_fixed(a.fz + x, g.z * scale, kForceScale);
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_sasa_forces(SasaArgs a) {
+// Force path, stage 1: the boundary of atom i as term records
+// (build_atom_cache + arc_other_cap_and_sign, analytical.rs:101-214, 655-670).
+__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
@@ -501,48 +505,74 @@ __global__ void __launch_bounds__(kWarps * 32) k_sasa_forces(SasaArgs a) {
   }
   if (outcome != kBounded || n_arcs == 0) return;
   link_boundary(w, n_arcs, n_verts, lane);
-
-  // F_x += gamma_i R_i^2 dA_i/dr_x per term: one lane per arc, then per
-  // vertex; atom i's share is summed over the warp first.
-  const D3 pi = pos(a, i);
-  const double ri = a.radius[i];
-  const double scale = a.gamma[i] * ri * ri;
-  D3 gi_sum = {0.0, 0.0, 0.0};
-  for (int it = lane; it < n_arcs + n_verts; it += 32) {
-    D3 gi = {0.0, 0.0, 0.0}, g1 = gi, g2 = gi, g3 = gi;
-    int x1, x2 = -1, x3 = -1;
-    if (it < n_arcs) {
-      const int e = it;
-      const int kc = w.a_cap[e];
-      x1 = w.owner[kc];
-      const int vs = w.a_vs[e], ve = w.a_ve[e];
-      const bool vertexed = !w.a_full[e] && vs >= 0 && ve >= 0;
-      int ss = 1, se = 1;
-      if (vertexed) {
-        const bool s_in = w.v_in[vs] == kc, e_in = w.v_in[ve] == kc;
-        x2 = w.owner[s_in ? w.v_out[vs] : w.v_in[vs]];
-        ss = s_in ? w.v_sign[vs] : -w.v_sign[vs];
-        x3 = w.owner[e_in ? w.v_out[ve] : w.v_in[ve]];
-        se = e_in ? w.v_sign[ve] : -w.v_sign[ve];
-      }
-      const D3 pl = vertexed ? pos(a, x2) : pi, pm = vertexed ? pos(a, x3) : pi;
-      const double rl = vertexed ? a.radius[x2] : ri, rm = vertexed ? a.radius[x3] : ri;
-      ogsasa::arc_gradient(pi, pos(a, x1), pl, pm, ri, a.radius[x1], rl, rm, ss, se, w.a_theta[e], vertexed, &gi,
-                           &g1, &g2, &g3);
-    } else {
-      const int v = it - n_arcs;
-      x1 = w.owner[w.v_in[v]];
-      x2 = w.owner[w.v_out[v]];
-      ogsasa::vertex_gradient(pi, pos(a, x1), pos(a, x2), ri, a.radius[x1], a.radius[x2], w.v_sign[v], &gi, &g1,
-                              &g2);
+  int arc_base = 0, vert_base = 0;
+  if (lane == 0) {
+    arc_base = atomicAdd(&a.counts[0], n_arcs);
+    vert_base = atomicAdd(&a.counts[1], n_verts);
+  }
+  arc_base = __shfl_sync(kFull, arc_base, 0);
+  vert_base = __shfl_sync(kFull, vert_base, 0);
+  if (arc_base + n_arcs > a.term_cap || vert_base + n_verts > a.term_cap) {
+    if (lane == 0) atomicOr(&a.sys[sys].status, kStatusSasaOverflow);
+    return;
+  }
+  for (int e = lane; e < n_arcs; e += 32) {
+    SasaArcTerm t;
+    const int kc = w.a_cap[e];
+    const int vs = w.a_vs[e], ve = w.a_ve[e];
+    t.i = i;
+    t.k = w.owner[kc];
+    t.theta = w.a_theta[e];
+    t.vertexed = (!w.a_full[e] && vs >= 0 && ve >= 0) ? 1 : 0;
+    t.l = t.m = -1;
+    t.ss = t.se = 1;
+    t.pad = 0;
+    if (t.vertexed) {
+      const bool s_in = w.v_in[vs] == kc, e_in = w.v_in[ve] == kc;
+      t.l = w.owner[s_in ? w.v_out[vs] : w.v_in[vs]];
+      t.ss = s_in ? w.v_sign[vs] : -w.v_sign[vs];
+      t.m = w.owner[e_in ? w.v_out[ve] : w.v_in[ve]];
+      t.se = e_in ? w.v_sign[ve] : -w.v_sign[ve];
     }
-    gi_sum = gi_sum + gi;
+    a.arc_terms[arc_base + e] = t;
+  }
+  for (int v = lane; v < n_verts; v += 32)
+    a.vertex_terms[vert_base + v] = SasaVertexTerm{i, w.owner[w.v_in[v]], w.owner[w.v_out[v]], w.v_sign[v]};
+}
+
+// Force path, stage 2: one term per thread, F_x += gamma_i R_i^2 dTerm/dr_x.
+__global__ void __launch_bounds__(128) k_sasa_terms(SasaArgs a) {
+  const int n_arc = min(a.counts[0], a.term_cap), n_vert = min(a.counts[1], a.term_cap);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_arc + n_vert; t += gridDim.x * blockDim.x) {
+    D3 gi = {0.0, 0.0, 0.0}, g1 = gi, g2 = gi, g3 = gi;
+    int i, x1, x2, x3 = -1;
+    if (t < n_arc) {
+      const SasaArcTerm r = a.arc_terms[t];
+      i = r.i;
+      x1 = r.k;
+      const D3 pi = pos(a, i);
+      const double ri = a.radius[i];
+      x2 = r.vertexed ? r.l : -1;
+      x3 = r.vertexed ? r.m : -1;
+      const D3 pl = r.vertexed ? pos(a, r.l) : pi, pm = r.vertexed ? pos(a, r.m) : pi;
+      const double rl = r.vertexed ? a.radius[r.l] : ri, rm = r.vertexed ? a.radius[r.m] : ri;
+      ogsasa::arc_gradient(pi, pos(a, x1), pl, pm, ri, a.radius[x1], rl, rm, r.ss, r.se, r.theta, r.vertexed != 0,
+                           &gi, &g1, &g2, &g3);
+    } else {
+      const SasaVertexTerm r = a.vertex_terms[t - n_arc];
+      i = r.i;
+      x1 = r.k;
+      x2 = r.l;
+      ogsasa::vertex_gradient(pos(a, i), pos(a, x1), pos(a, x2), a.radius[i], a.radius[x1], a.radius[x2], r.sign,
+                              &gi, &g1, &g2);
+    }
+    const double ri = a.radius[i];
+    const double scale = a.gamma[i] * ri * ri;
+    scatter(a, i, gi, scale);
     scatter(a, x1, g1, scale);
     if (x2 >= 0) scatter(a, x2, g2, scale);
     if (x3 >= 0) scatter(a, x3, g3, scale);
   }
-  gi_sum = {warp_sum(gi_sum.x), warp_sum(gi_sum.y), warp_sum(gi_sum.z)};
-  if (lane == 0) scatter(a, i, gi_sum, scale);
 }
 
 // Face walk with tangent disambiguation (area.rs:140-222): loop count and
@@ -769,7 +799,7 @@ constexpr size_t kWarpSmemBytes = sizeof(WarpSmem) * kWarps;
 }  // namespace
 
 cudaError_t sasa_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k_sasa_forces, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_sasa_boundary, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(kWarpSmemBytes));
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_sasa_areas, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -778,7 +808,9 @@ cudaError_t sasa_prepare() {
 
 void launch_sasa_forces(const SasaArgs& a, cudaStream_t s) {
   if (a.n_tasks <= 0) return;
-  k_sasa_forces<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  cudaMemsetAsync(a.counts, 0, 2 * sizeof(int32_t), s);
+  k_sasa_boundary<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  k_sasa_terms<<<148 * 8, 128, 0, s>>>(a);
 }
 
 void launch_sasa_areas(const SasaArgs& a, cudaStream_t s) {

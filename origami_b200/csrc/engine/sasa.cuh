@@ -13,14 +13,30 @@ namespace ogk {
 
 // Per-atom capacities of the on-chip boundary arrangement.  An atom that
 // exceeds one marks its system with kStatusSasaOverflow (the host reports
-// OG_E_UNSUPPORTED) instead of producing a wrong force.
+// OG_E_UNSUPPORTED) instead of producing a wrong force.  Protein atoms reach
+// about 90 caps, 46 of them left after contained caps are dropped, 72
+// transitions on one circle and 19 exposed arcs.
 constexpr int kSasaMaxCaps = 128;
 constexpr int kSasaMaxTrans = 128;
-constexpr int kSasaMaxArcs = 96;
+constexpr int kSasaMaxArcs = 48;
 constexpr int kStatusSasaOverflow = 8;
 
 // Probes of the accessible-component count (arrangement.rs:327-391).
 constexpr int kSasaProbes = 500;
+
+// One Gauss-Bonnet term of some atom i's boundary, as the force kernel's
+// second stage differentiates it: an arc of cap k (owner atom k) whose start
+// and end vertices are shared with the caps of atoms l and m (roots ss, se;
+// vertexed = 0 for a full circle or an unlinked vertex), or a vertex where
+// the boundary passes from the cap of atom k to that of atom l.
+struct SasaArcTerm {
+  int32_t i, k, l, m;
+  double theta;
+  int32_t ss, se, vertexed, pad;
+};
+struct SasaVertexTerm {
+  int32_t i, k, l, sign;
+};
 
 struct SasaArgs {
   const double* x;
@@ -43,10 +59,19 @@ struct SasaArgs {
   const int32_t* probe_adj_begin;  // CSR adjacency of the probe graph
   const int16_t* probe_adj;
   SysState* sys;
+  // force path: term records of every atom's boundary, appended through
+  // counts[0] (arcs) and counts[1] (vertices), capacity `term_cap` each
+  SasaArcTerm* arc_terms;
+  SasaVertexTerm* vertex_terms;
+  int32_t* counts;
+  int32_t term_cap;
 };
 
 // F_x += gamma_i R_i^2 (sum_arcs [theta dcos + cos_alpha dtheta] + sum_vertices
-// d epsilon) over every task atom i with a bounded boundary.
+// d epsilon) over every task atom i with a bounded boundary: a boundary
+// kernel (one warp per atom) appends term records, a second kernel
+// differentiates one record per thread.  counts must be zero on entry (the
+// launcher clears them on the stream).
 void launch_sasa_forces(const SasaArgs& a, cudaStream_t s);
 
 // area[i] and energy[i] = gamma_i area[i] for every task atom i (0 buried,
