@@ -1,10 +1,11 @@
 #!/usr/bin/env python3
-"""Throughput of the batched plain-GB MD step on B200 (and the CPU oracle port).
+"""Throughput of the batched GB + SASA MD step on B200 (and the CPU oracle port).
 
 Workload (one "step" = one BAOAB + SHAKE step of every replica):
   64 replicas of one 300-residue seeded-uniform chain (~4 900 atoms, built
-  extended by NeRF, relaxed), CHARMM36m bonded + LJ + Coulomb + GB, all-pairs
-  mode (no cutoffs), dt 2 fs, SHAKE on X-H bonds, 310 K, gamma 2 ps^-1.
+  extended by NeRF, relaxed), CHARMM36m bonded + LJ + Coulomb + GB + the
+  analytical PowerSasa hydrophobic term (gamma scale 0.25), all-pairs mode
+  (no cutoffs), dt 2 fs, SHAKE on X-H bonds, 310 K, gamma 2 ps^-1.
 Metric: aggregate ns/day over all replicas (and GPUs).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
@@ -110,9 +111,12 @@ def relax(og, chain, all_pairs: bool, max_steps: int = 300):
     return res
 
 
-def cpu_sample(chain, dt_fs: float, replicas: int, budget_s: float = 15.0, all_pairs: bool = True) -> dict:
+def cpu_sample(chain, dt_fs: float, replicas: int, budget_s: float = 15.0, all_pairs: bool = True,
+               sasa_scale: float | None = 0.25) -> dict:
     """Oracle port (FP64, OpenMP over all host threads): BAOAB+SHAKE steps of
-    one replica; returns aggregate ns/day for `replicas` replicas run on the CPU."""
+    one replica, plus (when sasa_scale is set) one analytical PowerSasa force
+    evaluation per step timed beside it; returns aggregate ns/day for
+    `replicas` replicas run on the CPU."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from conftest import INF, Orc, dp, oracle
     orc = Orc(chain)
@@ -120,18 +124,31 @@ def cpu_sample(chain, dt_fs: float, replicas: int, budget_s: float = 15.0, all_p
     v = np.zeros_like(x)
     cut = (INF, INF, INF) if all_pairs else (10.0, 20.0, 10.0)
     f = orc.total_force(x, *cut)
+    el_sasa = 0.0
+    if sasa_scale is not None:
+        el_ = np.array(chain.topology().element)
+        rad = np.array([oracle().orc_sasa_radius(int(e)) for e in el_])
+        gam = np.array([oracle().orc_sasa_gamma(int(e), sasa_scale) for e in el_])
+        fs = np.zeros_like(x)
     steps, t0 = 0, time.perf_counter()
     while True:
         oracle().orc_baoab(orc.tp, dp(x), dp(v), dp(f), 1, dt_fs, 2.0, 310.0, 1, 0, 0, steps, *cut)
+        if sasa_scale is not None:
+            ts = time.perf_counter()
+            fs[:] = 0.0
+            oracle().orc_sasa_forces(x.shape[0], dp(x), dp(rad), dp(gam), dp(fs))
+            el_sasa += time.perf_counter() - ts
         steps += 1
         el = time.perf_counter() - t0
         if el > budget_s or steps >= 50:
             break
     per_step = el / steps  # one replica
     agg = dt_fs * 1e-6 / (per_step * replicas) * 86400.0
+    what = "BAOAB+SHAKE step(s)" + (" + PowerSasa force evaluation(s)" if sasa_scale is not None else "")
     return {"value": agg, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} BAOAB+SHAKE step(s) of 1 replica ({chain.n_atoms} atoms, all pairs, FP64 oracle, "
-                      f"OpenMP {os.cpu_count()} threads), scaled to {replicas} replicas run back to back"}
+            "sample": f"{steps} {what} of 1 replica ({chain.n_atoms} atoms, all pairs, FP64 oracle, "
+                      f"OpenMP {os.cpu_count()} threads; SASA share {el_sasa / el:.0%}), scaled to {replicas} "
+                      "replicas run back to back"}
 
 
 def run_reference(args):
@@ -145,7 +162,8 @@ def run_reference(args):
         pass  # the oracle has no warm-up state; warm-up steps are skipped on the CPU arm
     t_all = time.perf_counter()
     for _ in range(max(args.steps, 1)):
-        samples.append(cpu_sample(chain, args.dt, args.replicas, budget_s=5.0, all_pairs=not args.cutoff)["value"])
+        samples.append(cpu_sample(chain, args.dt, args.replicas, budget_s=5.0, all_pairs=not args.cutoff,
+                                  sasa_scale=None if args.no_sasa else args.sasa_gamma_scale)["value"])
         if time.perf_counter() - t_all > 120:
             break
     val = statistics.median(samples)
@@ -156,20 +174,23 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args, chain),
         "cpu_baseline": {"value": val, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
-                         "sample": "one BAOAB+SHAKE step of one replica per timed step, FP64 oracle "
-                                   "(CPU restatement of origami's force/integrator path), OpenMP over all host "
-                                   f"threads, scaled to {args.replicas} replicas"},
+                         "sample": "BAOAB+SHAKE steps (+ one PowerSasa force evaluation each) of one replica "
+                                   "for about 5 s per timed step, FP64 oracle (CPU restatement of origami's "
+                                   "force/integrator path), OpenMP over all host threads, scaled to "
+                                   f"{args.replicas} replicas"},
         "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
 def workload_config(args, chain):
+    surface = "no SASA" if args.no_sasa else f"PowerSasa gamma scale {args.sasa_gamma_scale}"
     return {"workload": f"{args.replicas} replicas x {args.residues}-residue seeded chain, "
                         f"{'reference cutoffs 10/20/10 A' if args.cutoff else 'all pairs (no cutoff)'}, "
-                        f"dt {args.dt} fs + SHAKE, 310 K, plain GB",
+                        f"dt {args.dt} fs + SHAKE, 310 K, plain GB + {surface}",
             "replicas": args.replicas, "residues": args.residues, "atoms_per_replica": chain.n_atoms,
-            "mode": "cutoff" if args.cutoff else "all_pairs", "dt_fs": args.dt, "shake": True, "sasa": False,
+            "mode": "cutoff" if args.cutoff else "all_pairs", "dt_fs": args.dt, "shake": True,
+            "sasa": None if args.no_sasa else {"method": "analytical PowerSasa", "gamma_scale": args.sasa_gamma_scale},
             "born": "plain OBC-II pass", "l2": "flushed (256 MiB write) before every timed step",
             "seed": args.seed}
 
@@ -189,7 +210,8 @@ def run_b200(args):
     if not args.no_relax:
         relax(og, chain, all_pairs=not args.cutoff)
     mk = og.Params if args.cutoff else og.Params.all_pairs
-    params = mk(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1000 * rank)
+    params = mk(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1000 * rank,
+                include_sasa=not args.no_sasa, sasa_gamma_scale=args.sasa_gamma_scale)
     eng = og.Engine(params)
     x0 = chain.positions
     for _ in range(args.replicas):
@@ -264,7 +286,7 @@ def run_b200(args):
     e2e = ws * args.replicas * args.dt * 1e-6 / e2e_s * 86400.0
 
     shake_on = 1
-    launches_per_step = 9 + 2 * shake_on
+    launches_per_step = 9 + 2 * shake_on + (0 if args.no_sasa else 2)
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -275,6 +297,7 @@ def run_b200(args):
                      "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak)",
                      "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
         "kernels_ms_per_step": {k: v[0] / v[1] for k, v in prof.items()},
+        "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / ms_per_step) if "sasa" in prof else None,
         "born_pass_tflops": born_tflops,
         "pair_interactions_per_s": pairs / (ms_per_step * 1e-3) * ws,
         "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": args.replicas * atoms * 6 * 8,
@@ -284,7 +307,8 @@ def run_b200(args):
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(chain, args.dt, args.replicas, budget_s=args.cpu_budget,
-                                          all_pairs=not args.cutoff)
+                                          all_pairs=not args.cutoff,
+                                          sasa_scale=None if args.no_sasa else args.sasa_gamma_scale)
     if rank == 0:
         print(json.dumps(line))
     eng.close()
@@ -305,6 +329,8 @@ def main():
     ap.add_argument("--cutoff", action="store_true", help="reference cutoffs (10/20/10 A) instead of all pairs")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-sasa", action="store_true", help="leave out the PowerSasa surface term")
+    ap.add_argument("--sasa-gamma-scale", type=float, default=0.25)
     ap.add_argument("--no-relax", action="store_true",
                     help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")
     args = ap.parse_args()

@@ -118,7 +118,7 @@ struct WarpSmem {
   double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps];
   int32_t owner[kSasaMaxCaps];
   uint8_t live[kSasaMaxCaps];
-  // transitions of the cap being processed
+  // transitions of the cap being processed: sort key, unit radial direction
   double ta[kSasaMaxTrans], tx[kSasaMaxTrans], ty[kSasaMaxTrans], tz[kSasaMaxTrans];
   uint8_t tother[kSasaMaxTrans];
   uint8_t torder[kSasaMaxTrans];
@@ -134,6 +134,7 @@ struct WarpSmem {
 
 __device__ __forceinline__ Cap cap_at(const WarpSmem& w, int k) { return {{w.cx[k], w.cy[k], w.cz[k]}, w.cc[k]}; }
 __device__ __forceinline__ D3 pos(const SasaArgs& a, int j) { return {a.x[j], a.y[j], a.z[j]}; }
+// Unit radial direction of transition s of the circle being processed.
 __device__ __forceinline__ D3 tpoint(const WarpSmem& w, int s) { return {w.tx[s], w.ty[s], w.tz[s]}; }
 
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
@@ -148,33 +149,29 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
 
 enum Outcome { kExposed = 0, kBuried = 1, kBounded = 2, kInvalid = 3 };
 
-// Segment of circle k from transition point pa counter-clockwise to pb
-// (find_boundary's consecutive pair, arrangement.rs:190-215).  Returns false
-// for a segment the reference skips (ccw < 1e-9); else the exposure test
-// point *mid and the cosine / sine of the ccw angle.  single = the circle's
-// only transition (the segment is the whole circle, ccw = 2 pi).
-__device__ bool segment_midpoint(D3 pa, D3 pb, Cap ck, bool single, D3* mid, double* cos_ccw, double* sin_ccw) {
-  const D3 axial = ck.axis * dot(pa, ck.axis);
-  const D3 ra = pa - axial;
-  const double rn = norm(ra);
+// A point of circle k (cos alpha_k = ck.c, radius sk = sin alpha_k) from its
+// unit radial direction u (perpendicular to the axis).
+__device__ __forceinline__ D3 circle_point(Cap ck, double sk, D3 u) { return ck.axis * ck.c + u * sk; }
+
+// Segment of circle k from the transition with radial direction ua
+// counter-clockwise to the one with ub (find_boundary's consecutive pair,
+// arrangement.rs:190-215).  Returns false for a segment the reference skips
+// (ccw < 1e-9); else the exposure test point *mid (ua rotated by half the ccw
+// angle, midpoint_on_circle) and the cosine / sine of the ccw angle.
+// single = the circle's only transition (the whole circle, ccw = 2 pi).
+__device__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D3* mid, double* cos_ccw,
+                                 double* sin_ccw) {
   if (single) {
     *cos_ccw = 1.0;
     *sin_ccw = 0.0;
-    *mid = rn < 1e-12 ? pa : axial - ra;
+    *mid = ck.axis * ck.c - ua * sk;
     return true;
   }
-  const D3 rb = pb - ck.axis * dot(pb, ck.axis);
-  const double rnb = norm(rb);
-  const double inv = 1.0 / (rn * rnb);
-  const double c = dot(ra, rb) * inv;
-  const double s = dot(ck.axis, cross(ra, rb)) * inv;
+  const double c = dot(ua, ub);
+  const double s = dot(ck.axis, cross(ua, ub));
   *cos_ccw = c;
   *sin_ccw = s;
   if (c > 0.0 && s >= 0.0 && s < 2e-9 && atan2(s, c) < 1e-9) return false;
-  if (rn < 1e-12) {
-    *mid = pa;
-    return true;
-  }
   // cos / sin of half the ccw angle h in (0, pi], from c = cos 2h, s = sin 2h
   double ch, sh;
   if (c >= 0.0) {
@@ -185,9 +182,7 @@ __device__ bool segment_midpoint(D3 pa, D3 pb, Cap ck, bool single, D3* mid, dou
     sh = sqrt((1.0 - c) * 0.5);
     ch = s / (2.0 * sh);
   }
-  const D3 u = ra / rn;
-  const D3 v = cross(ck.axis, u);
-  *mid = axial + (u * ch + v * sh) * rn;
+  *mid = circle_point(ck, sk, ua * ch + cross(ck.axis, ua) * sh);
   return true;
 }
 
@@ -291,6 +286,10 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     const D3 h = helper_axis(ck.axis);
     const D3 fu = normalize(h - ck.axis * dot(h, ck.axis));
     const D3 fv = cross(ck.axis, fu);
+    // Transitions are kept as unit radial directions u: every one lies on
+    // circle k, p = axis cos(alpha_k) + u sin(alpha_k).
+    const double sk = sqrt(fmax(1.0 - ck.c * ck.c, 0.0));
+    const double inv_sk = sk > 0.0 ? 1.0 / sk : 0.0;
     int n_tr = 0;
     for (int m0 = 0; m0 < n_live; m0 += 32) {
       const int lm = m0 + lane;
@@ -318,20 +317,20 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
       }
       if (cnt >= 1) {
         const int s = n_tr + off;
-        const D3 pr = p - ck.axis * dot(p, ck.axis);
-        w.ta[s] = pseudo_angle(dot(pr, fu), dot(pr, fv));
-        w.tx[s] = p.x;
-        w.ty[s] = p.y;
-        w.tz[s] = p.z;
+        const D3 u = (p - ck.axis * ck.c) * inv_sk;
+        w.ta[s] = pseudo_angle(dot(u, fu), dot(u, fv));
+        w.tx[s] = u.x;
+        w.ty[s] = u.y;
+        w.tz[s] = u.z;
         w.tother[s] = static_cast<uint8_t>(m);
       }
       if (cnt == 2) {
         const int s = n_tr + off + 1;
-        const D3 pr = q - ck.axis * dot(q, ck.axis);
-        w.ta[s] = pseudo_angle(dot(pr, fu), dot(pr, fv));
-        w.tx[s] = q.x;
-        w.ty[s] = q.y;
-        w.tz[s] = q.z;
+        const D3 u = (q - ck.axis * ck.c) * inv_sk;
+        w.ta[s] = pseudo_angle(dot(u, fu), dot(u, fv));
+        w.tx[s] = u.x;
+        w.ty[s] = u.y;
+        w.tz[s] = u.z;
         w.tother[s] = static_cast<uint8_t>(m);
       }
       n_tr += total;
@@ -355,16 +354,19 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
       break;
     }
     __syncwarp();
-    // consecutive de-duplication (|dp|^2 < 1e-12 against the last kept)
+    // consecutive de-duplication (|dp|^2 < 1e-12 against the last kept;
+    // |dp| = sin(alpha_k) |du| on the circle)
+    const double sk2 = sk * sk;
     bool dup = false;
-    for (int r = 1 + lane; r < n_tr; r += 32) dup |= norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) < 1e-12;
+    for (int r = 1 + lane; r < n_tr; r += 32)
+      dup |= norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * sk2 < 1e-12;
     int n_kept = n_tr;
     if (__any_sync(kFull, dup)) {
       if (lane == 0) {
         int kept = 0;
         for (int r = 0; r < n_tr; ++r) {
           const int s = w.torder[r];
-          if (kept == 0 || norm2(tpoint(w, s) - tpoint(w, w.torder[kept - 1])) >= 1e-12)
+          if (kept == 0 || norm2(tpoint(w, s) - tpoint(w, w.torder[kept - 1])) * sk2 >= 1e-12)
             w.torder[kept++] = static_cast<uint8_t>(s);
         }
         n_kept = kept;
@@ -409,7 +411,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
         sa = w.torder[r];
         sb = w.torder[(r + 1) % n_kept];
         D3 mid;
-        if (segment_midpoint(tpoint(w, sa), tpoint(w, sb), ck, n_kept == 1, &mid, &cos_ccw, &sin_ccw)) {
+        if (segment_midpoint(tpoint(w, sa), tpoint(w, sb), ck, sk, n_kept == 1, &mid, &cos_ccw, &sin_ccw)) {
           // A buried segment usually lies in one of the two caps whose
           // circles bound it; testing those first ends most searches early
           // (the answer -- inside any other cap -- does not depend on order).
@@ -434,13 +436,14 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
         w.a_cap[e] = static_cast<uint8_t>(k);
         w.a_full[e] = 0;
         w.a_theta[e] = -ccw;
-        w.a_sx[e] = w.tx[sb];
-        w.a_sy[e] = w.ty[sb];
-        w.a_sz[e] = w.tz[sb];
+        const D3 pb = circle_point(ck, sk, tpoint(w, sb)), pa = circle_point(ck, sk, tpoint(w, sa));
+        w.a_sx[e] = pb.x;
+        w.a_sy[e] = pb.y;
+        w.a_sz[e] = pb.z;
         w.a_own[e] = static_cast<int16_t>(v);
-        w.v_x[v] = w.tx[sa];
-        w.v_y[v] = w.ty[sa];
-        w.v_z[v] = w.tz[sa];
+        w.v_x[v] = pa.x;
+        w.v_y[v] = pa.y;
+        w.v_z[v] = pa.z;
         w.v_in[v] = static_cast<uint8_t>(k);
         w.v_out[v] = w.tother[sa];
       }
