@@ -298,6 +298,17 @@ og_status og_gb_energy_noalloc(const double* xyz, const double* charge, const do
  * pair kernels' FP32-pipe roofline.  No counterpart in the reference. */
 og_status og_measure_fp32_peak(double* tflops);
 
+/* BF16 tensor-core GEMM (tcgen05, FP32 accumulate) on DEVICE buffers:
+ *   c[m*c_sm + n*c_sn] = sum_k a[m*a_sm + k*a_sk] * b[n*b_sn + k*b_sk]
+ * (+ bias[n] when bias is not NULL; c_act, when not NULL, receives SiLU(c)
+ * with c's strides).  Operands are FP32 and rounded to BF16 for the MMA.
+ * splits > 1 divides K among CTAs (c must then be row-major contiguous).
+ * The learned-Born-radius network trains and runs on it.  No counterpart
+ * in the reference. */
+og_status og_tc_gemm(const float* a, int64_t a_sm, int64_t a_sk, const float* b, int64_t b_sn, int64_t b_sk,
+                     float* c, int64_t c_sm, int64_t c_sn, int32_t m, int32_t n, int32_t k, const float* bias,
+                     float* c_act, int32_t splits, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

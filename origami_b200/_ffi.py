@@ -104,6 +104,9 @@ SIGNATURES = [
     ("og_measure_fp32_peak", C.c_int, [c_double_p]),
     ("og_gb_energy_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double,
                                        C.c_void_p, C.c_void_p]),
+    ("og_tc_gemm", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
+                             C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                             C.c_int32, C.c_void_p]),
 ]
 
 
