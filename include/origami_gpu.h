@@ -309,6 +309,48 @@ og_status og_tc_gemm(const float* a, int64_t a_sm, int64_t a_sk, const float* b,
                      float* c, int64_t c_sm, int64_t c_sn, int32_t m, int32_t n, int32_t k, const float* bias,
                      float* c_act, int32_t splits, void* cuda_stream);
 
+/* ---- Learned Born radii (born_mode = 1).  No counterpart in the reference.
+ * Per atom: 64 descriptors D (16 Gaussian shells, centres 1.5..12 A, width
+ * 0.7 A, x 4 element classes C/S, N/P, O, H; partner-radius weighted, cosine
+ * cutoff 12 A), input x = log(1 + D); a 64-128-128-128-1 SiLU network (BF16
+ * tensor-core products, FP32 accumulate) predicts y = log(R / R_cfa), R_cfa
+ * the Coulomb-field radius in its pairwise (HCT) form over the same 12 A
+ * neighbours: 1/R_cfa = max(1/rho~ - sum fc I_HCT(r, rho~_i, s_j rho~_j),
+ * 1/30).  Parameters: OG_LGB_N_PARAMS floats, W1[128x64] b1[128] W2[128x128]
+ * b2[128] W3[128x128] b3[128] w4[128] b4 (W row-major, out x in).  Forces use
+ * the predicted radii frozen, like the plain pass's.  Energies
+ * (og_compute_energies) stay plain GB. */
+#define OG_LGB_N_PARAMS 41473
+#define OG_LGB_N_DESC 64
+
+/* Uniform(+-1/sqrt(fan_in)) weights, zero biases, from `seed`. */
+og_status og_lgb_init_params(uint64_t seed, float* params);
+/* Minibatch Adam (beta 0.9 / 0.999) on the mean squared error of y over
+ * host samples x[n x 64], target[n]; params updated in place;
+ * loss_per_step (optional) receives each step's batch loss. */
+og_status og_lgb_train(const float* x, const float* target, int64_t n, int32_t steps, int32_t batch, double lr,
+                       uint64_t seed, float* params, float* loss_per_step);
+/* Mean squared error and its gradient (OG_LGB_N_PARAMS floats) over all n
+ * samples in one batch (n <= 2^20), by the same kernels. */
+og_status og_lgb_loss_and_gradient(const float* x, const float* target, int64_t n, const float* params,
+                                   double* loss, float* grad);
+/* Training samples of system `sys` at its current positions: x_out
+ * (n_atoms x 64, log(1 + D)) and target_out (n_atoms) = log(R_plain / R_cfa)
+ * with R_plain the FP64 plain-GB radii.  Any born_mode. */
+og_status og_lgb_samples(og_engine* e, int32_t sys, float* x_out, float* target_out);
+/* Loads the network (born_mode = 1 engines); required before stepping. */
+og_status og_lgb_set_params(og_engine* e, const float* params);
+/* Every `interval_steps` steps (default 500; 0 = never) og_step evaluates
+ * the forces with plain GB radii at the current positions; if the largest
+ * per-system RMS relative force difference exceeds `tolerance` (default
+ * 1e-3) the engine falls back to plain GB for the rest of the run. */
+og_status og_lgb_set_judge(og_engine* e, int32_t interval_steps, double tolerance);
+/* active = learned radii in use; judged = judge evaluations so far;
+ * last_error = the last judge's error (-1 before the first). */
+og_status og_lgb_status(og_engine* e, int32_t* active, int32_t* judged, double* last_error);
+/* Runs the judge now (and falls back if it fails); rms_rel receives the error. */
+og_status og_lgb_judge(og_engine* e, double* rms_rel);
+
 #ifdef __cplusplus
 }
 #endif

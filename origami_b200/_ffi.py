@@ -10,8 +10,11 @@ import ctypes as C
 c_double_p = C.POINTER(C.c_double)
 c_int32_p = C.POINTER(C.c_int32)
 c_int8_p = C.POINTER(C.c_int8)
+c_float_p = C.POINTER(C.c_float)
 
 OG_OK = 0
+LGB_N_PARAMS = 41473  # OG_LGB_N_PARAMS
+LGB_N_DESC = 64       # OG_LGB_N_DESC
 STATUS_NAMES = {
     0: "OG_OK", 1: "OG_E_BADARG", 2: "OG_E_NONFINITE", 3: "OG_E_SHAKE", 4: "OG_E_TIMEOUT",
     5: "OG_E_CUDA", 6: "OG_E_NOMEM", 7: "OG_E_STATE", 8: "OG_E_DATA", 9: "OG_E_UNSUPPORTED",
@@ -107,6 +110,15 @@ SIGNATURES = [
     ("og_tc_gemm", C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p,
                              C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                              C.c_int32, C.c_void_p]),
+    ("og_lgb_init_params", C.c_int, [C.c_uint64, c_float_p]),
+    ("og_lgb_train", C.c_int, [c_float_p, c_float_p, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64,
+                               c_float_p, c_float_p]),
+    ("og_lgb_loss_and_gradient", C.c_int, [c_float_p, c_float_p, C.c_int64, c_float_p, c_double_p, c_float_p]),
+    ("og_lgb_samples", C.c_int, [C.c_void_p, C.c_int32, c_float_p, c_float_p]),
+    ("og_lgb_set_params", C.c_int, [C.c_void_p, c_float_p]),
+    ("og_lgb_set_judge", C.c_int, [C.c_void_p, C.c_int32, C.c_double]),
+    ("og_lgb_status", C.c_int, [C.c_void_p, c_int32_p, c_int32_p, c_double_p]),
+    ("og_lgb_judge", C.c_int, [C.c_void_p, c_double_p]),
 ]
 
 

@@ -21,8 +21,10 @@
 #include "../../../include/origami_gpu.h"
 #include "../host/status.h"
 #include "common.cuh"
+#include "lgb.cuh"
 #include "pair_kernels.cuh"
 #include "sasa.cuh"
+#include "tc_gemm.cuh"
 #include "step_kernels.cuh"
 
 namespace ogk {
@@ -209,6 +211,16 @@ struct og_engine {
   DVec<int32_t> sasa_counts;
   int sasa_term_cap = 0;
   int n_sasa_tasks = 0, n_sasa_all = 0, n_sr_dots = 0;
+  // learned Born radii: descriptor class per atom, network input, Coulomb-
+  // field radii, two hidden-layer buffers, parameters; judge state
+  DVec<int32_t> lgb_class;
+  DVec<float> lgb_x, lgb_ha, lgb_hb, lgb_params;
+  DVec<double> lgb_rcfa, lgb_part;
+  DVec<unsigned long long> lgb_fx, lgb_fy, lgb_fz;
+  bool lgb_params_set = false, lgb_active = false;
+  int lgb_judge_interval = 500, lgb_judged = 0;
+  double lgb_tol = 1e-3, lgb_last_err = -1.0;
+  int64_t lgb_since_judge = 0;
   double sasa_rmax = 0.0;
   // graph
   cudaGraph_t graph = nullptr;
@@ -369,18 +381,73 @@ struct og_engine {
     }
   };
 
+  bool lgb_on() const { return p.born_mode == 1 && lgb_active; }
+
+  ogk::LgbDescArgs lgb_desc_args() {
+    ogk::LgbDescArgs a{};
+    a.x = x.p; a.y = y.p; a.z = z.p;
+    a.atom_sys = atom_sys.p;
+    a.klass = lgb_class.p;
+    a.rho = rho.p;
+    a.rho_tilde = rho_tilde.p;
+    a.srho = srho.p;
+    a.sys_tiles = sys_tiles.p;
+    a.origin = origin.p;
+    a.n_padded = n_padded;
+    a.xin = lgb_x.p;
+    a.r_cfa = lgb_rcfa.p;
+    return a;
+  }
+
+  // One tensor-core layer of the radius network over every padded atom:
+  // out = SiLU(in W^T + b) (the epilogue writes z, then SiLU(z), in place).
+  void lgb_layer(const float* in, int k_in, int w_off, int b_off, float* out) {
+    ogk::TcGemmArgs g{};
+    g.a = in; g.a_sm = k_in; g.a_sk = 1;
+    g.b = lgb_params.p + w_off; g.b_sn = k_in; g.b_sk = 1;
+    g.c = out; g.c_sm = ogk::kLgbHidden; g.c_sn = 1;
+    g.m = n_padded; g.n = ogk::kLgbHidden; g.k = k_in;
+    g.bias = lgb_params.p + b_off;
+    g.c_act = out;
+    g.error_flag = error_flag.p;
+    ogk::launch_tc_gemm(g, 1, nullptr, stream);
+  }
+
+  // Radii from the network: descriptors, three hidden layers, head.
+  void enqueue_learned_radii() {
+    {
+      Timer t(this, "lgb_descriptors");
+      ogk::launch_lgb_descriptors(lgb_desc_args(), stream);
+    }
+    {
+      Timer t(this, "lgb_network");
+      lgb_layer(lgb_x.p, ogk::kLgbIn, ogk::kLgbOffW1, ogk::kLgbOffB1, lgb_ha.p);
+      lgb_layer(lgb_ha.p, ogk::kLgbHidden, ogk::kLgbOffW2, ogk::kLgbOffB2, lgb_hb.p);
+      lgb_layer(lgb_hb.p, ogk::kLgbHidden, ogk::kLgbOffW3, ogk::kLgbOffB3, lgb_ha.p);
+    }
+    {
+      Timer t(this, "lgb_radii");
+      ogk::launch_lgb_radii(atoms(), lgb_ha.p, lgb_params.p, lgb_rcfa.p, stream);
+    }
+  }
+
   // Force evaluation on the device (positions already packed and
-  // accumulators zeroed): Born pass, radii, fused pair force, bonded terms.
+  // accumulators zeroed): Born radii (descreening pass, or the learned
+  // network), fused pair force, bonded terms, surface term.
   void enqueue_forces() {
     ogk::PairArgs pa = pair_args();
     ogk::AtomArrays at = atoms();
-    {
-      Timer t(this, "born_pass");
-      ogk::launch_born_pass(pa, stream);
-    }
-    {
-      Timer t(this, "born_finalize");
-      ogk::launch_born_finalize(at, nullptr, born_r.p, true, nullptr, stream);
+    if (lgb_on()) {
+      enqueue_learned_radii();
+    } else {
+      {
+        Timer t(this, "born_pass");
+        ogk::launch_born_pass(pa, stream);
+      }
+      {
+        Timer t(this, "born_finalize");
+        ogk::launch_born_finalize(at, nullptr, born_r.p, true, nullptr, stream);
+      }
     }
     {
       Timer t(this, "force_pass");
@@ -738,6 +805,26 @@ og_status finalize_impl(og_engine* e) {
     OG_CUDA(ogk::sasa_prepare());
   }
 
+  // ---- learned Born radii: descriptor class per atom (C,S -> 0; N,P -> 1;
+  // O -> 2; H -> 3), buffers when born_mode = 1
+  {
+    static const int32_t kClass[6] = {3, 0, 1, 2, 1, 0};
+    std::vector<int32_t> hc(np, 0);
+    for (int si = 0; si < n_sys; ++si)
+      for (int k = 0; k < e->sys[si].topo.n; ++k) hc[e->sys[si].atom_begin + k] = kClass[e->sys[si].topo.element[k]];
+    OG_CUDA(e->lgb_class.upload(hc, st));
+    OG_CUDA(ogk::tc_gemm_prepare());
+    if (e->p.born_mode == 1) {
+      OG_CUDA(e->lgb_x.alloc(static_cast<size_t>(np) * ogk::kLgbIn));
+      OG_CUDA(e->lgb_rcfa.alloc(np));
+      OG_CUDA(e->lgb_ha.alloc(static_cast<size_t>(np) * ogk::kLgbHidden));
+      OG_CUDA(e->lgb_hb.alloc(static_cast<size_t>(np) * ogk::kLgbHidden));
+      OG_CUDA(e->lgb_params.alloc(ogk::kLgbNParams));
+      for (auto* v : {&e->lgb_fx, &e->lgb_fy, &e->lgb_fz}) OG_CUDA(v->alloc(np));
+      OG_CUDA(e->lgb_part.alloc(2 * static_cast<size_t>(n_sys)));
+    }
+  }
+
   // ---- per-system state
   std::vector<ogk::SysState> hs(n_sys);
   for (int si = 0; si < n_sys; ++si) {
@@ -976,11 +1063,63 @@ og_status finalize_impl(og_engine* e) {
 }
 
 og_status eval_forces(og_engine* e) {
+  if (e->p.born_mode == 1 && !e->lgb_params_set)
+    return og_fail(OG_E_STATE, "born_mode 1 needs the network's parameters (og_lgb_set_params)");
   ogk::launch_pack(e->atoms(), true, e->stream);
   e->enqueue_forces();
   og_status st = launch_check("force evaluation");
   if (st != OG_OK) return st;
   e->forces_valid = true;
+  return OG_OK;
+}
+
+void reset_graph(og_engine* e) {
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  e->graph_exec = nullptr;
+  e->graph = nullptr;
+}
+
+og_status lgb_check(og_engine* e) {
+  if (e->p.born_mode == 1 && !e->lgb_params_set)
+    return og_fail(OG_E_STATE, "born_mode 1 needs the network's parameters (og_lgb_set_params)");
+  return OG_OK;
+}
+
+// Judge (plain GB against the network at the current positions): forces
+// with plain radii are kept aside, forces with learned radii are evaluated
+// last (they are the ones the next step uses), and the largest per-system
+// RMS relative difference decides; above the tolerance the engine falls
+// back to plain GB for good.
+og_status lgb_judge(og_engine* e, double* err_out) {
+  cudaStream_t st = e->stream;
+  const int n_sys = static_cast<int>(e->sys.size());
+  e->lgb_active = false;
+  og_status s = eval_forces(e);
+  if (s != OG_OK) return s;
+  const size_t bytes = sizeof(unsigned long long) * e->n_padded;
+  OG_CUDA(cudaMemcpyAsync(e->lgb_fx.p, e->fx.p, bytes, cudaMemcpyDeviceToDevice, st));
+  OG_CUDA(cudaMemcpyAsync(e->lgb_fy.p, e->fy.p, bytes, cudaMemcpyDeviceToDevice, st));
+  OG_CUDA(cudaMemcpyAsync(e->lgb_fz.p, e->fz.p, bytes, cudaMemcpyDeviceToDevice, st));
+  e->lgb_active = true;
+  if ((s = eval_forces(e)) != OG_OK) return s;
+  ogk::launch_lgb_force_error(e->fx.p, e->fy.p, e->fz.p, e->lgb_fx.p, e->lgb_fy.p, e->lgb_fz.p, e->seg_begin.p,
+                              e->seg_end.p, n_sys, e->lgb_part.p, st);
+  std::vector<double> part(2 * static_cast<size_t>(n_sys));
+  OG_CUDA(cudaMemcpyAsync(part.data(), e->lgb_part.p, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st));
+  OG_CUDA(cudaStreamSynchronize(st));
+  if ((s = launch_check("judge")) != OG_OK) return s;
+  double err = 0.0;
+  for (int k = 0; k < n_sys; ++k) err = std::max(err, std::sqrt(part[2 * k] / std::max(part[2 * k + 1], 1e-300)));
+  e->lgb_last_err = err;
+  e->lgb_judged += 1;
+  e->lgb_since_judge = 0;
+  if (!(err <= e->lgb_tol)) {
+    e->lgb_active = false;
+    reset_graph(e);
+    if ((s = eval_forces(e)) != OG_OK) return s;
+  }
+  if (err_out) *err_out = err;
   return OG_OK;
 }
 
@@ -1027,7 +1166,7 @@ og_status og_engine_create(const og_params* params, og_engine** out) {
   if (!params || !out) return og_fail(OG_E_BADARG, "null argument");
   *out = nullptr;
   if (!(params->dt_fs > 0.0)) return og_fail(OG_E_BADARG, "dt_fs must be positive");
-  if (params->born_mode != 0) return og_fail(OG_E_UNSUPPORTED, "learned Born radii are not built into this engine");
+  if (params->born_mode != 0 && params->born_mode != 1) return og_fail(OG_E_BADARG, "born_mode must be 0 or 1");
   int n_dev = 0;
   if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0)
     return og_fail(OG_E_CUDA, "no CUDA device available");
@@ -1328,13 +1467,29 @@ og_status og_step(og_engine* e, int32_t n_steps) {
   og_status st = check_ready(e);
   if (st != OG_OK) return st;
   if (n_steps < 0) return og_fail(OG_E_BADARG, "negative step count");
+  if ((st = lgb_check(e)) != OG_OK) return st;
   if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
-  if (e->profile) {
-    for (int k = 0; k < n_steps; ++k) e->enqueue_step();
-    if ((st = launch_check("step")) != OG_OK) return st;
-  } else if (n_steps > 0) {
-    if ((st = build_graph(e)) != OG_OK) return st;
-    for (int k = 0; k < n_steps; ++k) OG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
+  int done = 0;
+  while (done < n_steps) {
+    // with learned radii, plain GB judges the forces every lgb_judge_interval steps
+    int chunk = n_steps - done;
+    const bool judging = e->lgb_on() && e->lgb_judge_interval > 0;
+    if (judging) chunk = static_cast<int>(std::min<int64_t>(chunk, e->lgb_judge_interval - e->lgb_since_judge));
+    if (e->profile) {
+      for (int k = 0; k < chunk; ++k) e->enqueue_step();
+      if ((st = launch_check("step")) != OG_OK) return st;
+    } else if (chunk > 0) {
+      if ((st = build_graph(e)) != OG_OK) return st;
+      for (int k = 0; k < chunk; ++k) OG_CUDA(cudaGraphLaunch(e->graph_exec, e->stream));
+    }
+    done += chunk;
+    if (judging) {
+      e->lgb_since_judge += chunk;
+      if (e->lgb_since_judge >= e->lgb_judge_interval) {
+        double err = 0.0;
+        if ((st = lgb_judge(e, &err)) != OG_OK) return st;
+      }
+    }
   }
   std::vector<ogk::SysState> hs;
   if ((st = read_status(e, &hs)) != OG_OK) return st;
@@ -1439,6 +1594,74 @@ og_status og_compute_sasa(og_engine* e, int32_t s, int32_t method, int32_t n_dot
   if ((st = sasa_areas_all(e, method, dp, nd)) != OG_OK) return st;
   if ((st = copy_sys_range(e, e->sasa_area, s, area_out)) != OG_OK) return st;
   OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_lgb_set_params(og_engine* e, const float* params) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!params) return og_fail(OG_E_BADARG, "null parameters");
+  if (e->p.born_mode != 1) return og_fail(OG_E_STATE, "the engine was not created with born_mode = 1");
+  for (int k = 0; k < ogk::kLgbNParams; ++k)
+    if (!std::isfinite(params[k])) return og_fail(OG_E_NONFINITE, "non-finite network parameter");
+  OG_CUDA(cudaMemcpyAsync(e->lgb_params.p, params, sizeof(float) * ogk::kLgbNParams, cudaMemcpyHostToDevice,
+                          e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  if (!e->lgb_active) reset_graph(e);
+  e->lgb_params_set = true;
+  e->lgb_active = true;
+  e->lgb_since_judge = 0;
+  e->forces_valid = false;
+  return OG_OK;
+}
+
+og_status og_lgb_set_judge(og_engine* e, int32_t interval_steps, double tolerance) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  if (interval_steps < 0 || !(tolerance > 0.0)) return og_fail(OG_E_BADARG, "bad judge settings");
+  e->lgb_judge_interval = interval_steps;
+  e->lgb_tol = tolerance;
+  return OG_OK;
+}
+
+og_status og_lgb_status(og_engine* e, int32_t* active, int32_t* judged, double* last_error) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  if (active) *active = e->lgb_on() ? 1 : 0;
+  if (judged) *judged = e->lgb_judged;
+  if (last_error) *last_error = e->lgb_last_err;
+  return OG_OK;
+}
+
+og_status og_lgb_judge(og_engine* e, double* rms_rel) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!e->lgb_on()) return og_fail(OG_E_STATE, "learned radii are not active");
+  return lgb_judge(e, rms_rel);
+}
+
+og_status og_lgb_samples(og_engine* e, int32_t s, float* x_out, float* target_out) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!x_out || !target_out) return og_fail(OG_E_BADARG, "null output");
+  const int np = e->n_padded;
+  if (!e->lgb_x.p) OG_CUDA(e->lgb_x.alloc(static_cast<size_t>(np) * ogk::kLgbIn));
+  if (!e->lgb_rcfa.p) OG_CUDA(e->lgb_rcfa.alloc(np));
+  // plain GB radii of the FP64 energy path (born_r64) at the current positions
+  og_energies en{};
+  if ((st = og_compute_energies(e, s, &en)) != OG_OK) return st;
+  ogk::launch_pack(e->atoms(), false, e->stream);
+  ogk::launch_lgb_descriptors(e->lgb_desc_args(), e->stream);
+  if ((st = launch_check("descriptors")) != OG_OK) return st;
+  const SysHost& sh = e->sys[s];
+  const int n = sh.topo.n;
+  std::vector<double> rc(n), rp(n);
+  OG_CUDA(cudaMemcpyAsync(x_out, e->lgb_x.p + static_cast<size_t>(sh.atom_begin) * ogk::kLgbIn,
+                          sizeof(float) * ogk::kLgbIn * n, cudaMemcpyDeviceToHost, e->stream));
+  OG_CUDA(cudaMemcpyAsync(rc.data(), e->lgb_rcfa.p + sh.atom_begin, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                          e->stream));
+  OG_CUDA(cudaMemcpyAsync(rp.data(), e->born_r64.p + sh.atom_begin, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                          e->stream));
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  for (int k = 0; k < n; ++k) target_out[k] = static_cast<float>(std::log(rp[k] / rc[k]));
   return OG_OK;
 }
 

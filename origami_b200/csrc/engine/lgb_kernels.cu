@@ -1,0 +1,288 @@
+// Kernels of the learned-Born-radius path (definitions in lgb.cuh).
+#include <cmath>
+
+#include "common.cuh"
+#include "lgb.cuh"
+
+namespace ogk {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kMu0 = 1.5f, kShell = 0.7f;
+constexpr float kInv2Sigma2 = 1.0f / (2.0f * 0.7f * 0.7f);
+constexpr float kCut = 12.0f;
+constexpr float kPiF = 3.14159265358979f;
+
+// Hawkins-Cramer-Truhlar pairwise descreening integral of atom i (offset
+// radius rti) by a partner sphere of scaled radius sj at distance r (the
+// standard closed form of the 1/r^4 volume integral outside atom i).
+__device__ __forceinline__ float hct_term(float r, float rti, float sj) {
+  if (!(rti < r + sj)) return 0.0f;
+  const float l = fmaxf(rti, fabsf(r - sj)), u = r + sj;
+  const float il = 1.0f / l, iu = 1.0f / u, ir = 1.0f / r;
+  float t = 0.5f * (il - iu + 0.25f * r * (iu * iu - il * il) + 0.5f * ir * __logf(l * iu) +
+                    0.25f * sj * sj * ir * (il * il - iu * iu));
+  if (rti < sj - r) t += 2.0f * (1.0f / rti - il);
+  return t;
+}
+
+__device__ __forceinline__ void add_shells(float* acc, float r, float w) {
+#pragma unroll
+  for (int s = 0; s < 16; ++s) {
+    const float d = r - (kMu0 + kShell * s);
+    acc[s] += w * __expf(-d * d * kInv2Sigma2);
+  }
+}
+
+// One warp per tile of 32 i-atoms; j tiles of the same system whose bounding
+// spheres come within the cutoff are broadcast one atom at a time, so the
+// partner's class -- and the accumulator block it feeds -- is warp-uniform.
+__global__ void __launch_bounds__(128) k_lgb_desc(LgbDescArgs a) {
+  const int ti = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (ti >= (a.n_padded >> 5)) return;
+  const int i = ti * 32 + lane;
+  const bool live_i = a.atom_sys[i] >= 0;
+  const int sys = a.atom_sys[ti * 32];
+  const double4 oi = a.origin[ti];
+  const float xi = live_i ? static_cast<float>(a.x[i] - oi.x) : 0.0f;
+  const float yi = live_i ? static_cast<float>(a.y[i] - oi.y) : 0.0f;
+  const float zi = live_i ? static_cast<float>(a.z[i] - oi.z) : 0.0f;
+  const float rti = live_i ? static_cast<float>(a.rho_tilde[i]) : 1.0f;
+  float acc[64];
+#pragma unroll
+  for (int k = 0; k < 64; ++k) acc[k] = 0.0f;
+  float cfa = 0.0f;
+  if (sys >= 0) {
+    const int2 st = a.sys_tiles[sys];
+    for (int tj = st.x; tj < st.x + st.y; ++tj) {
+      const double4 oj = a.origin[tj];
+      const double ddx = oj.x - oi.x, ddy = oj.y - oi.y, ddz = oj.z - oi.z;
+      const double lim = oi.w + oj.w + kLgbCutoff + 1e-3;
+      if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) continue;
+      const int j = tj * 32 + lane;
+      const bool live_j = a.atom_sys[j] >= 0;
+      const float xj = live_j ? static_cast<float>(a.x[j] - oi.x) : 0.0f;
+      const float yj = live_j ? static_cast<float>(a.y[j] - oi.y) : 0.0f;
+      const float zj = live_j ? static_cast<float>(a.z[j] - oi.z) : 0.0f;
+      const float wj = live_j ? static_cast<float>(a.rho[j]) : 0.0f;
+      const float sj = live_j ? static_cast<float>(a.srho[j]) : 0.0f;
+      const int cj = live_j ? a.klass[j] : -1;
+      for (int b = 0; b < 32; ++b) {
+        const int cb = __shfl_sync(kFull, cj, b);
+        if (cb < 0) continue;  // padding partner (warp-uniform)
+        const float dx = __shfl_sync(kFull, xj, b) - xi;
+        const float dy = __shfl_sync(kFull, yj, b) - yi;
+        const float dz = __shfl_sync(kFull, zj, b) - zi;
+        const float wb = __shfl_sync(kFull, wj, b);
+        const float sb = __shfl_sync(kFull, sj, b);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const bool ok = live_i && r2 < kCut * kCut && !(tj == ti && b == lane);
+        const float r = sqrtf(r2);
+        const float fc = ok ? 0.5f * (__cosf(kPiF * r / kCut) + 1.0f) : 0.0f;
+        const float w = wb * fc;
+        if (ok) cfa += fc * hct_term(r, rti, sb);
+        switch (cb) {
+          case 0: add_shells(acc + 0, r, w); break;
+          case 1: add_shells(acc + 16, r, w); break;
+          case 2: add_shells(acc + 32, r, w); break;
+          default: add_shells(acc + 48, r, w); break;
+        }
+      }
+    }
+  }
+  if (i < a.n_padded) {
+    float4* out = reinterpret_cast<float4*>(a.xin + static_cast<int64_t>(i) * 64);
+#pragma unroll
+    for (int k = 0; k < 64; k += 4)
+      out[k / 4] = live_i ? make_float4(log1pf(acc[k]), log1pf(acc[k + 1]), log1pf(acc[k + 2]), log1pf(acc[k + 3]))
+                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    double rc = 1.0;
+    if (live_i) {
+      const double inv = fmax(1.0 / a.rho_tilde[i] - static_cast<double>(cfa), 1.0 / 30.0);
+      rc = 1.0 / inv;
+    }
+    a.r_cfa[i] = rc;
+  }
+}
+
+__global__ void k_lgb_radii(AtomArrays at, const float* h3, const float* params, const double* r_cfa) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= at.n_padded || at.atom_sys[i] < 0) return;
+  const float* w4 = params + kLgbOffW4;
+  const float4* h = reinterpret_cast<const float4*>(h3 + static_cast<int64_t>(i) * kLgbHidden);
+  float y = params[kLgbOffB4];
+#pragma unroll 8
+  for (int k = 0; k < kLgbHidden / 4; ++k) {
+    const float4 v = h[k];
+    y += w4[4 * k] * v.x + w4[4 * k + 1] * v.y + w4[4 * k + 2] * v.z + w4[4 * k + 3] * v.w;
+  }
+  y = fminf(fmaxf(y, -5.0f), 5.0f);
+  const double r = r_cfa[i] * exp(static_cast<double>(y));
+  at.born_r[i] = r;
+  at.gb[soa_index(i, 0)] = static_cast<float>(r);
+  at.gb[soa_index(i, 1)] = static_cast<float>(1.0 / r);
+}
+
+__global__ void k_lgb_gather(const float* x, const float* t, const int64_t* idx, int b, float* xb, float* tb) {
+  const int r = blockIdx.x;
+  if (r >= b) return;
+  const int64_t src = idx[r];
+  if (threadIdx.x < kLgbIn) xb[static_cast<int64_t>(r) * kLgbIn + threadIdx.x] = x[src * kLgbIn + threadIdx.x];
+  if (threadIdx.x == 0) tb[r] = t[src];
+}
+
+__device__ __forceinline__ float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+__global__ void k_lgb_head(const float* h3, const float* z3, const float* tb, const float* params, int b, float* y,
+                           float* dy, float* dz3, float* loss_part) {
+  __shared__ float red[256];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const float* w4 = params + kLgbOffW4;
+  float l = 0.0f;
+  if (r < b) {
+    float v = params[kLgbOffB4];
+    for (int k = 0; k < kLgbHidden; ++k) v += w4[k] * h3[static_cast<int64_t>(r) * kLgbHidden + k];
+    const float d = v - tb[r];
+    l = d * d;
+    const float g = 2.0f * d / static_cast<float>(b);
+    y[r] = v;
+    dy[r] = g;
+    for (int k = 0; k < kLgbHidden; ++k) {
+      const int64_t o = static_cast<int64_t>(r) * kLgbHidden + k;
+      dz3[o] = g * w4[k] * silu_grad(z3[o]);
+    }
+  }
+  red[threadIdx.x] = l;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss_part[blockIdx.x] = red[0];
+}
+
+// Block k sums column k (k = 128: the column of ones) over the rows.
+__global__ void k_lgb_colsum(const float* m, const float* dy, int b, int cols, float* g) {
+  __shared__ float red[256];
+  const int k = blockIdx.x;
+  float s = 0.0f;
+  for (int r = threadIdx.x; r < b; r += blockDim.x)
+    s += (dy ? dy[r] : 1.0f) * (k < cols ? m[static_cast<int64_t>(r) * cols + k] : 1.0f);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int t = blockDim.x / 2; t > 0; t >>= 1) {
+    if (threadIdx.x < t) red[threadIdx.x] += red[threadIdx.x + t];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) g[k] = red[0];
+}
+
+__global__ void k_lgb_silu_bwd(const float* dh, const float* z, int64_t n, float* dz) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dz[t] = dh[t] * silu_grad(z[t]);
+}
+
+__global__ void k_lgb_adam(float* p, const float* g, float* m, float* v, int n, float lr, float c1, float c2) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float gt = g[t];
+  const float mt = 0.9f * m[t] + 0.1f * gt;
+  const float vt = 0.999f * v[t] + 0.001f * gt * gt;
+  m[t] = mt;
+  v[t] = vt;
+  p[t] -= lr * (mt / c1) / (sqrtf(vt / c2) + 1e-8f);
+}
+
+__global__ void k_lgb_force_error(const unsigned long long* fax, const unsigned long long* fay,
+                                  const unsigned long long* faz, const unsigned long long* fbx,
+                                  const unsigned long long* fby, const unsigned long long* fbz,
+                                  const int32_t* begin, const int32_t* end, double* part) {
+  __shared__ double rn[256], rd[256];
+  const int s = blockIdx.x;
+  double num = 0.0, den = 0.0;
+  auto f = [](unsigned long long v) { return static_cast<double>(static_cast<long long>(v)) * kForceUnscale; };
+  for (int i = begin[s] + threadIdx.x; i < end[s]; i += blockDim.x) {
+    const double bx = f(fbx[i]), by = f(fby[i]), bz = f(fbz[i]);
+    const double dx = f(fax[i]) - bx, dy = f(fay[i]) - by, dz = f(faz[i]) - bz;
+    num += dx * dx + dy * dy + dz * dz;
+    den += bx * bx + by * by + bz * bz;
+  }
+  rn[threadIdx.x] = num;
+  rd[threadIdx.x] = den;
+  __syncthreads();
+  for (int t = blockDim.x / 2; t > 0; t >>= 1) {
+    if (threadIdx.x < t) {
+      rn[threadIdx.x] += rn[threadIdx.x + t];
+      rd[threadIdx.x] += rd[threadIdx.x + t];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * s] = rn[0];
+    part[2 * s + 1] = rd[0];
+  }
+}
+
+__global__ void k_lgb_sum(const float* part, int n, float* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float s = 0.0f;
+  for (int k = 0; k < n; ++k) s += part[k];
+  *out = s;
+}
+
+}  // namespace
+
+void launch_lgb_descriptors(const LgbDescArgs& a, cudaStream_t s) {
+  const int tiles = a.n_padded >> 5;
+  k_lgb_desc<<<(tiles + 3) / 4, 128, 0, s>>>(a);
+}
+
+void launch_lgb_radii(const AtomArrays& at, const float* h3, const float* params, const double* r_cfa,
+                      cudaStream_t s) {
+  k_lgb_radii<<<(at.n_padded + 255) / 256, 256, 0, s>>>(at, h3, params, r_cfa);
+}
+
+void launch_lgb_gather(const float* x, const float* t, const int64_t* idx, int b, float* xb, float* tb,
+                       cudaStream_t s) {
+  k_lgb_gather<<<b, kLgbIn, 0, s>>>(x, t, idx, b, xb, tb);
+}
+
+void launch_lgb_head(const float* h3, const float* z3, const float* tb, const float* params, int b, float* y,
+                     float* dy, float* dz3, float* loss_part, int loss_blocks, cudaStream_t s) {
+  k_lgb_head<<<loss_blocks, 256, 0, s>>>(h3, z3, tb, params, b, y, dy, dz3, loss_part);
+}
+
+void launch_lgb_head_grad(const float* h3, const float* dy, int b, float* g_w4b4, cudaStream_t s) {
+  k_lgb_colsum<<<kLgbHidden + 1, 256, 0, s>>>(h3, dy, b, kLgbHidden, g_w4b4);
+}
+
+void launch_lgb_colsum(const float* dz, int b, float* g, cudaStream_t s) {
+  k_lgb_colsum<<<kLgbHidden, 256, 0, s>>>(dz, nullptr, b, kLgbHidden, g);
+}
+
+void launch_lgb_silu_bwd(const float* dh, const float* z, int64_t n, float* dz, cudaStream_t s) {
+  k_lgb_silu_bwd<<<148 * 8, 256, 0, s>>>(dh, z, n, dz);
+}
+
+void launch_lgb_adam(float* p, const float* g, float* m, float* v, int n, float lr, int t, cudaStream_t s) {
+  const float c1 = 1.0f - powf(0.9f, static_cast<float>(t));
+  const float c2 = 1.0f - powf(0.999f, static_cast<float>(t));
+  k_lgb_adam<<<(n + 255) / 256, 256, 0, s>>>(p, g, m, v, n, lr, c1, c2);
+}
+
+void launch_lgb_sum(const float* part, int n, float* out, cudaStream_t s) { k_lgb_sum<<<1, 32, 0, s>>>(part, n, out); }
+
+void launch_lgb_force_error(const unsigned long long* fax, const unsigned long long* fay,
+                            const unsigned long long* faz, const unsigned long long* fbx,
+                            const unsigned long long* fby, const unsigned long long* fbz, const int32_t* begin,
+                            const int32_t* end, int n_sys, double* part, cudaStream_t s) {
+  k_lgb_force_error<<<n_sys, 256, 0, s>>>(fax, fay, faz, fbx, fby, fbz, begin, end, part);
+}
+
+}  // namespace ogk
