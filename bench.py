@@ -195,40 +195,30 @@ def workload_config(args, chain):
             "seed": args.seed}
 
 
-def run_b200(args):
-    import torch
-    import origami_b200 as og
-    ws, rank, local = dist_env()
-    torch.cuda.set_device(local)
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    stream = torch.cuda.current_stream()
-
-    seq, chain = build_workload(og, args.residues, args.seed)
-    if not args.no_relax:
-        relax(og, chain, all_pairs=not args.cutoff)
+def make_engine(og, args, chain, rank: int, born_mode: int, stream):
     mk = og.Params if args.cutoff else og.Params.all_pairs
     params = mk(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1000 * rank,
-                include_sasa=not args.no_sasa, sasa_gamma_scale=args.sasa_gamma_scale)
+                include_sasa=not args.no_sasa, sasa_gamma_scale=args.sasa_gamma_scale, born_mode=born_mode)
     eng = og.Engine(params)
-    x0 = chain.positions
     for _ in range(args.replicas):
-        eng.add_system(chain, x0, 310.0)
+        eng.add_system(chain, chain.positions, 310.0)
     eng.finalize()
     eng.set_stream(stream.cuda_stream)
     for r in range(args.replicas):
         eng.init_velocities(r, (args.seed + r * 0xC0FFEE) & og.Xoshiro256pp.M, remove_com=False)
+    return eng
 
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+def timed_steps(eng, args, stream, flush, local, ws):
+    """Warm-up, then K steps each bracketed by CUDA events on the engine's
+    stream after an L2 flush; max over ranks.  Returns (ms/step, clocks)."""
+    import torch
     for _ in range(args.warmup):
         eng.step(1)
     torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with Clocks(local) as clk:
         for k in range(args.steps):
@@ -237,26 +227,111 @@ def run_b200(args):
             eng.step(1)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = sum(step_ms)
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
     if ws > 1:
         t = torch.tensor([total_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
+    return total_ms / args.steps, clk.summary
+
+
+def train_network(og, args, stream):
+    """The network's training set: plain-GB (+ SASA) Langevin frames of 64
+    replicas of a seeded 60-residue chain (the 60-residue configuration),
+    every descriptor row with its log(R_plainGB / R_cfa) target; Adam on the
+    GPU.  Untimed set-up."""
+    from origami_b200 import lgb
+    t0 = time.perf_counter()
+    seq = seeded_sequence(60, args.seed + 1)
+    chain = og.Chain.build(seq)
+    relax(og, chain, all_pairs=True, max_steps=200)
+    p = og.Params.all_pairs(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 77,
+                            include_sasa=not args.no_sasa, sasa_gamma_scale=args.sasa_gamma_scale)
+    eng = og.Engine(p)
+    for _ in range(64):
+        eng.add_system(chain, chain.positions, 310.0)
+    eng.finalize()
+    eng.set_stream(stream.cuda_stream)
+    for r in range(64):
+        eng.init_velocities(r, (args.seed + 5 + r * 0xC0FFEE) & og.Xoshiro256pp.M, remove_com=False)
+    xs, ts = [], []
+    for _ in range(args.train_frames):
+        eng.step(args.train_stride)
+        x, t = lgb.samples(eng, -1)
+        xs.append(x)
+        ts.append(t)
+    eng.close()
+    x, t = np.concatenate(xs), np.concatenate(ts)
+    t1 = time.perf_counter()
+    params, hist = lgb.train(x, t, lgb.init_params(args.seed + 3), steps=args.train_steps, batch=8192,
+                             lr=2e-3, seed=args.seed + 4)
+    t2 = time.perf_counter()
+    return params, {"samples": int(x.shape[0]), "frames": args.train_frames * 64, "chain_atoms": chain.n_atoms,
+                    "steps": args.train_steps, "batch": 8192, "lr": 2e-3, "loss_first": float(hist[:20].mean()),
+                    "loss_last": float(hist[-50:].mean()), "sampling_s": t1 - t0, "training_s": t2 - t1}
+
+
+def run_b200(args):
+    import torch
+    import origami_b200 as og
+    from origami_b200 import lgb
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    seq, chain = build_workload(og, args.residues, args.seed)
+    if not args.no_relax:
+        relax(og, chain, all_pairs=not args.cutoff)
     atoms = chain.n_atoms
+    pairs = args.replicas * atoms * (atoms - 1) / 2
+
+    # ---- plain GB arm
+    plain = make_engine(og, args, chain, rank, 0, stream)
+    plain_ms, plain_clk = timed_steps(plain, args, stream, flush, local, ws)
+    plain.profile(True)
+    plain.step(5)
+    prof = plain.profile_read()
+    plain.profile(False)
+    plain.close()
+    plain_value = ws * args.replicas * args.dt * 1e-6 / (plain_ms * 1e-3) * 86400.0
+
+    # ---- learned GB arm (the headline): network trained on the GPU first
+    learned_info = None
+    if not args.plain_only:
+        params, train_info = train_network(og, args, stream)
+        eng = make_engine(og, args, chain, rank, 1, stream)
+        lgb.set_params(eng, params)
+        lgb.set_judge(eng, args.judge_interval, 1e-3)
+        torch.cuda.synchronize()
+        tj = time.perf_counter()
+        judge_err = lgb.judge(eng)  # also the judge's cost, amortised below
+        torch.cuda.synchronize()
+        judge_ms = (time.perf_counter() - tj) * 1e3
+        learned_ms, clk = timed_steps(eng, args, stream, flush, local, ws)
+        st = lgb.status(eng)
+        eff_ms = learned_ms + (judge_ms / args.judge_interval if args.judge_interval > 0 else 0.0)
+        eng.profile(True)
+        eng.step(5)
+        lprof = eng.profile_read()
+        eng.profile(False)
+        learned_info = {"ms_per_step_steps_only": learned_ms, "judge_ms": judge_ms,
+                        "judge_interval": args.judge_interval, "judge_rms_rel_force_error": judge_err,
+                        "judge_tolerance": 1e-3, "active_after_timing": st["active"], "judges": st["judged"],
+                        "training": train_info,
+                        "kernels_ms_per_step": {k: v[0] / v[1] for k, v in lprof.items()}}
+        ms_per_step = eff_ms
+    else:
+        eng = make_engine(og, args, chain, rank, 0, stream)
+        ms_per_step, clk = plain_ms, plain_clk
     value = ws * args.replicas * args.dt * 1e-6 / (ms_per_step * 1e-3) * 86400.0
 
-    # ---- kernel breakdown (profile mode: CUDA events around every launch)
-    eng.profile(True)
-    prof_steps = 5
-    eng.step(prof_steps)
-    prof = eng.profile_read()
-    eng.profile(False)
     force_ms = prof["force_pass"][0] / prof["force_pass"][1]
     born_ms = prof["born_pass"][0] / prof["born_pass"][1]
-    pairs = args.replicas * atoms * (atoms - 1) / 2
-    peak = og.lib()
     import ctypes as C
     tf = C.c_double()
     og._check(og.lib().og_measure_fp32_peak(C.byref(tf)))
@@ -264,7 +339,7 @@ def run_b200(args):
     force_tflops = 55 * pairs / (force_ms * 1e-3) / 1e12
     born_tflops = 60 * pairs / (born_ms * 1e-3) / 1e12
 
-    # ---- end to end through the C ABI with host buffers
+    # ---- end to end through the C ABI with host buffers (headline arm)
     e2e_steps = max(3, min(args.steps, 20))
     hx = [np.ascontiguousarray(eng.positions(r)) for r in range(args.replicas)]
     hv = [np.ascontiguousarray(eng.velocities(r)) for r in range(args.replicas)]
@@ -285,25 +360,33 @@ def run_b200(args):
         e2e_s = float(t.item())
     e2e = ws * args.replicas * args.dt * 1e-6 / e2e_s * 86400.0
 
-    shake_on = 1
-    launches_per_step = 9 + 2 * shake_on + (0 if args.no_sasa else 2)
+    sasa_k = 0 if args.no_sasa else 2
+    launches_plain = 9 + 2 + sasa_k
+    launches_learned = 7 + 2 + 5 + sasa_k  # descriptors, 3 GEMM layers, radii instead of Born pass + finalize
+    launches = launches_plain if args.plain_only else launches_learned
+    cfg = workload_config(args, chain)
+    cfg["born"] = "plain OBC-II pass" if args.plain_only else "learned radii (network on tcgen05 GEMMs), plain-GB judge"
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "precision": "FP32 pair math, FP64 tile sums, int64 fixed-point forces, FP64 integrator",
-        "data": "synthetic", "config": workload_config(args, chain),
+        "dtype": "f32", "precision": "FP32 pair math, FP64 tile sums, int64 fixed-point forces, FP64 integrator; "
+                                      "network BF16 tensor-core products, FP32 accumulate",
+        "data": "synthetic", "config": cfg,
+        "plain_gb": {"value": plain_value, "unit": "ns/day", "ms_per_step": plain_ms,
+                     "kernels_ms_per_step": {k: v[0] / v[1] for k, v in prof.items()}, "clocks": plain_clk},
+        "learned_vs_plain": (value / plain_value) if not args.plain_only else None,
+        "learned_gb": learned_info,
         "roofline": {"bound": "fp32", "kernel": "force_pass", "achieved": force_tflops, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": force_tflops / fp32_peak, "traffic": None,
                      "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak)",
                      "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
-        "kernels_ms_per_step": {k: v[0] / v[1] for k, v in prof.items()},
-        "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / ms_per_step) if "sasa" in prof else None,
+        "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / plain_ms) if "sasa" in prof else None,
         "born_pass_tflops": born_tflops,
         "pair_interactions_per_s": pairs / (ms_per_step * 1e-3) * ws,
         "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": args.replicas * atoms * 6 * 8,
                 "d2h_bytes_per_step": args.replicas * atoms * 3 * 8},
-        "gpu_launches": args.steps * launches_per_step,
-        "clocks": clk.summary,
+        "gpu_launches": args.steps * launches,
+        "clocks": clk,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(chain, args.dt, args.replicas, budget_s=args.cpu_budget,
@@ -330,6 +413,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-sasa", action="store_true", help="leave out the PowerSasa surface term")
+    ap.add_argument("--plain-only", action="store_true", help="time the plain-GB engine only (no network)")
+    ap.add_argument("--judge-interval", type=int, default=500)
+    ap.add_argument("--train-frames", type=int, default=16)
+    ap.add_argument("--train-stride", type=int, default=50)
+    ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--sasa-gamma-scale", type=float, default=0.25)
     ap.add_argument("--no-relax", action="store_true",
                     help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")

@@ -316,17 +316,26 @@ og_status og_tc_gemm(const float* a, int64_t a_sm, int64_t a_sk, const float* b,
  * tensor-core products, FP32 accumulate) predicts y = log(R / R_cfa), R_cfa
  * the Coulomb-field radius in its pairwise (HCT) form over the same 12 A
  * neighbours: 1/R_cfa = max(1/rho~ - sum fc I_HCT(r, rho~_i, s_j rho~_j),
- * 1/30).  Parameters: OG_LGB_N_PARAMS floats, W1[128x64] b1[128] W2[128x128]
- * b2[128] W3[128x128] b3[128] w4[128] b4 (W row-major, out x in).  Forces use
+ * 1/30).  The network input is OG_LGB_N_INPUT = 80 wide: the 64
+ * descriptors, then the atom's own class one-hot (4), rho~, HCT scale,
+ * rho~/R_cfa, log R_cfa, 0, log(rho~/R_cfa) and 6 zeros; the output adds a
+ * linear FP32 term v . x[64..80) to the network's.  Parameters:
+ * OG_LGB_N_PARAMS floats, W1[128x80] b1[128] W2[128x128]
+ * b2[128] W3[128x128] b3[128] w4[128] b4 v[16] (W row-major, out x in).  Forces use
  * the predicted radii frozen, like the plain pass's.  Energies
  * (og_compute_energies) stay plain GB. */
-#define OG_LGB_N_PARAMS 41473
-#define OG_LGB_N_DESC 64
+#define OG_LGB_N_PARAMS 43537
+#define OG_LGB_N_INPUT 80
 
-/* Uniform(+-1/sqrt(fan_in)) weights, zero biases, from `seed`. */
+/* Uniform(+-1/sqrt(fan_in)) hidden weights, zero biases, zero output
+ * weights w4 and v (the untrained network predicts y = 0, i.e. R = R_cfa),
+ * from `seed`. */
 og_status og_lgb_init_params(uint64_t seed, float* params);
-/* Minibatch Adam (beta 0.9 / 0.999) on the mean squared error of y over
- * host samples x[n x 64], target[n]; params updated in place;
+/* Training: the linear path (v, b4) is first set by an FP64 least-squares
+ * fit over all samples, then minibatch Adam (beta 0.9 / 0.999, step size lr
+ * with cosine decay to 0 over `steps`) trains every parameter on the mean
+ * squared error of y over
+ * host samples x[n x 80], target[n]; params updated in place;
  * loss_per_step (optional) receives each step's batch loss. */
 og_status og_lgb_train(const float* x, const float* target, int64_t n, int32_t steps, int32_t batch, double lr,
                        uint64_t seed, float* params, float* loss_per_step);
@@ -334,9 +343,10 @@ og_status og_lgb_train(const float* x, const float* target, int64_t n, int32_t s
  * samples in one batch (n <= 2^20), by the same kernels. */
 og_status og_lgb_loss_and_gradient(const float* x, const float* target, int64_t n, const float* params,
                                    double* loss, float* grad);
-/* Training samples of system `sys` at its current positions: x_out
- * (n_atoms x 64, log(1 + D)) and target_out (n_atoms) = log(R_plain / R_cfa)
- * with R_plain the FP64 plain-GB radii.  Any born_mode. */
+/* Training samples of system `sys` (or of every system, in order, when
+ * sys = -1) at the current positions: x_out (n_atoms x 80 network inputs) and
+ * target_out (n_atoms) = log(R_plain / R_cfa) with R_plain the FP64
+ * plain-GB radii.  Any born_mode. */
 og_status og_lgb_samples(og_engine* e, int32_t sys, float* x_out, float* target_out);
 /* Loads the network (born_mode = 1 engines); required before stepping. */
 og_status og_lgb_set_params(og_engine* e, const float* params);

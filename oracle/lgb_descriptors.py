@@ -3,8 +3,11 @@
 NumPy float64 restatement of the learned-Born-radius inputs defined in
 include/origami_gpu.h: the 64 environment descriptors (16 Gaussian shells x
 4 element classes, partner-radius weighted, cosine cutoff at 12 A) as
-x = log(1 + D), and the Coulomb-field radius in its pairwise
-(Hawkins-Cramer-Truhlar) form 1/R_cfa = max(1/rho~_i - sum_j fc I_HCT, 1/30).
+x = log(1 + D) followed by the 16 self features (class one-hot, rho~, HCT
+scale, rho~/R_cfa, log R_cfa, 0, log(rho~/R_cfa), zeros), and the
+Coulomb-field radius in its
+pairwise (Hawkins-Cramer-Truhlar) form 1/R_cfa = max(1/rho~_i - sum_j fc
+I_HCT, 1/30).
 These are this project's definitions (the reference has no learned radii).
 """
 from __future__ import annotations
@@ -48,5 +51,13 @@ def descriptors(xyz: np.ndarray, element: np.ndarray, rho: np.ndarray, rho_tilde
     sj = np.asarray(srho)[None, :]
     rr = np.where(mask, r, 1.0)
     cfa = np.where(mask, fc * hct(rr, rti + 0 * rr, sj + 0 * rr), 0.0).sum(1)
-    rcfa = 1.0 / np.maximum(1.0 / np.asarray(rho_tilde) - cfa, 1.0 / 30.0)
-    return np.log1p(d), rcfa
+    rt = np.asarray(rho_tilde, dtype=np.float64)
+    rcfa = 1.0 / np.maximum(1.0 / rt - cfa, 1.0 / 30.0)
+    selfx = np.zeros((n, 16))
+    selfx[np.arange(n), cls] = 1.0
+    selfx[:, 4] = rt
+    selfx[:, 5] = np.asarray(srho) / rt
+    selfx[:, 6] = rt / rcfa
+    selfx[:, 7] = np.log(rcfa)
+    selfx[:, 9] = np.log(rt / rcfa)
+    return np.concatenate([np.log1p(d), selfx], axis=1), rcfa

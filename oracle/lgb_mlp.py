@@ -12,7 +12,9 @@ from __future__ import annotations
 
 import numpy as np
 
-HIDDEN, N_DESC = 128, 64
+HIDDEN, N_INPUT = 128, 80
+N_SELF = N_INPUT - 64
+N_PARAMS = HIDDEN * N_INPUT + HIDDEN + 2 * (HIDDEN * HIDDEN + HIDDEN) + HIDDEN + 1 + N_SELF
 
 
 def bf16(a: np.ndarray) -> np.ndarray:
@@ -34,8 +36,9 @@ def silu_grad(z):
 def unpack(p: np.ndarray) -> dict:
     p = np.asarray(p, dtype=np.float64)
     o, d = 0, {}
-    for name, shape in (("W1", (HIDDEN, N_DESC)), ("b1", (HIDDEN,)), ("W2", (HIDDEN, HIDDEN)), ("b2", (HIDDEN,)),
-                        ("W3", (HIDDEN, HIDDEN)), ("b3", (HIDDEN,)), ("w4", (HIDDEN,)), ("b4", (1,))):
+    for name, shape in (("W1", (HIDDEN, N_INPUT)), ("b1", (HIDDEN,)), ("W2", (HIDDEN, HIDDEN)), ("b2", (HIDDEN,)),
+                        ("W3", (HIDDEN, HIDDEN)), ("b3", (HIDDEN,)), ("w4", (HIDDEN,)), ("b4", (1,)),
+                        ("v", (N_SELF,))):
         n = int(np.prod(shape))
         d[name] = p[o:o + n].reshape(shape)
         o += n
@@ -50,7 +53,7 @@ def forward(p: np.ndarray, x: np.ndarray) -> dict:
     h2 = silu(z2)
     z3 = bf16(h2) @ bf16(w["W3"]).T + w["b3"]
     h3 = silu(z3)
-    y = h3 @ w["w4"] + w["b4"][0]
+    y = h3 @ w["w4"] + w["b4"][0] + np.asarray(x, np.float64)[:, 64:] @ w["v"]
     return {"x": x, "z1": z1, "h1": h1, "z2": z2, "h2": h2, "z3": z3, "h3": h3, "y": y}
 
 
@@ -61,7 +64,7 @@ def loss_and_gradient(p: np.ndarray, x: np.ndarray, t: np.ndarray) -> tuple[floa
     d = f["y"] - t
     loss = float(np.mean(d * d))
     dy = 2.0 * d / b
-    g = {"w4": dy @ f["h3"], "b4": np.array([dy.sum()])}
+    g = {"w4": dy @ f["h3"], "b4": np.array([dy.sum()]), "v": dy @ np.asarray(x, np.float64)[:, 64:]}
     dz3 = dy[:, None] * w["w4"][None, :] * silu_grad(f["z3"])
     g["b3"] = dz3.sum(0)
     g["W3"] = bf16(dz3).T @ bf16(f["h2"])
@@ -71,5 +74,5 @@ def loss_and_gradient(p: np.ndarray, x: np.ndarray, t: np.ndarray) -> tuple[floa
     dz1 = (bf16(dz2) @ bf16(w["W2"])) * silu_grad(f["z1"])
     g["b1"] = dz1.sum(0)
     g["W1"] = bf16(dz1).T @ bf16(x)
-    flat = np.concatenate([g[k].ravel() for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4")])
+    flat = np.concatenate([g[k].ravel() for k in ("W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4", "v")])
     return loss, flat

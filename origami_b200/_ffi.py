@@ -13,8 +13,8 @@ c_int8_p = C.POINTER(C.c_int8)
 c_float_p = C.POINTER(C.c_float)
 
 OG_OK = 0
-LGB_N_PARAMS = 41473  # OG_LGB_N_PARAMS
-LGB_N_DESC = 64       # OG_LGB_N_DESC
+LGB_N_PARAMS = 43537  # OG_LGB_N_PARAMS
+LGB_N_INPUT = 80      # OG_LGB_N_INPUT
 STATUS_NAMES = {
     0: "OG_OK", 1: "OG_E_BADARG", 2: "OG_E_NONFINITE", 3: "OG_E_SHAKE", 4: "OG_E_TIMEOUT",
     5: "OG_E_CUDA", 6: "OG_E_NOMEM", 7: "OG_E_STATE", 8: "OG_E_DATA", 9: "OG_E_UNSUPPORTED",

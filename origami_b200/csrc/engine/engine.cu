@@ -218,6 +218,10 @@ struct og_engine {
   DVec<double> lgb_rcfa, lgb_part;
   DVec<unsigned long long> lgb_fx, lgb_fy, lgb_fz;
   bool lgb_params_set = false, lgb_active = false;
+  // the network as three GEMM launches + head (OG_LGB_UNFUSED=1) instead of
+  // the fused kernel; both give the same radii
+  bool lgb_unfused = false;
+  int n_sm = 148;
   int lgb_judge_interval = 500, lgb_judged = 0;
   double lgb_tol = 1e-3, lgb_last_err = -1.0;
   int64_t lgb_since_judge = 0;
@@ -421,13 +425,14 @@ struct og_engine {
     }
     {
       Timer t(this, "lgb_network");
-      lgb_layer(lgb_x.p, ogk::kLgbIn, ogk::kLgbOffW1, ogk::kLgbOffB1, lgb_ha.p);
-      lgb_layer(lgb_ha.p, ogk::kLgbHidden, ogk::kLgbOffW2, ogk::kLgbOffB2, lgb_hb.p);
-      lgb_layer(lgb_hb.p, ogk::kLgbHidden, ogk::kLgbOffW3, ogk::kLgbOffB3, lgb_ha.p);
-    }
-    {
-      Timer t(this, "lgb_radii");
-      ogk::launch_lgb_radii(atoms(), lgb_ha.p, lgb_params.p, lgb_rcfa.p, stream);
+      if (lgb_unfused) {
+        lgb_layer(lgb_x.p, ogk::kLgbIn, ogk::kLgbOffW1, ogk::kLgbOffB1, lgb_ha.p);
+        lgb_layer(lgb_ha.p, ogk::kLgbHidden, ogk::kLgbOffW2, ogk::kLgbOffB2, lgb_hb.p);
+        lgb_layer(lgb_hb.p, ogk::kLgbHidden, ogk::kLgbOffW3, ogk::kLgbOffB3, lgb_ha.p);
+        ogk::launch_lgb_radii(atoms(), lgb_ha.p, lgb_x.p, lgb_params.p, lgb_rcfa.p, stream);
+      } else {
+        ogk::launch_lgb_mlp_radii(atoms(), lgb_x.p, lgb_params.p, lgb_rcfa.p, error_flag.p, n_sm, stream);
+      }
     }
   }
 
@@ -814,6 +819,12 @@ og_status finalize_impl(og_engine* e) {
       for (int k = 0; k < e->sys[si].topo.n; ++k) hc[e->sys[si].atom_begin + k] = kClass[e->sys[si].topo.element[k]];
     OG_CUDA(e->lgb_class.upload(hc, st));
     OG_CUDA(ogk::tc_gemm_prepare());
+    OG_CUDA(ogk::lgb_mlp_prepare());
+    int dev = 0;
+    OG_CUDA(cudaGetDevice(&dev));
+    OG_CUDA(cudaDeviceGetAttribute(&e->n_sm, cudaDevAttrMultiProcessorCount, dev));
+    const char* unf = std::getenv("OG_LGB_UNFUSED");
+    e->lgb_unfused = unf && unf[0] == '1';
     if (e->p.born_mode == 1) {
       OG_CUDA(e->lgb_x.alloc(static_cast<size_t>(np) * ogk::kLgbIn));
       OG_CUDA(e->lgb_rcfa.alloc(np));
@@ -1639,29 +1650,41 @@ og_status og_lgb_judge(og_engine* e, double* rms_rel) {
 }
 
 og_status og_lgb_samples(og_engine* e, int32_t s, float* x_out, float* target_out) {
-  og_status st = check_sys(e, s);
+  og_status st = check_ready(e);
   if (st != OG_OK) return st;
+  const int n_sys = static_cast<int>(e->sys.size());
+  if (s < -1 || s >= n_sys) return og_fail(OG_E_BADARG, "system index out of range");
   if (!x_out || !target_out) return og_fail(OG_E_BADARG, "null output");
   const int np = e->n_padded;
   if (!e->lgb_x.p) OG_CUDA(e->lgb_x.alloc(static_cast<size_t>(np) * ogk::kLgbIn));
   if (!e->lgb_rcfa.p) OG_CUDA(e->lgb_rcfa.alloc(np));
-  // plain GB radii of the FP64 energy path (born_r64) at the current positions
-  og_energies en{};
-  if ((st = og_compute_energies(e, s, &en)) != OG_OK) return st;
+  // plain GB radii of the FP64 energy path (born_r64, every system) at the
+  // current positions
+  std::vector<og_energies> en(n_sys);
+  if ((st = og_compute_energies(e, -1, en.data())) != OG_OK) return st;
   ogk::launch_pack(e->atoms(), false, e->stream);
   ogk::launch_lgb_descriptors(e->lgb_desc_args(), e->stream);
   if ((st = launch_check("descriptors")) != OG_OK) return st;
-  const SysHost& sh = e->sys[s];
-  const int n = sh.topo.n;
-  std::vector<double> rc(n), rp(n);
-  OG_CUDA(cudaMemcpyAsync(x_out, e->lgb_x.p + static_cast<size_t>(sh.atom_begin) * ogk::kLgbIn,
-                          sizeof(float) * ogk::kLgbIn * n, cudaMemcpyDeviceToHost, e->stream));
-  OG_CUDA(cudaMemcpyAsync(rc.data(), e->lgb_rcfa.p + sh.atom_begin, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                          e->stream));
-  OG_CUDA(cudaMemcpyAsync(rp.data(), e->born_r64.p + sh.atom_begin, sizeof(double) * n, cudaMemcpyDeviceToHost,
-                          e->stream));
+  std::vector<double> rc(np), rp(np);
+  OG_CUDA(cudaMemcpyAsync(rc.data(), e->lgb_rcfa.p, sizeof(double) * np, cudaMemcpyDeviceToHost, e->stream));
+  OG_CUDA(cudaMemcpyAsync(rp.data(), e->born_r64.p, sizeof(double) * np, cudaMemcpyDeviceToHost, e->stream));
+  size_t row = 0;
+  for (int k = 0; k < n_sys; ++k) {
+    if (s >= 0 && k != s) continue;
+    const SysHost& sh = e->sys[k];
+    OG_CUDA(cudaMemcpyAsync(x_out + row * ogk::kLgbIn, e->lgb_x.p + static_cast<size_t>(sh.atom_begin) * ogk::kLgbIn,
+                            sizeof(float) * ogk::kLgbIn * sh.topo.n, cudaMemcpyDeviceToHost, e->stream));
+    row += sh.topo.n;
+  }
   OG_CUDA(cudaStreamSynchronize(e->stream));
-  for (int k = 0; k < n; ++k) target_out[k] = static_cast<float>(std::log(rp[k] / rc[k]));
+  row = 0;
+  for (int k = 0; k < n_sys; ++k) {
+    if (s >= 0 && k != s) continue;
+    const SysHost& sh = e->sys[k];
+    for (int a = 0; a < sh.topo.n; ++a)
+      target_out[row + a] = static_cast<float>(std::log(rp[sh.atom_begin + a] / rc[sh.atom_begin + a]));
+    row += sh.topo.n;
+  }
   return OG_OK;
 }
 

@@ -118,8 +118,9 @@ struct Trainer {
     gemm(xb.p, kLgbIn, 1, params + kLgbOffW1, kLgbIn, 1, z1.p, H, b, H, kLgbIn, params + kLgbOffB1, h1.p, 1, s);
     gemm(h1.p, H, 1, params + kLgbOffW2, H, 1, z2.p, H, b, H, H, params + kLgbOffB2, h2.p, 1, s);
     gemm(h2.p, H, 1, params + kLgbOffW3, H, 1, z3.p, H, b, H, H, params + kLgbOffB3, h3.p, 1, s);
-    launch_lgb_head(h3.p, z3.p, tb.p, params, b, y.p, dy.p, dz3.p, loss_part.p, loss_blocks, s);
+    launch_lgb_head(h3.p, z3.p, xb.p, tb.p, params, b, y.p, dy.p, dz3.p, loss_part.p, loss_blocks, s);
     launch_lgb_head_grad(h3.p, dy.p, b, g.p + kLgbOffW4, s);  // w4 and b4 (adjacent)
+    launch_lgb_self_grad(xb.p, dy.p, b, g.p + kLgbOffV, s);
     // layer 3
     launch_lgb_colsum(dz3.p, b, g.p + kLgbOffB3, s);
     gemm(dz3.p, 1, H, h2.p, 1, H, g.p + kLgbOffW3, H, H, H, b, nullptr, nullptr, splits, s);
@@ -135,6 +136,53 @@ struct Trainer {
     gemm(dz3.p, 1, H, xb.p, 1, kLgbIn, g.p + kLgbOffW1, kLgbIn, H, kLgbIn, b, nullptr, nullptr, splits, s);
   }
 };
+
+// Least-squares fit of the output's linear path, t ~ b4 + v . x[64..80), by
+// FP64 normal equations with a small ridge term (constant self features make
+// them singular otherwise), solved by Cholesky.
+void fit_linear_path(const float* x, const float* t, int64_t n, float* params) {
+  constexpr int d = kLgbNSelf + 1;  // v and the bias
+  double a[d][d] = {}, rhs[d] = {};
+  double f[d];
+  for (int64_t r = 0; r < n; ++r) {
+    for (int k = 0; k < kLgbNSelf; ++k) f[k] = x[r * kLgbIn + kLgbDesc + k];
+    f[kLgbNSelf] = 1.0;
+    for (int p = 0; p < d; ++p) {
+      rhs[p] += f[p] * t[r];
+      for (int q = 0; q <= p; ++q) a[p][q] += f[p] * f[q];
+    }
+  }
+  double tr = 0.0;
+  for (int p = 0; p < d; ++p) tr += a[p][p];
+  for (int p = 0; p < d; ++p) {
+    a[p][p] += 1e-10 * tr / d + 1e-30;
+    for (int q = p + 1; q < d; ++q) a[p][q] = a[q][p];
+  }
+  // Cholesky a = L L^T in place (lower), then two triangular solves
+  for (int j = 0; j < d; ++j) {
+    double s = a[j][j];
+    for (int k = 0; k < j; ++k) s -= a[j][k] * a[j][k];
+    a[j][j] = std::sqrt(std::max(s, 1e-300));
+    for (int i = j + 1; i < d; ++i) {
+      double u = a[i][j];
+      for (int k = 0; k < j; ++k) u -= a[i][k] * a[j][k];
+      a[i][j] = u / a[j][j];
+    }
+  }
+  double z[d], w[d];
+  for (int i = 0; i < d; ++i) {
+    double u = rhs[i];
+    for (int k = 0; k < i; ++k) u -= a[i][k] * z[k];
+    z[i] = u / a[i][i];
+  }
+  for (int i = d - 1; i >= 0; --i) {
+    double u = z[i];
+    for (int k = i + 1; k < d; ++k) u -= a[k][i] * w[k];
+    w[i] = u / a[i][i];
+  }
+  for (int k = 0; k < kLgbNSelf; ++k) params[kLgbOffV + k] = static_cast<float>(w[k]);
+  params[kLgbOffB4] = static_cast<float>(w[kLgbNSelf]);
+}
 
 og_status check_samples(const float* x, const float* t, int64_t n) {
   if (!x || !t) return og_fail(OG_E_BADARG, "null samples");
@@ -204,10 +252,11 @@ og_status og_lgb_init_params(uint64_t seed, float* params) {
   fill(kLgbOffW1, H * kLgbIn, kLgbIn);
   fill(kLgbOffW2, H * H, H);
   fill(kLgbOffW3, H * H, H);
-  fill(kLgbOffW4, H, H);
+  for (int k = 0; k < H; ++k) params[kLgbOffW4 + k] = 0.0f;  // the network starts at output 0
   for (int off : {kLgbOffB1, kLgbOffB2, kLgbOffB3})
     for (int k = 0; k < H; ++k) params[off + k] = 0.0f;
   params[kLgbOffB4] = 0.0f;
+  for (int k = 0; k < kLgbNSelf; ++k) params[kLgbOffV + k] = 0.0f;
   return OG_OK;
 }
 
@@ -268,6 +317,7 @@ og_status og_lgb_train(const float* x, const float* target, int64_t n, int32_t s
   LGB_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int32_t), s));
   LGB_CUDA(cudaMemsetAsync(m.p, 0, sizeof(float) * kLgbNParams, s));
   LGB_CUDA(cudaMemsetAsync(v.p, 0, sizeof(float) * kLgbNParams, s));
+  fit_linear_path(x, target, n, params);
   LGB_CUDA(cudaMemcpyAsync(p.p, params, sizeof(float) * kLgbNParams, cudaMemcpyHostToDevice, s));
   LGB_CUDA(cudaMemcpyAsync(xd.p, x, sizeof(float) * kLgbIn * n, cudaMemcpyHostToDevice, s));
   LGB_CUDA(cudaMemcpyAsync(td.p, target, sizeof(float) * n, cudaMemcpyHostToDevice, s));
@@ -286,7 +336,9 @@ og_status og_lgb_train(const float* x, const float* target, int64_t n, int32_t s
     cursor += b;
     tr.step(p.p, s);
     launch_lgb_sum(tr.loss_part.p, tr.loss_blocks, hist.p + t - 1, s);
-    launch_lgb_adam(p.p, tr.g.p, m.p, v.p, kLgbNParams, static_cast<float>(lr), t, s);
+    // cosine decay of the step size over the run
+    const double lr_t = lr * 0.5 * (1.0 + std::cos(M_PI * (t - 1) / std::max(steps, 1)));
+    launch_lgb_adam(p.p, tr.g.p, m.p, v.p, kLgbNParams, static_cast<float>(lr_t), t, s);
   }
   LGB_CUDA(cudaGetLastError());
   std::vector<float> h(static_cast<size_t>(steps));

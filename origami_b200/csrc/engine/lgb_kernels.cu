@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(128) k_lgb_desc(LgbDescArgs a) {
         const float sb = __shfl_sync(kFull, sj, b);
         const float r2 = dx * dx + dy * dy + dz * dz;
         const bool ok = live_i && r2 < kCut * kCut && !(tj == ti && b == lane);
+        if (!__any_sync(kFull, ok)) continue;  // partner out of range of the whole tile
         const float r = sqrtf(r2);
         const float fc = ok ? 0.5f * (__cosf(kPiF * r / kCut) + 1.0f) : 0.0f;
         const float w = wb * fc;
@@ -93,26 +94,42 @@ __global__ void __launch_bounds__(128) k_lgb_desc(LgbDescArgs a) {
     }
   }
   if (i < a.n_padded) {
-    float4* out = reinterpret_cast<float4*>(a.xin + static_cast<int64_t>(i) * 64);
-#pragma unroll
-    for (int k = 0; k < 64; k += 4)
-      out[k / 4] = live_i ? make_float4(log1pf(acc[k]), log1pf(acc[k + 1]), log1pf(acc[k + 2]), log1pf(acc[k + 3]))
-                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     double rc = 1.0;
     if (live_i) {
       const double inv = fmax(1.0 / a.rho_tilde[i] - static_cast<double>(cfa), 1.0 / 30.0);
       rc = 1.0 / inv;
     }
     a.r_cfa[i] = rc;
+    float4* out = reinterpret_cast<float4*>(a.xin + static_cast<int64_t>(i) * kLgbIn);
+#pragma unroll
+    for (int k = 0; k < kLgbDesc; k += 4)
+      out[k / 4] = live_i ? make_float4(log1pf(acc[k]), log1pf(acc[k + 1]), log1pf(acc[k + 2]), log1pf(acc[k + 3]))
+                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (live_i) {
+      const int ci = a.klass[i];
+      const double rt = a.rho_tilde[i];
+      out[16] = make_float4(ci == 0 ? 1.0f : 0.0f, ci == 1 ? 1.0f : 0.0f, ci == 2 ? 1.0f : 0.0f, ci == 3 ? 1.0f : 0.0f);
+      out[17] = make_float4(static_cast<float>(rt), static_cast<float>(a.srho[i] / rt), static_cast<float>(rt / rc),
+                            static_cast<float>(log(rc)));
+      out[18] = make_float4(0.0f, static_cast<float>(log(rt / rc)), 0.0f, 0.0f);
+    } else {
+      out[16] = zero;
+      out[17] = zero;
+      out[18] = zero;
+    }
+    out[19] = zero;
   }
 }
 
-__global__ void k_lgb_radii(AtomArrays at, const float* h3, const float* params, const double* r_cfa) {
+__global__ void k_lgb_radii(AtomArrays at, const float* h3, const float* xin, const float* params,
+                            const double* r_cfa) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= at.n_padded || at.atom_sys[i] < 0) return;
   const float* w4 = params + kLgbOffW4;
   const float4* h = reinterpret_cast<const float4*>(h3 + static_cast<int64_t>(i) * kLgbHidden);
   float y = params[kLgbOffB4];
+  for (int k = 0; k < kLgbNSelf; ++k) y += params[kLgbOffV + k] * xin[static_cast<int64_t>(i) * kLgbIn + kLgbDesc + k];
 #pragma unroll 8
   for (int k = 0; k < kLgbHidden / 4; ++k) {
     const float4 v = h[k];
@@ -138,14 +155,15 @@ __device__ __forceinline__ float silu_grad(float z) {
   return s * (1.0f + z * (1.0f - s));
 }
 
-__global__ void k_lgb_head(const float* h3, const float* z3, const float* tb, const float* params, int b, float* y,
-                           float* dy, float* dz3, float* loss_part) {
+__global__ void k_lgb_head(const float* h3, const float* z3, const float* xb, const float* tb, const float* params,
+                           int b, float* y, float* dy, float* dz3, float* loss_part) {
   __shared__ float red[256];
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const float* w4 = params + kLgbOffW4;
   float l = 0.0f;
   if (r < b) {
     float v = params[kLgbOffB4];
+    for (int k = 0; k < kLgbNSelf; ++k) v += params[kLgbOffV + k] * xb[static_cast<int64_t>(r) * kLgbIn + kLgbDesc + k];
     for (int k = 0; k < kLgbHidden; ++k) v += w4[k] * h3[static_cast<int64_t>(r) * kLgbHidden + k];
     const float d = v - tb[r];
     l = d * d;
@@ -166,13 +184,14 @@ __global__ void k_lgb_head(const float* h3, const float* z3, const float* tb, co
   if (threadIdx.x == 0) loss_part[blockIdx.x] = red[0];
 }
 
-// Block k sums column k (k = 128: the column of ones) over the rows.
-__global__ void k_lgb_colsum(const float* m, const float* dy, int b, int cols, float* g) {
+// Block k sums column offset + k of a row-major matrix with `stride` columns
+// (weighted by dy when given; k >= cols: the column of ones) over the rows.
+__global__ void k_lgb_colsum(const float* m, const float* dy, int b, int stride, int offset, int cols, float* g) {
   __shared__ float red[256];
   const int k = blockIdx.x;
   float s = 0.0f;
   for (int r = threadIdx.x; r < b; r += blockDim.x)
-    s += (dy ? dy[r] : 1.0f) * (k < cols ? m[static_cast<int64_t>(r) * cols + k] : 1.0f);
+    s += (dy ? dy[r] : 1.0f) * (k < cols ? m[static_cast<int64_t>(r) * stride + offset + k] : 1.0f);
   red[threadIdx.x] = s;
   __syncthreads();
   for (int t = blockDim.x / 2; t > 0; t >>= 1) {
@@ -243,9 +262,9 @@ void launch_lgb_descriptors(const LgbDescArgs& a, cudaStream_t s) {
   k_lgb_desc<<<(tiles + 3) / 4, 128, 0, s>>>(a);
 }
 
-void launch_lgb_radii(const AtomArrays& at, const float* h3, const float* params, const double* r_cfa,
-                      cudaStream_t s) {
-  k_lgb_radii<<<(at.n_padded + 255) / 256, 256, 0, s>>>(at, h3, params, r_cfa);
+void launch_lgb_radii(const AtomArrays& at, const float* h3, const float* xin, const float* params,
+                      const double* r_cfa, cudaStream_t s) {
+  k_lgb_radii<<<(at.n_padded + 255) / 256, 256, 0, s>>>(at, h3, xin, params, r_cfa);
 }
 
 void launch_lgb_gather(const float* x, const float* t, const int64_t* idx, int b, float* xb, float* tb,
@@ -253,17 +272,21 @@ void launch_lgb_gather(const float* x, const float* t, const int64_t* idx, int b
   k_lgb_gather<<<b, kLgbIn, 0, s>>>(x, t, idx, b, xb, tb);
 }
 
-void launch_lgb_head(const float* h3, const float* z3, const float* tb, const float* params, int b, float* y,
-                     float* dy, float* dz3, float* loss_part, int loss_blocks, cudaStream_t s) {
-  k_lgb_head<<<loss_blocks, 256, 0, s>>>(h3, z3, tb, params, b, y, dy, dz3, loss_part);
+void launch_lgb_head(const float* h3, const float* z3, const float* xb, const float* tb, const float* params, int b,
+                     float* y, float* dy, float* dz3, float* loss_part, int loss_blocks, cudaStream_t s) {
+  k_lgb_head<<<loss_blocks, 256, 0, s>>>(h3, z3, xb, tb, params, b, y, dy, dz3, loss_part);
 }
 
 void launch_lgb_head_grad(const float* h3, const float* dy, int b, float* g_w4b4, cudaStream_t s) {
-  k_lgb_colsum<<<kLgbHidden + 1, 256, 0, s>>>(h3, dy, b, kLgbHidden, g_w4b4);
+  k_lgb_colsum<<<kLgbHidden + 1, 256, 0, s>>>(h3, dy, b, kLgbHidden, 0, kLgbHidden, g_w4b4);
+}
+
+void launch_lgb_self_grad(const float* xb, const float* dy, int b, float* g_v, cudaStream_t s) {
+  k_lgb_colsum<<<kLgbNSelf, 256, 0, s>>>(xb, dy, b, kLgbIn, kLgbDesc, kLgbNSelf, g_v);
 }
 
 void launch_lgb_colsum(const float* dz, int b, float* g, cudaStream_t s) {
-  k_lgb_colsum<<<kLgbHidden, 256, 0, s>>>(dz, nullptr, b, kLgbHidden, g);
+  k_lgb_colsum<<<kLgbHidden, 256, 0, s>>>(dz, nullptr, b, kLgbHidden, 0, kLgbHidden, g);
 }
 
 void launch_lgb_silu_bwd(const float* dh, const float* z, int64_t n, float* dz, cudaStream_t s) {

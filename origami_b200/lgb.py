@@ -1,8 +1,9 @@
 """Learned Born radii: the Python face of the og_lgb_* entries.
 
-The network maps an atom's 64 environment descriptors to
-y = log(R_plainGB / R_cfa); see include/origami_gpu.h for the descriptor,
-the Coulomb-field baseline R_cfa and the parameter layout.
+The network maps an atom's 80 inputs (64 environment descriptors and 16
+features of the atom itself) to y = log(R_plainGB / R_cfa); see
+include/origami_gpu.h for the inputs, the Coulomb-field baseline R_cfa and
+the parameter layout.
 """
 from __future__ import annotations
 
@@ -14,19 +15,21 @@ from . import _ffi as F
 from . import _check, lib
 
 N_PARAMS = F.LGB_N_PARAMS
-N_DESC = F.LGB_N_DESC
+N_INPUT = F.LGB_N_INPUT
 HIDDEN = 128
 
 # offsets into the flat parameter vector (W row-major, out x in)
 OFF_W1 = 0
-OFF_B1 = OFF_W1 + HIDDEN * N_DESC
+OFF_B1 = OFF_W1 + HIDDEN * N_INPUT
 OFF_W2 = OFF_B1 + HIDDEN
 OFF_B2 = OFF_W2 + HIDDEN * HIDDEN
 OFF_W3 = OFF_B2 + HIDDEN
 OFF_B3 = OFF_W3 + HIDDEN * HIDDEN
 OFF_W4 = OFF_B3 + HIDDEN
 OFF_B4 = OFF_W4 + HIDDEN
-assert OFF_B4 + 1 == N_PARAMS
+OFF_V = OFF_B4 + 1
+N_SELF = N_INPUT - 64
+assert OFF_V + N_SELF == N_PARAMS
 
 
 def _fptr(a: np.ndarray):
@@ -37,10 +40,10 @@ def _fptr(a: np.ndarray):
 def unpack(params: np.ndarray) -> dict:
     p = np.asarray(params, dtype=np.float32)
     return {
-        "W1": p[OFF_W1:OFF_B1].reshape(HIDDEN, N_DESC), "b1": p[OFF_B1:OFF_W2],
+        "W1": p[OFF_W1:OFF_B1].reshape(HIDDEN, N_INPUT), "b1": p[OFF_B1:OFF_W2],
         "W2": p[OFF_W2:OFF_B2].reshape(HIDDEN, HIDDEN), "b2": p[OFF_B2:OFF_W3],
         "W3": p[OFF_W3:OFF_B3].reshape(HIDDEN, HIDDEN), "b3": p[OFF_B3:OFF_W4],
-        "w4": p[OFF_W4:OFF_B4], "b4": p[OFF_B4:OFF_B4 + 1],
+        "w4": p[OFF_W4:OFF_B4], "b4": p[OFF_B4:OFF_V], "v": p[OFF_V:N_PARAMS],
     }
 
 
@@ -75,9 +78,10 @@ def train(x: np.ndarray, target: np.ndarray, params: np.ndarray, steps: int, bat
 # ------------------------------------------------------------ engine hooks
 
 def samples(engine, sys: int = 0) -> tuple[np.ndarray, np.ndarray]:
-    """(x [n_atoms x 64], target [n_atoms]) of one system at its current positions."""
-    n = engine._n_atoms[sys]
-    x = np.empty((n, N_DESC), dtype=np.float32)
+    """(x [n_atoms x 80], target [n_atoms]) of one system (sys = -1: all
+    systems, concatenated) at the current positions."""
+    n = sum(engine._n_atoms) if sys == -1 else engine._n_atoms[sys]
+    x = np.empty((n, N_INPUT), dtype=np.float32)
     t = np.empty(n, dtype=np.float32)
     _check(lib().og_lgb_samples(engine._h, sys, _fptr(x), _fptr(t)))
     return x, t

@@ -63,6 +63,7 @@ def constant_params(origami, b4):
     p = lgb.init_params(1)
     p[lgb.OFF_W4:lgb.OFF_B4] = 0.0
     p[lgb.OFF_B4] = b4
+    p[lgb.OFF_V:] = 0.0
     return p
 
 
@@ -87,6 +88,37 @@ def test_learned_radii_are_cfa_times_exp_output(origami):
         got = eng.born_radii(k)
         np.testing.assert_allclose(got, rcfa * math.exp(np.float32(0.25)), rtol=1e-5)
         assert np.isfinite(eng.total_force(k)).all()
+
+
+def random_params(origami, seed):
+    from origami_b200 import lgb
+    rng = np.random.default_rng(seed)
+    p = lgb.init_params(seed)
+    p[lgb.OFF_B1:lgb.OFF_W2] = rng.normal(scale=0.1, size=128)
+    p[lgb.OFF_W4:lgb.OFF_B4] = rng.normal(scale=0.05, size=128)
+    p[lgb.OFF_B4] = -0.1
+    p[lgb.OFF_V:] = rng.normal(scale=0.05, size=lgb.N_SELF)
+    return p
+
+
+def test_fused_network_matches_layers_and_oracle(origami, monkeypatch):
+    """The fused tensor-core kernel against the three GEMM layers + head
+    (same rounding points: 1e-5) and against the NumPy network on the
+    engine's own inputs (BF16 rounding of operands emulated: 2e-3)."""
+    import lgb_mlp
+    from origami_b200 import lgb
+    rows = chains(origami)
+    params = random_params(origami, 9)
+    fused = learned_engine(origami, rows, params)
+    monkeypatch.setenv("OG_LGB_UNFUSED", "1")
+    layered = learned_engine(origami, rows, params)
+    for k, (ch, x) in enumerate(rows):
+        r_f, r_l = fused.born_radii(k), layered.born_radii(k)
+        np.testing.assert_allclose(r_f, r_l, rtol=1e-5)
+        xin, target = lgb.samples(fused, k)
+        rcfa = Orc(ch).born_radii(x) / np.exp(target.astype(np.float64))
+        y = np.clip(lgb_mlp.forward(params, xin)["y"], -5.0, 5.0)
+        np.testing.assert_allclose(r_f, rcfa * np.exp(y), rtol=2e-3)
 
 
 def test_engine_requires_parameters(origami):

@@ -19,15 +19,19 @@ import lgb_mlp  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-BLOCKS = (("W1", 0, 8192), ("b1", 8192, 8320), ("W2", 8320, 24704), ("b2", 24704, 24832),
-          ("W3", 24832, 41216), ("b3", 41216, 41344), ("w4", 41344, 41472), ("b4", 41472, 41473))
+def blocks():
+    from origami_b200 import lgb
+    o = [lgb.OFF_W1, lgb.OFF_B1, lgb.OFF_W2, lgb.OFF_B2, lgb.OFF_W3, lgb.OFF_B3, lgb.OFF_W4, lgb.OFF_B4, lgb.OFF_V,
+         lgb.N_PARAMS]
+    names = ("W1", "b1", "W2", "b2", "W3", "b3", "w4", "b4", "v")
+    return [(names[k], o[k], o[k + 1]) for k in range(9)]
 
 
 def data(n, seed):
     """Samples drawn with `seed` from one fixed smooth target function."""
-    a = np.random.default_rng(1234).normal(size=64) / 8.0
+    a = np.random.default_rng(1234).normal(size=80) / 8.0
     rng = np.random.default_rng(seed)
-    x = np.log1p(rng.gamma(2.0, 1.5, size=(n, 64))).astype(np.float32)
+    x = np.log1p(rng.gamma(2.0, 1.5, size=(n, 80))).astype(np.float32)
     t = (0.4 * np.tanh(x @ a - 2.0) - 0.1).astype(np.float32)
     return x, t
 
@@ -38,10 +42,13 @@ def test_gradient_matches_oracle(origami, n):
     x, t = data(n, n)
     p = lgb.init_params(3)
     p[lgb.OFF_B1:lgb.OFF_W2] = np.random.default_rng(1).normal(scale=0.1, size=128)
+    p[lgb.OFF_V:] = np.random.default_rng(2).normal(scale=0.1, size=lgb.N_SELF)
+    # non-zero output weights, so every layer's gradient is exercised
+    p[lgb.OFF_W4:lgb.OFF_B4] = np.random.default_rng(3).normal(scale=0.1, size=128)
     loss, g = lgb.loss_and_gradient(x, t, p)
     loss_ref, g_ref = lgb_mlp.loss_and_gradient(p, x, t)
     assert abs(loss - loss_ref) <= 1e-4 * loss_ref
-    for name, a, b in BLOCKS:
+    for name, a, b in blocks():
         num = np.linalg.norm(g[a:b] - g_ref[a:b])
         den = np.linalg.norm(g_ref[a:b])
         assert num <= 3e-3 * den + 1e-12, (name, num / den)

@@ -17,11 +17,12 @@ import lgb_mlp  # noqa: E402
 def test_oracle_gradient_matches_central_differences(monkeypatch):
     monkeypatch.setattr(lgb_mlp, "bf16", lambda a: np.asarray(a, np.float64))
     rng = np.random.default_rng(0)
-    p = rng.normal(scale=0.05, size=41473)
-    x = rng.random((40, 64))
+    p = rng.normal(scale=0.05, size=lgb_mlp.N_PARAMS)
+    x = rng.random((40, lgb_mlp.N_INPUT))
     t = rng.normal(scale=0.2, size=40)
     _, g = lgb_mlp.loss_and_gradient(p, x, t)
-    for idx in rng.choice(41473, 40, replace=False).tolist() + [41472, 41344, 8192, 0]:
+    n = lgb_mlp.N_PARAMS
+    for idx in rng.choice(n, 40, replace=False).tolist() + [n - 1, n - 17, n - 145, 128 * lgb_mlp.N_INPUT, 0]:
         e = np.zeros_like(p)
         e[idx] = 1e-6
         lp, _ = lgb_mlp.loss_and_gradient(p + e, x, t)
