@@ -46,6 +46,8 @@ using ogsasa::norm2;
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;
+constexpr int kSasaBatch = 32;        // circles per arrangement batch
+constexpr uint8_t kNoOther = 0xFF;    // pseudo entry of a transition-free circle
 constexpr double kPi = 3.14159265358979323846;
 
 __device__ __forceinline__ D3 normalize(D3 a) { return a / norm(a); }
@@ -59,9 +61,11 @@ __device__ __forceinline__ bool contains_strict(Cap c, D3 p) { return dot(p, c.a
 
 enum { kTwo = 0, kTangent = 1, kDisjoint = 2, kCoincident = 3 };
 
-// geometry.rs:70-102 (one reciprocal for the shared denominator and one
-// reciprocal square root for the normal's length; same values to rounding).
-__device__ int intersect(Cap c1, Cap c2, D3* p, D3* q) {
+// geometry.rs:70-102, classification part (one reciprocal for the shared
+// denominator; same values to rounding).  Not inlined: the counting pass and
+// the writing pass of the arrangement must classify every pair identically,
+// which one shared body guarantees.  a, b, c_sq are set for kTwo / kTangent.
+__device__ __noinline__ int classify(Cap c1, Cap c2, double* a_out, double* b_out, double* csq_out) {
   const double sigma = dot(c1.axis, c2.axis);
   const double denom = 1.0 - sigma * sigma;
   if (fabs(denom) < 1e-12) return fabs(c1.c - sigma * c2.c) < 1e-9 ? kCoincident : kDisjoint;
@@ -70,16 +74,38 @@ __device__ int intersect(Cap c1, Cap c2, D3* p, D3* q) {
   const double b = (c2.c - sigma * c1.c) * inv;
   const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * sigma;
   if (c_sq < -1e-9) return kDisjoint;
+  *a_out = a;
+  *b_out = b;
+  *csq_out = c_sq;
+  return fabs(c_sq) <= 1e-9 ? kTangent : kTwo;
+}
+
+// The transition points of a kTwo / kTangent pair (reciprocal square root
+// for the normal's length).
+__device__ __forceinline__ void transition_points(Cap c1, Cap c2, int kind, double a, double b, double c_sq, D3* p,
+                                                  D3* q) {
   const D3 base = c1.axis * a + c2.axis * b;
-  if (fabs(c_sq) <= 1e-9) {
+  if (kind == kTangent) {
     *p = base;
-    return kTangent;
+    return;
   }
   const D3 nc = cross(c1.axis, c2.axis);
   const D3 off = nc * (sqrt(c_sq) * rsqrt(norm2(nc)));
   *p = base + off;
   *q = base - off;
-  return kTwo;
+}
+
+__device__ __forceinline__ int transition_count(int kind) { return kind == kTwo ? 2 : (kind == kTangent ? 1 : 0); }
+
+// Transitions of circle 1 cut by cap 2 (0, 1 or 2), classifying the pair.
+// nn = (1 - sigma^2) c_sq costs no division; far below the tangency threshold
+// it means no transition whatever the rounding (classify would say kDisjoint
+// or kCoincident as well), so the two passes still agree pair by pair.
+__device__ __forceinline__ int pair_transitions(Cap c1, Cap c2, double* a, double* b, double* csq) {
+  const double sig = dot(c1.axis, c2.axis);
+  const double nn = 1.0 - sig * sig - c1.c * c1.c - c2.c * c2.c + 2.0 * sig * c1.c * c2.c;
+  if (nn < -1e-6) return 0;
+  return transition_count(classify(c1, c2, a, b, csq));
 }
 
 __device__ __forceinline__ D3 helper_axis(D3 axis) {
@@ -118,10 +144,18 @@ struct WarpSmem {
   double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps];
   int32_t owner[kSasaMaxCaps];
   uint8_t live[kSasaMaxCaps];
-  // transitions of the cap being processed: sort key, unit radial direction
+  int32_t tcnt[kSasaMaxCaps];  // transitions of each live circle
+  // transitions of the batch of circles being processed: sort key, unit
+  // radial direction, the other cap, the batch circle, the sorted order
   double ta[kSasaMaxTrans], tx[kSasaMaxTrans], ty[kSasaMaxTrans], tz[kSasaMaxTrans];
   uint8_t tother[kSasaMaxTrans];
+  uint8_t tseg[kSasaMaxTrans];
   uint8_t torder[kSasaMaxTrans];
+  // per batch circle: first entry, entries kept after de-duplication,
+  // transition-free circles before it, sin(alpha) and 1 / sin(alpha)
+  uint16_t sbeg[kSasaBatch + 1];
+  uint8_t skept[kSasaBatch], zpre[kSasaBatch];
+  double bsk[kSasaBatch], binv[kSasaBatch];
   // exposed arcs
   double a_theta[kSasaMaxArcs], a_sx[kSasaMaxArcs], a_sy[kSasaMaxArcs], a_sz[kSasaMaxArcs];
   uint8_t a_cap[kSasaMaxArcs], a_full[kSasaMaxArcs], a_vis[kSasaMaxArcs];
@@ -277,180 +311,251 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
   }
   __syncwarp();
 
-  // ---- boundary arcs, cap by cap (find_boundary)
+  // ---- boundary arcs (find_boundary), a batch of circles at a time: the
+  // transitions of every circle are counted first (each ordered pair once,
+  // by the same classification the writing pass uses), then consecutive
+  // circles whose transition lists fit the buffer are processed together --
+  // their transitions written, sorted and tested across all lanes -- and the
+  // exposed arcs appended in circle order and, within a circle, in angular
+  // order, the reference's order.  A circle without transitions takes one
+  // pseudo entry (its probe test).
+  for (int li = lane; li < n_live; li += 32) w.tcnt[li] = 0;
+  __syncwarp();
+  const int n_pairs = n_live * n_live;
+  for (int p = lane; p < n_pairs; p += 32) {
+    const int li = p / n_live, lm = p - li * n_live;
+    if (li == lm) continue;
+    double a, b, csq;
+    const int cnt = pair_transitions(cap_at(w, w.live[li]), cap_at(w, w.live[lm]), &a, &b, &csq);
+    if (cnt) atomicAdd(&w.tcnt[li], cnt);
+  }
+  __syncwarp();
+
   int n_arcs = 0, n_verts = 0;
   bool bad = false;
-  for (int li = 0; li < n_live && !bad; ++li) {
-    const int k = w.live[li];
-    const Cap ck = cap_at(w, k);
-    const D3 h = helper_axis(ck.axis);
-    const D3 fu = normalize(h - ck.axis * dot(h, ck.axis));
-    const D3 fv = cross(ck.axis, fu);
-    // Transitions are kept as unit radial directions u: every one lies on
-    // circle k, p = axis cos(alpha_k) + u sin(alpha_k).
-    const double sk = sqrt(fmax(1.0 - ck.c * ck.c, 0.0));
-    const double inv_sk = sk > 0.0 ? 1.0 / sk : 0.0;
-    int n_tr = 0;
-    for (int m0 = 0; m0 < n_live; m0 += 32) {
-      const int lm = m0 + lane;
-      int cnt = 0, m = -1;
-      D3 p{}, q{};
-      if (lm < n_live) {
+  for (int b0 = 0; b0 < n_live && !bad;) {
+    // the batch: consecutive live circles whose (padded) lists fit
+    int b1 = b0, total = 0;
+    while (b1 < n_live && b1 - b0 < kSasaBatch) {
+      const int sz = max(w.tcnt[b1], 1);
+      if (total + sz > kSasaMaxTrans) break;
+      total += sz;
+      ++b1;
+    }
+    if (b1 == b0) {
+      bad = true;  // one circle alone has more transitions than the buffer
+      break;
+    }
+    const int nb = b1 - b0;
+    if (lane == 0) {
+      int s0 = 0, z = 0;
+      for (int j = 0; j < nb; ++j) {
+        const int c = w.tcnt[b0 + j];
+        w.sbeg[j] = static_cast<uint16_t>(s0);
+        w.zpre[j] = static_cast<uint8_t>(z);
+        s0 += max(c, 1);
+        z += c == 0 ? 1 : 0;
+      }
+      w.sbeg[nb] = static_cast<uint16_t>(s0);
+    }
+    for (int j = lane; j < nb; j += 32) {
+      const double c = w.cc[w.live[b0 + j]];
+      const double sk = sqrt(fmax(1.0 - c * c, 0.0));
+      w.bsk[j] = sk;
+      w.binv[j] = sk > 0.0 ? 1.0 / sk : 0.0;
+    }
+    __syncwarp();
+
+    // transitions: pairs (batch circle j, live circle m), j-major, m ascending
+    // (the reference's push order), kept as unit radial directions u
+    // (p = axis cos(alpha) + u sin(alpha)) with a pseudo-angle sort key
+    int run = 0;
+    const int np = nb * n_live;
+    for (int p0 = 0; p0 < np; p0 += 32) {
+      const int p = p0 + lane;
+      int cnt = 0, j = 0, m = -1;
+      D3 pt{}, qt{};
+      Cap ck{};
+      if (p < np) {
+        j = p / n_live;
+        const int lm = p - j * n_live;
+        const int k = w.live[b0 + j];
         m = w.live[lm];
-        if (m != k) {
-          const double cm = w.cc[m];
-          const double sig = ck.axis.x * w.cx[m] + ck.axis.y * w.cy[m] + ck.axis.z * w.cz[m];
-          // (1 - sigma^2) c_sq; far below the tangency threshold means no
-          // transition whatever the rounding.
-          const double nn = 1.0 - sig * sig - ck.c * ck.c - cm * cm + 2.0 * sig * ck.c * cm;
-          if (nn >= -1e-6) {
-            const int kind = intersect(ck, cap_at(w, m), &p, &q);
-            cnt = kind == kTwo ? 2 : (kind == kTangent ? 1 : 0);
-          }
+        if (k != m) {
+          ck = cap_at(w, k);
+          const Cap cm = cap_at(w, m);
+          double a = 0.0, b = 0.0, csq = 0.0;
+          cnt = pair_transitions(ck, cm, &a, &b, &csq);
+          if (cnt) transition_points(ck, cm, cnt == 2 ? kTwo : kTangent, a, b, csq, &pt, &qt);
         }
       }
-      int total;
-      const int off = warp_excl_scan(cnt, lane, &total);
-      if (n_tr + total > kSasaMaxTrans) {
-        bad = true;
-        break;
+      int tot;
+      const int off = warp_excl_scan(cnt, lane, &tot);
+      const int base = run + off + (cnt ? w.zpre[j] : 0);
+      if (cnt && base + cnt <= w.sbeg[j + 1]) {
+        const double inv = w.binv[j];
+        const D3 h = helper_axis(ck.axis);
+        const D3 fu = h - ck.axis * dot(h, ck.axis);  // the angle is scale-free
+        const D3 fv = cross(ck.axis, fu);
+        for (int e = 0; e < cnt; ++e) {
+          const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
+          const int sl = base + e;
+          w.ta[sl] = pseudo_angle(dot(u, fu), dot(u, fv));
+          w.tx[sl] = u.x;
+          w.ty[sl] = u.y;
+          w.tz[sl] = u.z;
+          w.tother[sl] = static_cast<uint8_t>(m);
+          w.tseg[sl] = static_cast<uint8_t>(j);
+        }
       }
-      if (cnt >= 1) {
-        const int s = n_tr + off;
-        const D3 u = (p - ck.axis * ck.c) * inv_sk;
-        w.ta[s] = pseudo_angle(dot(u, fu), dot(u, fv));
-        w.tx[s] = u.x;
-        w.ty[s] = u.y;
-        w.tz[s] = u.z;
-        w.tother[s] = static_cast<uint8_t>(m);
-      }
-      if (cnt == 2) {
-        const int s = n_tr + off + 1;
-        const D3 u = (q - ck.axis * ck.c) * inv_sk;
-        w.ta[s] = pseudo_angle(dot(u, fu), dot(u, fv));
-        w.tx[s] = u.x;
-        w.ty[s] = u.y;
-        w.tz[s] = u.z;
-        w.tother[s] = static_cast<uint8_t>(m);
-      }
-      n_tr += total;
+      run += tot;
     }
-    if (bad) break;
+    if (run + w.zpre[nb - 1] + (w.tcnt[b1 - 1] == 0 ? 1 : 0) != w.sbeg[nb]) {
+      bad = true;  // the two passes disagree: never expected, but never written past
+      break;
+    }
+    for (int j = lane; j < nb; j += 32) {
+      if (w.tcnt[b0 + j] != 0) continue;
+      const int sl = w.sbeg[j];
+      w.tseg[sl] = static_cast<uint8_t>(j);
+      w.tother[sl] = kNoOther;
+      w.ta[sl] = 0.0;
+    }
     __syncwarp();
-    // stable sort by angle (ties keep push order)
+    const int n_tr = w.sbeg[nb];
+
+    // stable sort of each circle's transitions by angle (ties: push order)
     bool nonfinite = false;
-    for (int s = lane; s < n_tr; s += 32) {
-      const double as = w.ta[s];
-      if (!isfinite(as)) nonfinite = true;
+    for (int sl = lane; sl < n_tr; sl += 32) {
+      const int j = w.tseg[sl];
+      const int sb = w.sbeg[j], se = w.sbeg[j + 1];
       int rank = 0;
-      for (int t = 0; t < n_tr; ++t) {
-        const double at = w.ta[t];
-        rank += (at < as) || (at == as && t < s);
+      if (w.tother[sl] != kNoOther) {
+        const double as = w.ta[sl];
+        if (!isfinite(as)) nonfinite = true;
+        for (int t = sb; t < se; ++t) {
+          const double at = w.ta[t];
+          rank += (at < as) || (at == as && t < sl);
+        }
       }
-      if (rank < kSasaMaxTrans) w.torder[rank] = static_cast<uint8_t>(s);
+      w.torder[sb + min(rank, se - sb - 1)] = static_cast<uint8_t>(sl);
     }
     if (__any_sync(kFull, nonfinite)) {
       bad = true;
       break;
     }
     __syncwarp();
-    // consecutive de-duplication (|dp|^2 < 1e-12 against the last kept;
-    // |dp| = sin(alpha_k) |du| on the circle)
-    const double sk2 = sk * sk;
+
+    // consecutive de-duplication within each circle (|dp|^2 < 1e-12 against
+    // the last kept; |dp| = sin(alpha) |du|)
     bool dup = false;
-    for (int r = 1 + lane; r < n_tr; r += 32)
-      dup |= norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * sk2 < 1e-12;
-    int n_kept = n_tr;
+    for (int r = lane; r < n_tr; r += 32) {
+      const int j = w.tseg[w.torder[r]];
+      if (r == w.sbeg[j]) continue;
+      dup |= norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * (w.bsk[j] * w.bsk[j]) < 1e-12;
+    }
     if (__any_sync(kFull, dup)) {
       if (lane == 0) {
-        int kept = 0;
-        for (int r = 0; r < n_tr; ++r) {
-          const int s = w.torder[r];
-          if (kept == 0 || norm2(tpoint(w, s) - tpoint(w, w.torder[kept - 1])) * sk2 >= 1e-12)
-            w.torder[kept++] = static_cast<uint8_t>(s);
+        for (int j = 0; j < nb; ++j) {
+          const int sb = w.sbeg[j], se = w.sbeg[j + 1];
+          const double sk2 = w.bsk[j] * w.bsk[j];
+          int kept = 0;
+          for (int r = sb; r < se; ++r) {
+            const int sl = w.torder[r];
+            if (kept == 0 || norm2(tpoint(w, sl) - tpoint(w, w.torder[sb + kept - 1])) * sk2 >= 1e-12)
+              w.torder[sb + kept++] = static_cast<uint8_t>(sl);
+          }
+          w.skept[j] = static_cast<uint8_t>(kept);
         }
-        n_kept = kept;
       }
-      n_kept = __shfl_sync(kFull, n_kept, 0);
-      __syncwarp();
+    } else {
+      for (int j = lane; j < nb; j += 32) w.skept[j] = static_cast<uint8_t>(w.sbeg[j + 1] - w.sbeg[j]);
     }
+    __syncwarp();
 
-    if (n_kept == 0) {
-      // no vertices: the whole circle is exposed unless a probe on it is buried
-      const D3 probe = sample_circle_point(ck);
-      bool buried = false;
-      for (int lm = lane; lm < n_live; lm += 32) {
-        const int m = w.live[lm];
-        if (m != k && contains_strict(cap_at(w, m), probe)) buried = true;
-      }
-      if (!__any_sync(kFull, buried)) {
-        if (n_arcs >= kSasaMaxArcs) {
-          bad = true;
-          break;
-        }
-        if (lane == 0) {
-          w.a_cap[n_arcs] = static_cast<uint8_t>(k);
-          w.a_full[n_arcs] = 1;
-          w.a_theta[n_arcs] = -2.0 * kPi;
-          w.a_sx[n_arcs] = probe.x;
-          w.a_sy[n_arcs] = probe.y;
-          w.a_sz[n_arcs] = probe.z;
-          w.a_own[n_arcs] = -1;
-        }
-        ++n_arcs;
-      }
-      __syncwarp();
-      continue;
-    }
-    for (int r0 = 0; r0 < n_kept; r0 += 32) {
+    // exposure of every segment (and of every transition-free circle)
+    for (int r0 = 0; r0 < n_tr; r0 += 32) {
       const int r = r0 + lane;
-      bool exposed = false;
+      bool exposed = false, full = false;
       double cos_ccw = 1.0, sin_ccw = 0.0;
-      int sa = 0, sb = 0;
-      if (r < n_kept) {
-        sa = w.torder[r];
-        sb = w.torder[(r + 1) % n_kept];
-        D3 mid;
-        if (segment_midpoint(tpoint(w, sa), tpoint(w, sb), ck, sk, n_kept == 1, &mid, &cos_ccw, &sin_ccw)) {
-          // A buried segment usually lies in one of the two caps whose
-          // circles bound it; testing those first ends most searches early
-          // (the answer -- inside any other cap -- does not depend on order).
-          exposed = !contains_strict(cap_at(w, w.tother[sa]), mid) && !contains_strict(cap_at(w, w.tother[sb]), mid);
-          for (int lm = 0; lm < n_live && exposed; ++lm) {
-            const int m = w.live[lm];
-            if (m != k && contains_strict(cap_at(w, m), mid)) exposed = false;
+      int sa = 0, sbn = 0, j = 0, k = 0;
+      D3 probe{};
+      if (r < n_tr) {
+        const int jr = w.tseg[w.torder[r]];
+        const int pos = r - w.sbeg[jr], kept = w.skept[jr];
+        if (pos < kept) {
+          j = jr;
+          sa = w.torder[r];
+          k = w.live[b0 + j];
+          const Cap ck = cap_at(w, k);
+          if (w.tother[sa] == kNoOther) {
+            // no transitions: exposed unless a probe on the circle is buried
+            full = true;
+            probe = sample_circle_point(ck);
+            exposed = true;
+            for (int lm = 0; lm < n_live && exposed; ++lm) {
+              const int m = w.live[lm];
+              if (m != k && contains_strict(cap_at(w, m), probe)) exposed = false;
+            }
+          } else {
+            sbn = w.torder[w.sbeg[j] + (pos + 1) % kept];
+            D3 mid;
+            if (segment_midpoint(tpoint(w, sa), tpoint(w, sbn), ck, w.bsk[j], kept == 1, &mid, &cos_ccw,
+                                 &sin_ccw)) {
+              // a buried segment usually lies in one of the two caps whose
+              // circles bound it; testing those first ends most searches early
+              exposed = !contains_strict(cap_at(w, w.tother[sa]), mid) &&
+                        !contains_strict(cap_at(w, w.tother[sbn]), mid);
+              for (int lm = 0; lm < n_live && exposed; ++lm) {
+                const int m = w.live[lm];
+                if (m != k && contains_strict(cap_at(w, m), mid)) exposed = false;
+              }
+            }
           }
         }
       }
       const unsigned ex = __ballot_sync(kFull, exposed);
-      const int cnt = __popc(ex);
-      if (n_arcs + cnt > kSasaMaxArcs) {
+      const unsigned exv = __ballot_sync(kFull, exposed && !full);
+      if (n_arcs + __popc(ex) > kSasaMaxArcs) {
         bad = true;
         break;
       }
       if (exposed) {
-        double ccw = atan2(sin_ccw, cos_ccw);
-        if (ccw <= 0.0) ccw += 2.0 * kPi;
-        const int rank = __popc(ex & ((1u << lane) - 1u));
-        const int e = n_arcs + rank, v = n_verts + rank;
+        const unsigned below = (1u << lane) - 1u;
+        const int e = n_arcs + __popc(ex & below);
         w.a_cap[e] = static_cast<uint8_t>(k);
-        w.a_full[e] = 0;
-        w.a_theta[e] = -ccw;
-        const D3 pb = circle_point(ck, sk, tpoint(w, sb)), pa = circle_point(ck, sk, tpoint(w, sa));
-        w.a_sx[e] = pb.x;
-        w.a_sy[e] = pb.y;
-        w.a_sz[e] = pb.z;
-        w.a_own[e] = static_cast<int16_t>(v);
-        w.v_x[v] = pa.x;
-        w.v_y[v] = pa.y;
-        w.v_z[v] = pa.z;
-        w.v_in[v] = static_cast<uint8_t>(k);
-        w.v_out[v] = w.tother[sa];
+        if (full) {
+          w.a_full[e] = 1;
+          w.a_theta[e] = -2.0 * kPi;
+          w.a_sx[e] = probe.x;
+          w.a_sy[e] = probe.y;
+          w.a_sz[e] = probe.z;
+          w.a_own[e] = -1;
+        } else {
+          const Cap ck = cap_at(w, k);
+          const double sk = w.bsk[j];
+          double ccw = atan2(sin_ccw, cos_ccw);
+          if (ccw <= 0.0) ccw += 2.0 * kPi;
+          const int v = n_verts + __popc(exv & below);
+          const D3 pb = circle_point(ck, sk, tpoint(w, sbn)), pa = circle_point(ck, sk, tpoint(w, sa));
+          w.a_full[e] = 0;
+          w.a_theta[e] = -ccw;
+          w.a_sx[e] = pb.x;
+          w.a_sy[e] = pb.y;
+          w.a_sz[e] = pb.z;
+          w.a_own[e] = static_cast<int16_t>(v);
+          w.v_x[v] = pa.x;
+          w.v_y[v] = pa.y;
+          w.v_z[v] = pa.z;
+          w.v_in[v] = static_cast<uint8_t>(k);
+          w.v_out[v] = w.tother[sa];
+        }
       }
-      n_arcs += cnt;
-      n_verts += cnt;
+      n_arcs += __popc(ex);
+      n_verts += __popc(exv);
     }
     __syncwarp();
+    b0 = b1;
   }
   if (bad) return kInvalid;
   __syncwarp();
