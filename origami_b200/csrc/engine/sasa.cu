@@ -48,6 +48,8 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;
 constexpr int kSasaBatch = 32;        // circles per arrangement batch
 constexpr uint8_t kNoOther = 0xFF;    // pseudo entry of a transition-free circle
+constexpr int32_t kContained = 1 << 16;  // circle inside a cap it does not cross
+constexpr int32_t kCountMask = kContained - 1;
 constexpr double kPi = 3.14159265358979323846;
 
 __device__ __forceinline__ D3 normalize(D3 a) { return a / norm(a); }
@@ -59,53 +61,50 @@ struct Cap {
 
 __device__ __forceinline__ bool contains_strict(Cap c, D3 p) { return dot(p, c.axis) > c.c + 1e-12; }
 
-enum { kTwo = 0, kTangent = 1, kDisjoint = 2, kCoincident = 3 };
+// geometry.rs:70-102, restated.  Circle 1 (cap axis a1, cos c1) and circle 2
+// meet where the line through base = a a1 + b a2 along a1 x a2 pierces the
+// unit sphere, a = (c1 - sigma c2) / (1 - sigma^2), b = (c2 - sigma c1) /
+// (1 - sigma^2), c_sq = 1 - a^2 - b^2 - 2ab sigma; none for c_sq < -1e-9,
+// one (tangent) for |c_sq| <= 1e-9, none for parallel axes (1 - sigma^2 <
+// 1e-12).  Since (1 - sigma^2) c_sq = nn = 1 - sigma^2 - c1^2 - c2^2 + 2 sigma
+// c1 c2, the classification needs no division.  It is written with explicit
+// round-to-nearest intrinsics, which the compiler neither contracts nor
+// reorders, so the counting pass (each unordered pair once) and the writing
+// pass (each ordered pair) classify every pair bit for bit alike.
+struct PairClass {
+  double sigma, denom;
+  int count;  // transitions: 0, 1 (tangent) or 2
+};
 
-// geometry.rs:70-102, classification part (one reciprocal for the shared
-// denominator; same values to rounding).  Not inlined: the counting pass and
-// the writing pass of the arrangement must classify every pair identically,
-// which one shared body guarantees.  a, b, c_sq are set for kTwo / kTangent.
-__device__ __noinline__ int classify(Cap c1, Cap c2, double* a_out, double* b_out, double* csq_out) {
-  const double sigma = dot(c1.axis, c2.axis);
-  const double denom = 1.0 - sigma * sigma;
-  if (fabs(denom) < 1e-12) return fabs(c1.c - sigma * c2.c) < 1e-9 ? kCoincident : kDisjoint;
-  const double inv = 1.0 / denom;
-  const double a = (c1.c - sigma * c2.c) * inv;
-  const double b = (c2.c - sigma * c1.c) * inv;
-  const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * sigma;
-  if (c_sq < -1e-9) return kDisjoint;
-  *a_out = a;
-  *b_out = b;
-  *csq_out = c_sq;
-  return fabs(c_sq) <= 1e-9 ? kTangent : kTwo;
+__device__ __forceinline__ PairClass classify(Cap c1, Cap c2) {
+  PairClass r;
+  r.sigma = __fma_rn(c1.axis.x, c2.axis.x, __fma_rn(c1.axis.y, c2.axis.y, __dmul_rn(c1.axis.z, c2.axis.z)));
+  r.denom = __fma_rn(-r.sigma, r.sigma, 1.0);
+  r.count = 0;
+  if (fabs(r.denom) < 1e-12) return r;
+  // every step is symmetric in the two caps, so (1, 2) and (2, 1) agree too
+  const double t = __fma_rn(2.0 * r.sigma, __dmul_rn(c1.c, c2.c), r.denom);
+  const double nn = __dsub_rn(t, __dadd_rn(__dmul_rn(c1.c, c1.c), __dmul_rn(c2.c, c2.c)));
+  const double eps = 1e-9 * r.denom;
+  r.count = nn > eps ? 2 : (nn >= -eps ? 1 : 0);
+  return r;
 }
 
-// The transition points of a kTwo / kTangent pair (reciprocal square root
-// for the normal's length).
-__device__ __forceinline__ void transition_points(Cap c1, Cap c2, int kind, double a, double b, double c_sq, D3* p,
-                                                  D3* q) {
+// The transition points of a pair with count 1 or 2 (q only for 2).
+__device__ __forceinline__ void transition_points(Cap c1, Cap c2, PairClass pc, D3* p, D3* q) {
+  const double inv = 1.0 / pc.denom;
+  const double a = (c1.c - pc.sigma * c2.c) * inv;
+  const double b = (c2.c - pc.sigma * c1.c) * inv;
   const D3 base = c1.axis * a + c2.axis * b;
-  if (kind == kTangent) {
+  if (pc.count == 1) {
     *p = base;
     return;
   }
+  const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * pc.sigma;
   const D3 nc = cross(c1.axis, c2.axis);
-  const D3 off = nc * (sqrt(c_sq) * rsqrt(norm2(nc)));
+  const D3 off = nc * (sqrt(fmax(c_sq, 0.0)) * rsqrt(norm2(nc)));
   *p = base + off;
   *q = base - off;
-}
-
-__device__ __forceinline__ int transition_count(int kind) { return kind == kTwo ? 2 : (kind == kTangent ? 1 : 0); }
-
-// Transitions of circle 1 cut by cap 2 (0, 1 or 2), classifying the pair.
-// nn = (1 - sigma^2) c_sq costs no division; far below the tangency threshold
-// it means no transition whatever the rounding (classify would say kDisjoint
-// or kCoincident as well), so the two passes still agree pair by pair.
-__device__ __forceinline__ int pair_transitions(Cap c1, Cap c2, double* a, double* b, double* csq) {
-  const double sig = dot(c1.axis, c2.axis);
-  const double nn = 1.0 - sig * sig - c1.c * c1.c - c2.c * c2.c + 2.0 * sig * c1.c * c2.c;
-  if (nn < -1e-6) return 0;
-  return transition_count(classify(c1, c2, a, b, csq));
 }
 
 __device__ __forceinline__ D3 helper_axis(D3 axis) {
@@ -144,7 +143,8 @@ struct WarpSmem {
   double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps];
   int32_t owner[kSasaMaxCaps];
   uint8_t live[kSasaMaxCaps];
-  int32_t tcnt[kSasaMaxCaps];  // transitions of each live circle
+  // transitions of each live circle (low 16 bits) and kContained
+  int32_t tcnt[kSasaMaxCaps];
   // transitions of the batch of circles being processed: sort key, unit
   // radial direction, the other cap, the batch circle, the sorted order
   double ta[kSasaMaxTrans], tx[kSasaMaxTrans], ty[kSasaMaxTrans], tz[kSasaMaxTrans];
@@ -156,6 +156,14 @@ struct WarpSmem {
   uint16_t sbeg[kSasaBatch + 1];
   uint8_t skept[kSasaBatch], zpre[kSasaBatch];
   double bsk[kSasaBatch], binv[kSasaBatch];
+  // crossing toggle of each transition, the toggles up to it in angular
+  // order, its sorted position, and per batch circle the mode (0: burial
+  // depth by toggles, 1: explicit midpoint tests) and the depth before its
+  // first transition
+  int8_t ttog[kSasaMaxTrans], tdep[kSasaMaxTrans];
+  uint8_t trank[kSasaMaxTrans];
+  int32_t bmode[kSasaBatch];
+  int32_t bbase[kSasaBatch];
   // exposed arcs
   double a_theta[kSasaMaxArcs], a_sx[kSasaMaxArcs], a_sy[kSasaMaxArcs], a_sz[kSasaMaxArcs];
   uint8_t a_cap[kSasaMaxArcs], a_full[kSasaMaxArcs], a_vis[kSasaMaxArcs];
@@ -179,6 +187,21 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
   }
   *total = __shfl_sync(kFull, s, 31);
   return s - v;
+}
+
+// Position of the n-th (0-based) set bit of mask, which has more than n.
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int width = 16; width > 0; width >>= 1) {
+    const int c = __popc(mask & ((1u << width) - 1u));
+    if (n >= c) {
+      n -= c;
+      mask >>= width;
+      pos += width;
+    }
+  }
+  return pos;
 }
 
 enum Outcome { kExposed = 0, kBuried = 1, kBounded = 2, kInvalid = 3 };
@@ -318,16 +341,30 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
   // their transitions written, sorted and tested across all lanes -- and the
   // exposed arcs appended in circle order and, within a circle, in angular
   // order, the reference's order.  A circle without transitions takes one
-  // pseudo entry (its probe test).
+  // pseudo entry (its probe test).  A circle that lies inside a cap without
+  // crossing its rim (possible only within the culling margin) is marked
+  // kContained.
   for (int li = lane; li < n_live; li += 32) w.tcnt[li] = 0;
   __syncwarp();
+  // p / n_live by a float reciprocal: exact here, since p + 0.5 keeps the
+  // quotient at least 0.5 / n_live from an integer, far above the rounding
+  const float inv_live = 1.0f / static_cast<float>(n_live);
+  // the counts are symmetric (circle k crosses cap m where circle m crosses
+  // cap k), so each unordered pair is classified once: row li, columns lm > li
   const int n_pairs = n_live * n_live;
   for (int p = lane; p < n_pairs; p += 32) {
-    const int li = p / n_live, lm = p - li * n_live;
-    if (li == lm) continue;
-    double a, b, csq;
-    const int cnt = pair_transitions(cap_at(w, w.live[li]), cap_at(w, w.live[lm]), &a, &b, &csq);
-    if (cnt) atomicAdd(&w.tcnt[li], cnt);
+    const int li = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live), lm = p - li * n_live;
+    if (lm <= li) continue;
+    const Cap ck = cap_at(w, w.live[li]), cm = cap_at(w, w.live[lm]);
+    const PairClass pc = classify(ck, cm);
+    if (pc.count) {
+      atomicAdd(&w.tcnt[li], pc.count);
+      atomicAdd(&w.tcnt[lm], pc.count);
+    } else {
+      // a circle inside the other cap without crossing its rim
+      if (ck.c * pc.sigma - cm.c > -1e-9) atomicOr(&w.tcnt[li], kContained);
+      if (cm.c * pc.sigma - ck.c > -1e-9) atomicOr(&w.tcnt[lm], kContained);
+    }
   }
   __syncwarp();
 
@@ -337,7 +374,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     // the batch: consecutive live circles whose (padded) lists fit
     int b1 = b0, total = 0;
     while (b1 < n_live && b1 - b0 < kSasaBatch) {
-      const int sz = max(w.tcnt[b1], 1);
+      const int sz = max(w.tcnt[b1] & kCountMask, 1);
       if (total + sz > kSasaMaxTrans) break;
       total += sz;
       ++b1;
@@ -350,7 +387,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     if (lane == 0) {
       int s0 = 0, z = 0;
       for (int j = 0; j < nb; ++j) {
-        const int c = w.tcnt[b0 + j];
+        const int c = w.tcnt[b0 + j] & kCountMask;
         w.sbeg[j] = static_cast<uint16_t>(s0);
         w.zpre[j] = static_cast<uint8_t>(z);
         s0 += max(c, 1);
@@ -363,82 +400,119 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
       const double sk = sqrt(fmax(1.0 - c * c, 0.0));
       w.bsk[j] = sk;
       w.binv[j] = sk > 0.0 ? 1.0 / sk : 0.0;
+      w.bmode[j] = (w.tcnt[b0 + j] & kContained) ? 1 : 0;
+      w.bbase[j] = 0;
     }
     __syncwarp();
 
     // transitions: pairs (batch circle j, live circle m), j-major, m ascending
     // (the reference's push order), kept as unit radial directions u
-    // (p = axis cos(alpha) + u sin(alpha)) with a pseudo-angle sort key
-    int run = 0;
+    // (p = axis cos(alpha) + u sin(alpha)) with a pseudo-angle sort key.
+    // Pairs are classified 32 at a time; those that cross, with their
+    // output positions, go to a warp queue (one entry per lane) whose full
+    // rounds build the points with every lane busy.
+    int run = 0, queued = 0;
+    unsigned qentry = 0;  // pair index | output position << 16
     const int np = nb * n_live;
-    for (int p0 = 0; p0 < np; p0 += 32) {
-      const int p = p0 + lane;
-      int cnt = 0, j = 0, m = -1;
-      D3 pt{}, qt{};
-      Cap ck{};
-      if (p < np) {
-        j = p / n_live;
-        const int lm = p - j * n_live;
-        const int k = w.live[b0 + j];
-        m = w.live[lm];
-        if (k != m) {
-          ck = cap_at(w, k);
-          const Cap cm = cap_at(w, m);
-          double a = 0.0, b = 0.0, csq = 0.0;
-          cnt = pair_transitions(ck, cm, &a, &b, &csq);
-          if (cnt) transition_points(ck, cm, cnt == 2 ? kTwo : kTangent, a, b, csq, &pt, &qt);
-        }
-      }
-      int tot;
-      const int off = warp_excl_scan(cnt, lane, &tot);
-      const int base = run + off + (cnt ? w.zpre[j] : 0);
-      if (cnt && base + cnt <= w.sbeg[j + 1]) {
+    auto drain = [&](int n_entries) {
+      if (lane < n_entries) {
+        const int pidx = static_cast<int>(qentry & 0xFFFFu), base = static_cast<int>(qentry >> 16);
+        const int j = __float2int_rz((static_cast<float>(pidx) + 0.5f) * inv_live), m = w.live[pidx - j * n_live];
+        const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
+        const PairClass pc = classify(ck, cm);
+        D3 pt{}, qt{};
+        transition_points(ck, cm, pc, &pt, &qt);
         const double inv = w.binv[j];
         const D3 h = helper_axis(ck.axis);
         const D3 fu = h - ck.axis * dot(h, ck.axis);  // the angle is scale-free
         const D3 fv = cross(ck.axis, fu);
-        for (int e = 0; e < cnt; ++e) {
-          const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
+        for (int e = 0; e < pc.count; ++e) {
           const int sl = base + e;
+          if (sl >= w.sbeg[j + 1]) break;  // never expected: the counts agree
+          const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
           w.ta[sl] = pseudo_angle(dot(u, fu), dot(u, fv));
           w.tx[sl] = u.x;
           w.ty[sl] = u.y;
           w.tz[sl] = u.z;
           w.tother[sl] = static_cast<uint8_t>(m);
           w.tseg[sl] = static_cast<uint8_t>(j);
+          // crossing direction: moving counter-clockwise (along axis x u)
+          // the point enters cap m where the rate is positive and leaves it
+          // where negative; a tangent or a shallow crossing gets 0
+          const double rate = dot(cross(ck.axis, u), cm.axis);
+          w.ttog[sl] = pc.count == 1 ? 0 : (rate > 1e-4 ? 1 : (rate < -1e-4 ? -1 : 0));
         }
+      }
+    };
+    for (int p0 = 0; p0 < np; p0 += 32) {
+      const int p = p0 + lane;
+      int cnt = 0, j = 0;
+      if (p < np) {
+        j = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live);
+        const int lm = p - j * n_live;
+        const int k = w.live[b0 + j], m = w.live[lm];
+        if (k != m) cnt = classify(cap_at(w, k), cap_at(w, m)).count;
+      }
+      int tot;
+      const int off = warp_excl_scan(cnt, lane, &tot);
+      const unsigned packed = static_cast<unsigned>(p) | (static_cast<unsigned>(run + off + (cnt ? w.zpre[j] : 0)) << 16);
+      const unsigned crossing = __ballot_sync(kFull, cnt != 0);
+      const int n_new = __popc(crossing);
+      // lanes queued .. 31 take the first new entries
+      int t = lane - queued;
+      unsigned v = __shfl_sync(kFull, packed, (t >= 0 && t < n_new) ? nth_set_bit(crossing, t) : lane);
+      if (t >= 0 && t < n_new) qentry = v;
+      if (queued + n_new >= 32) {
+        drain(32);
+        // the rest start the next queue
+        t = lane + (32 - queued);
+        v = __shfl_sync(kFull, packed, t < n_new ? nth_set_bit(crossing, t) : lane);
+        if (t < n_new) qentry = v;
+        queued = queued + n_new - 32;
+      } else {
+        queued += n_new;
       }
       run += tot;
     }
-    if (run + w.zpre[nb - 1] + (w.tcnt[b1 - 1] == 0 ? 1 : 0) != w.sbeg[nb]) {
+    drain(queued);
+    if (run + w.zpre[nb - 1] + ((w.tcnt[b1 - 1] & kCountMask) == 0 ? 1 : 0) != w.sbeg[nb]) {
       bad = true;  // the two passes disagree: never expected, but never written past
       break;
     }
     for (int j = lane; j < nb; j += 32) {
-      if (w.tcnt[b0 + j] != 0) continue;
+      if ((w.tcnt[b0 + j] & kCountMask) != 0) continue;
       const int sl = w.sbeg[j];
       w.tseg[sl] = static_cast<uint8_t>(j);
       w.tother[sl] = kNoOther;
       w.ta[sl] = 0.0;
+      w.ttog[sl] = 0;
     }
     __syncwarp();
     const int n_tr = w.sbeg[nb];
 
-    // stable sort of each circle's transitions by angle (ties: push order)
+    // stable sort of each circle's transitions by angle (ties: push order),
+    // summing the toggles met on the way
     bool nonfinite = false;
     for (int sl = lane; sl < n_tr; sl += 32) {
       const int j = w.tseg[sl];
       const int sb = w.sbeg[j], se = w.sbeg[j + 1];
-      int rank = 0;
+      int rank = 0, dep = 0;
       if (w.tother[sl] != kNoOther) {
         const double as = w.ta[sl];
         if (!isfinite(as)) nonfinite = true;
         for (int t = sb; t < se; ++t) {
           const double at = w.ta[t];
-          rank += (at < as) || (at == as && t < sl);
+          const bool before = (at < as) || (at == as && t < sl);
+          rank += before;
+          dep += before ? w.ttog[t] : 0;
         }
+        if (w.ttog[sl] == 0) atomicOr(&w.bmode[j], 1);
       }
-      w.torder[sb + min(rank, se - sb - 1)] = static_cast<uint8_t>(sl);
+      rank = min(rank, se - sb - 1);
+      // the crossings up to and including this one, in angular order
+      w.tdep[sl] = static_cast<int8_t>(dep + w.ttog[sl]);
+      w.trank[sl] = static_cast<uint8_t>(rank);
+      w.torder[sb + rank] = static_cast<uint8_t>(sl);
     }
     if (__any_sync(kFull, nonfinite)) {
       bad = true;
@@ -452,8 +526,31 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     for (int r = lane; r < n_tr; r += 32) {
       const int j = w.tseg[w.torder[r]];
       if (r == w.sbeg[j]) continue;
-      dup |= norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * (w.bsk[j] * w.bsk[j]) < 1e-12;
+      if (norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * (w.bsk[j] * w.bsk[j]) < 1e-12) {
+        dup = true;
+        atomicOr(&w.bmode[j], 1);
+      }
     }
+    // Burial depth.  Along a circle whose crossings are all clean (no
+    // tangent, no shallow crossing, nothing merged by de-duplication, no cap
+    // holding it without a crossing), the point enters and leaves each
+    // crossing cap once, so the depth just after a transition is the toggles
+    // up to it plus the depth before the first transition -- the number of
+    // caps whose leaving crossing comes before their entering one in angular
+    // order.  A segment is exposed where the depth is 0.  The other circles
+    // test every segment's midpoint against every cap.
+    for (int sl = lane; sl < n_tr; sl += 32) {
+      if (w.ttog[sl] != -1) continue;
+      const int j = w.tseg[sl], m = w.tother[sl];
+      // the pair's other transition is the neighbouring slot with the same
+      // circle and cap
+      const int q = (sl + 1 < n_tr && w.tother[sl + 1] == m && w.tseg[sl + 1] == j) ? sl + 1 : sl - 1;
+      if (q < 0 || w.ttog[q] != 1 || w.tother[q] != m || w.tseg[q] != j)
+        atomicOr(&w.bmode[j], 1);
+      else if (w.trank[sl] < w.trank[q])
+        atomicAdd(&w.bbase[j], 1);
+    }
+    __syncwarp();
     if (__any_sync(kFull, dup)) {
       if (lane == 0) {
         for (int j = 0; j < nb; ++j) {
@@ -496,6 +593,15 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
             for (int lm = 0; lm < n_live && exposed; ++lm) {
               const int m = w.live[lm];
               if (m != k && contains_strict(cap_at(w, m), probe)) exposed = false;
+            }
+          } else if (w.bmode[j] == 0) {
+            sbn = w.torder[w.sbeg[j] + (pos + 1) % kept];
+            if (w.bbase[j] + w.tdep[sa] == 0) {
+              // the reference's skip of a vanishing segment (ccw < 1e-9)
+              const D3 ua = tpoint(w, sa), ub = tpoint(w, sbn);
+              cos_ccw = dot(ua, ub);
+              sin_ccw = dot(ck.axis, cross(ua, ub));
+              exposed = !(cos_ccw > 0.0 && sin_ccw >= 0.0 && sin_ccw < 2e-9 && atan2(sin_ccw, cos_ccw) < 1e-9);
             }
           } else {
             sbn = w.torder[w.sbeg[j] + (pos + 1) % kept];
@@ -903,6 +1009,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const
 }
 
 constexpr size_t kWarpSmemBytes = sizeof(WarpSmem) * kWarps;
+// four resident CTAs per SM (228 KB, 1 KB reserved per CTA)
+static_assert(4 * (kWarpSmemBytes + 1024) <= 228 * 1024, "boundary kernel no longer fits four CTAs per SM");
 
 }  // namespace
 
