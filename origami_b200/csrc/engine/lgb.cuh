@@ -62,7 +62,7 @@ struct LgbDescArgs {
   double* r_cfa;               // n_padded (padding: 1)
 };
 
-// Descriptors and Coulomb-field radii of every atom (one warp per tile).
+// Descriptors and Coulomb-field radii of every atom (one 4-warp block per tile).
 void launch_lgb_descriptors(const LgbDescArgs& a, cudaStream_t s);
 
 // y = w4 . h3 + b4 + v . xself per row, R = r_cfa exp(clamp(y)) -> born_r

@@ -20,28 +20,67 @@ constexpr float kPiF = 3.14159265358979f;
 __device__ __forceinline__ float hct_term(float r, float rti, float sj) {
   if (!(rti < r + sj)) return 0.0f;
   const float l = fmaxf(rti, fabsf(r - sj)), u = r + sj;
-  const float il = 1.0f / l, iu = 1.0f / u, ir = 1.0f / r;
+  const float il = __frcp_rn(l), iu = __frcp_rn(u), ir = __frcp_rn(r);
   float t = 0.5f * (il - iu + 0.25f * r * (iu * iu - il * il) + 0.5f * ir * __logf(l * iu) +
                     0.25f * sj * sj * ir * (il * il - iu * iu));
   if (rti < sj - r) t += 2.0f * (1.0f / rti - il);
   return t;
 }
 
-__device__ __forceinline__ void add_shells(float* acc, float r, float w) {
+// Gaussian shells g_s = exp(-a (r - mu_s)^2), mu_s = 1.5 + 0.7 s, a = 1 /
+// (2 sigma^2), by recurrence: with d = r - mu_s, g_{s+1} = g_s exp(a (2 D d -
+// D^2)) and g_{s-1} = g_s exp(-a (2 D d + D^2)) (D = 0.7), and each of those
+// factors changes by exp(-2 a D^2) = exp(-1) per shell (sigma = D).  Seeds at
+// shells kMid run the recurrence over [kLo, kHi]: two seeds of four shells
+// each side keep the error within a few 1e-6 of the shell value (about five
+// times the direct evaluation's) at 6 exponentials per partner instead of 16,
+// which is what bounds this kernel (the special-function unit).
+template <int kMid, int kLo, int kHi>
+__device__ __forceinline__ void add_shell_run(float* acc, float r, float w) {
+  constexpr float kStep = 0.36787944117144233f;  // exp(-2 a D^2) = exp(-1)
+  const float d = r - (kMu0 + kShell * kMid);
+  const float g = __expf(-d * d * kInv2Sigma2);
+  float up = __expf(kInv2Sigma2 * (2.0f * kShell * d - kShell * kShell));
+  float dn = __expf(-kInv2Sigma2 * (2.0f * kShell * d + kShell * kShell));
+  acc[kMid] += w * g;
+  float gu = g, gd = g;
 #pragma unroll
-  for (int s = 0; s < 16; ++s) {
-    const float d = r - (kMu0 + kShell * s);
-    acc[s] += w * __expf(-d * d * kInv2Sigma2);
+  for (int s = kMid + 1; s <= kHi; ++s) {
+    gu *= up;
+    up *= kStep;
+    acc[s] += w * gu;
+  }
+#pragma unroll
+  for (int s = kMid - 1; s >= kLo; --s) {
+    gd *= dn;
+    dn *= kStep;
+    acc[s] += w * gd;
   }
 }
 
-// One warp per tile of 32 i-atoms; j tiles of the same system whose bounding
-// spheres come within the cutoff are broadcast one atom at a time, so the
-// partner's class -- and the accumulator block it feeds -- is warp-uniform.
-__global__ void __launch_bounds__(128) k_lgb_desc(LgbDescArgs a) {
-  const int ti = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (ti >= (a.n_padded >> 5)) return;
+__device__ __forceinline__ void add_shells(float* acc, float r, float w) {
+  add_shell_run<4, 0, 7>(acc, r, w);
+  add_shell_run<12, 8, 15>(acc, r, w);
+}
+
+// One block of four warps per tile of 32 i-atoms (lane = atom).  The warps
+// split the partners by descriptor class, so each keeps 16 or 32 shell
+// accumulators instead of 64: warps 0 and 1 take the H partners (even and
+// odd partner slots -- about half of all atoms), warp 2 the C/S partners,
+// warp 3 the N/P and O partners.  Each warp scans the system's tiles 32 at a
+// time for bounding spheres within the cutoff, then broadcasts its partners
+// of each such tile one at a time (class and slot are warp-uniform).  The
+// partial shell sums and Coulomb-field integrals meet in shared memory.
+// (Eight warps, splitting H four ways, measured slower: every warp repeats
+// the tile scan and the partner loads.)
+constexpr int kDescWarps = 4;
+constexpr int kDescSlots = 5;  // one per warp, plus the second class of warp 3
+
+__global__ void __launch_bounds__(kDescWarps * 32) k_lgb_desc(LgbDescArgs a) {
+  __shared__ float part[kDescSlots][16][33];  // [slot][shell][atom], padded
+  __shared__ float cfa_part[kDescWarps][32];
+  const int ti = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = ti * 32 + lane;
   const bool live_i = a.atom_sys[i] >= 0;
   const int sys = a.atom_sys[ti * 32];
@@ -50,75 +89,107 @@ __global__ void __launch_bounds__(128) k_lgb_desc(LgbDescArgs a) {
   const float yi = live_i ? static_cast<float>(a.y[i] - oi.y) : 0.0f;
   const float zi = live_i ? static_cast<float>(a.z[i] - oi.z) : 0.0f;
   const float rti = live_i ? static_cast<float>(a.rho_tilde[i]) : 1.0f;
-  float acc[64];
+  // this warp's classes (second -1 for a single class) and partner slots
+  const int cls0 = warp < 2 ? 3 : (warp == 2 ? 0 : 1);
+  const int cls1 = warp == 3 ? 2 : -1;
+  const int stride_mask = warp < 2 ? 1 : 0;
+  const int residue = warp < 2 ? warp : 0;
+  float acc[32];
 #pragma unroll
-  for (int k = 0; k < 64; ++k) acc[k] = 0.0f;
+  for (int k = 0; k < 32; ++k) acc[k] = 0.0f;
   float cfa = 0.0f;
   if (sys >= 0) {
     const int2 st = a.sys_tiles[sys];
-    for (int tj = st.x; tj < st.x + st.y; ++tj) {
-      const double4 oj = a.origin[tj];
-      const double ddx = oj.x - oi.x, ddy = oj.y - oi.y, ddz = oj.z - oi.z;
-      const double lim = oi.w + oj.w + kLgbCutoff + 1e-3;
-      if (ddx * ddx + ddy * ddy + ddz * ddz > lim * lim) continue;
-      const int j = tj * 32 + lane;
-      const bool live_j = a.atom_sys[j] >= 0;
-      const float xj = live_j ? static_cast<float>(a.x[j] - oi.x) : 0.0f;
-      const float yj = live_j ? static_cast<float>(a.y[j] - oi.y) : 0.0f;
-      const float zj = live_j ? static_cast<float>(a.z[j] - oi.z) : 0.0f;
-      const float wj = live_j ? static_cast<float>(a.rho[j]) : 0.0f;
-      const float sj = live_j ? static_cast<float>(a.srho[j]) : 0.0f;
-      const int cj = live_j ? a.klass[j] : -1;
-      for (int b = 0; b < 32; ++b) {
-        const int cb = __shfl_sync(kFull, cj, b);
-        if (cb < 0) continue;  // padding partner (warp-uniform)
-        const float dx = __shfl_sync(kFull, xj, b) - xi;
-        const float dy = __shfl_sync(kFull, yj, b) - yi;
-        const float dz = __shfl_sync(kFull, zj, b) - zi;
-        const float wb = __shfl_sync(kFull, wj, b);
-        const float sb = __shfl_sync(kFull, sj, b);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const bool ok = live_i && r2 < kCut * kCut && !(tj == ti && b == lane);
-        if (!__any_sync(kFull, ok)) continue;  // partner out of range of the whole tile
-        const float r = sqrtf(r2);
-        const float fc = ok ? 0.5f * (__cosf(kPiF * r / kCut) + 1.0f) : 0.0f;
-        const float w = wb * fc;
-        if (ok) cfa += fc * hct_term(r, rti, sb);
-        switch (cb) {
-          case 0: add_shells(acc + 0, r, w); break;
-          case 1: add_shells(acc + 16, r, w); break;
-          case 2: add_shells(acc + 32, r, w); break;
-          default: add_shells(acc + 48, r, w); break;
+    for (int t0 = 0; t0 < st.y; t0 += 32) {
+      bool near = false;
+      if (t0 + lane < st.y) {
+        const double4 oj = a.origin[st.x + t0 + lane];
+        const double ddx = oj.x - oi.x, ddy = oj.y - oi.y, ddz = oj.z - oi.z;
+        const double lim = oi.w + oj.w + kLgbCutoff + 1e-3;
+        near = ddx * ddx + ddy * ddy + ddz * ddz <= lim * lim;
+      }
+      unsigned tiles = __ballot_sync(kFull, near);
+      while (tiles) {
+        const int tj = st.x + t0 + __ffs(tiles) - 1;
+        tiles &= tiles - 1;
+        const int j = tj * 32 + lane;
+        const bool live_j = a.atom_sys[j] >= 0;
+        const int cj = live_j ? a.klass[j] : -1;
+        const bool mine = (cj == cls0 || cj == cls1) && (lane & stride_mask) == residue;
+        unsigned todo = __ballot_sync(kFull, mine);
+        if (!todo) continue;
+        const float xj = static_cast<float>(a.x[j] - oi.x);
+        const float yj = static_cast<float>(a.y[j] - oi.y);
+        const float zj = static_cast<float>(a.z[j] - oi.z);
+        const float wj = live_j ? static_cast<float>(a.rho[j]) : 0.0f;
+        const float sj = live_j ? static_cast<float>(a.srho[j]) : 0.0f;
+        while (todo) {
+          const int b = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const float dx = __shfl_sync(kFull, xj, b) - xi;
+          const float dy = __shfl_sync(kFull, yj, b) - yi;
+          const float dz = __shfl_sync(kFull, zj, b) - zi;
+          const float wb = __shfl_sync(kFull, wj, b);
+          const float sb = __shfl_sync(kFull, sj, b);
+          const int cb = __shfl_sync(kFull, cj, b);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const bool ok = live_i && r2 < kCut * kCut && !(tj == ti && b == lane);
+          if (!__any_sync(kFull, ok)) continue;  // partner out of range of the whole tile
+          const float r = sqrtf(r2);
+          const float fc = ok ? 0.5f * (__cosf(kPiF * r / kCut) + 1.0f) : 0.0f;
+          const float w = wb * fc;
+          if (ok) cfa += fc * hct_term(r, rti, sb);
+          if (cb == cls0)
+            add_shells(acc, r, w);
+          else
+            add_shells(acc + 16, r, w);
         }
       }
     }
   }
-  if (i < a.n_padded) {
-    double rc = 1.0;
-    if (live_i) {
-      const double inv = fmax(1.0 / a.rho_tilde[i] - static_cast<double>(cfa), 1.0 / 30.0);
-      rc = 1.0 / inv;
-    }
-    a.r_cfa[i] = rc;
-    float4* out = reinterpret_cast<float4*>(a.xin + static_cast<int64_t>(i) * kLgbIn);
+  // partial sums -> shared memory
 #pragma unroll
-    for (int k = 0; k < kLgbDesc; k += 4)
-      out[k / 4] = live_i ? make_float4(log1pf(acc[k]), log1pf(acc[k + 1]), log1pf(acc[k + 2]), log1pf(acc[k + 3]))
-                          : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (live_i) {
+  for (int k = 0; k < 16; ++k) part[warp][k][lane] = acc[k];
+  if (cls1 >= 0) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) part[4][k][lane] = acc[16 + k];
+  }
+  cfa_part[warp][lane] = cfa;
+  __syncthreads();
+  float4* out = reinterpret_cast<float4*>(a.xin + static_cast<int64_t>(i) * kLgbIn);
+  float cfa_sum = 0.0f;
+#pragma unroll
+  for (int w = 0; w < kDescWarps; ++w) cfa_sum += cfa_part[w][lane];
+  double rc = 1.0;
+  if (live_i) {
+    const double inv = fmax(1.0 / a.rho_tilde[i] - static_cast<double>(cfa_sum), 1.0 / 30.0);
+    rc = 1.0 / inv;
+  }
+  if (warp == 0) a.r_cfa[i] = rc;
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // warp w writes float4 chunks w, w + 4, ..., w + 16 of the atom's 20
+  for (int q = warp; q < kLgbIn / 4; q += kDescWarps) {
+    float4 v = zero;
+    if (live_i && q < kLgbDesc / 4) {
+      const int c = q >> 2, s0 = (q & 3) * 4;
+      float d[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int s = s0 + e;
+        d[e] = c == 3 ? part[0][s][lane] + part[1][s][lane] : part[c == 0 ? 2 : (c == 1 ? 3 : 4)][s][lane];
+      }
+      v = make_float4(log1pf(d[0]), log1pf(d[1]), log1pf(d[2]), log1pf(d[3]));
+    } else if (live_i && q == 16) {
       const int ci = a.klass[i];
+      v = make_float4(ci == 0 ? 1.0f : 0.0f, ci == 1 ? 1.0f : 0.0f, ci == 2 ? 1.0f : 0.0f, ci == 3 ? 1.0f : 0.0f);
+    } else if (live_i && q == 17) {
       const double rt = a.rho_tilde[i];
-      out[16] = make_float4(ci == 0 ? 1.0f : 0.0f, ci == 1 ? 1.0f : 0.0f, ci == 2 ? 1.0f : 0.0f, ci == 3 ? 1.0f : 0.0f);
-      out[17] = make_float4(static_cast<float>(rt), static_cast<float>(a.srho[i] / rt), static_cast<float>(rt / rc),
-                            static_cast<float>(log(rc)));
-      out[18] = make_float4(0.0f, static_cast<float>(log(rt / rc)), 0.0f, 0.0f);
-    } else {
-      out[16] = zero;
-      out[17] = zero;
-      out[18] = zero;
+      v = make_float4(static_cast<float>(rt), static_cast<float>(a.srho[i] / rt), static_cast<float>(rt / rc),
+                      static_cast<float>(log(rc)));
+    } else if (live_i && q == 18) {
+      v = make_float4(0.0f, static_cast<float>(log(a.rho_tilde[i] / rc)), 0.0f, 0.0f);
     }
-    out[19] = zero;
+    out[q] = v;
   }
 }
 
@@ -259,7 +330,7 @@ __global__ void k_lgb_sum(const float* part, int n, float* out) {
 
 void launch_lgb_descriptors(const LgbDescArgs& a, cudaStream_t s) {
   const int tiles = a.n_padded >> 5;
-  k_lgb_desc<<<(tiles + 3) / 4, 128, 0, s>>>(a);
+  if (tiles > 0) k_lgb_desc<<<tiles, kDescWarps * 32, 0, s>>>(a);
 }
 
 void launch_lgb_radii(const AtomArrays& at, const float* h3, const float* xin, const float* params,
