@@ -33,6 +33,11 @@ sys.path.insert(0, ROOT)
 
 AA_ORDER = "ARNDCQEGHILKMFPSTWYV"  # AminoAcid::ALL (chem/src/amino_acid.rs:31)
 METRIC = "aggregate ns/day (64 replicas, 5k atoms, GB+SASA): learned-GB vs plain GB"
+# DRAM bytes (read + write) of one force-pass launch per replica of the
+# 4 694-atom chain: ncu at 4 replicas read 1.51 MB and wrote nothing; each
+# replica's packed arrays stay in L2 across its tile sweep, so the traffic
+# grows with replicas, not with pairs.
+FORCE_PASS_DRAM_BYTES_PER_REPLICA = 1.514496e6 / 4
 
 
 def seeded_sequence(n_res: int, seed: int) -> str:
@@ -377,9 +382,19 @@ def run_b200(args):
         "learned_vs_plain": (value / plain_value) if not args.plain_only else None,
         "learned_gb": learned_info,
         "roofline": {"bound": "fp32", "kernel": "force_pass", "achieved": force_tflops, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": force_tflops / fp32_peak, "traffic": None,
-                     "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak)",
+                     "unit": "TFLOP/s", "frac": force_tflops / fp32_peak,
+                     "traffic": FORCE_PASS_DRAM_BYTES_PER_REPLICA * args.replicas,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_force<1> at 4 "
+                                       "replicas (profiles/pair_kernels_4x4694_extended.md), per replica x replicas",
+                     "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak); the pair math is FP32 "
+                                    "CUDA-core work, so neither the HBM copy nor the BF16 tensor peak bounds it",
                      "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
+        "dominant_kernel": {
+            "kernel": "k_sasa_boundary + k_sasa_terms (PowerSasa, FP64)",
+            "ms_per_step": (prof["sasa"][0] / prof["sasa"][1]) if "sasa" in prof else None,
+            "bound": "FP64 dependency latency at 16 warps per SM (ncu: issue active 43.5 %, FP64 pipe 15 %, "
+                     "DRAM 0.02 %); data-dependent geometry, no flop or byte roofline",
+            "profile": "profiles/sasa_boundary_4x4694_extended.md"},
         "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / plain_ms) if "sasa" in prof else None,
         "born_pass_tflops": born_tflops,
         "pair_interactions_per_s": pairs / (ms_per_step * 1e-3) * ws,
