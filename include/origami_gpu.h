@@ -312,8 +312,9 @@ og_status og_tc_gemm(const float* a, int64_t a_sm, int64_t a_sk, const float* b,
 /* ---- Learned Born radii (born_mode = 1).  No counterpart in the reference.
  * Per atom: 64 descriptors D (16 Gaussian shells, centres 1.5..12 A, width
  * 0.7 A, x 4 element classes C/S, N/P, O, H; partner-radius weighted, cosine
- * cutoff 12 A), input x = log(1 + D); a 64-128-128-128-1 SiLU network (BF16
- * tensor-core products, FP32 accumulate) predicts y = log(R / R_cfa), R_cfa
+ * cutoff 12 A), input x = log(1 + D); an 80-128-128-128-1 SiLU network over
+ * the inputs below (BF16 tensor-core products, FP32 accumulate) predicts
+ * y = log(R / R_cfa), clamped to [-5, 5], R_cfa
  * the Coulomb-field radius in its pairwise (HCT) form over the same 12 A
  * neighbours: 1/R_cfa = max(1/rho~ - sum fc I_HCT(r, rho~_i, s_j rho~_j),
  * 1/30).  The network input is OG_LGB_N_INPUT = 80 wide: the 64
