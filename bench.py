@@ -53,6 +53,30 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, ws: int, device: str = "cuda") -> float:
+    """The largest value of x over all ranks (every rank calls it, in the
+    same order); x itself with one rank."""
+    if ws <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(seed: int, rank: int, replicas: int, r: int) -> int:
+    """Velocity seed of replica r on `rank`: replicas are numbered globally
+    (rank-major), so every replica of the whole job starts differently."""
+    return (seed + (rank * replicas + r) * 0xC0FFEE) & ((1 << 64) - 1)
+
+
+def aggregate_ns_per_day(ws: int, replicas: int, dt_fs: float, ms_per_step: float) -> float:
+    """Whole-job throughput: ws ranks x replicas systems, each advancing
+    dt_fs per step, at the slowest rank's time per step."""
+    return ws * replicas * dt_fs * 1e-6 / (ms_per_step * 1e-3) * 86400.0
+
+
 class Clocks:
     """nvidia-smi sampler for the timed region."""
 
@@ -210,7 +234,7 @@ def make_engine(og, args, chain, rank: int, born_mode: int, stream):
     eng.finalize()
     eng.set_stream(stream.cuda_stream)
     for r in range(args.replicas):
-        eng.init_velocities(r, (args.seed + r * 0xC0FFEE) & og.Xoshiro256pp.M, remove_com=False)
+        eng.init_velocities(r, replica_seed(args.seed, rank, args.replicas, r), remove_com=False)
     return eng
 
 
@@ -232,11 +256,7 @@ def timed_steps(eng, args, stream, flush, local, ws):
             eng.step(1)
             ev[k][1].record(stream)
         torch.cuda.synchronize()
-    total_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if ws > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), ws)
     return total_ms / args.steps, clk.summary
 
 
@@ -303,7 +323,7 @@ def run_b200(args):
     prof = plain.profile_read()
     plain.profile(False)
     plain.close()
-    plain_value = ws * args.replicas * args.dt * 1e-6 / (plain_ms * 1e-3) * 86400.0
+    plain_value = aggregate_ns_per_day(ws, args.replicas, args.dt, plain_ms)
 
     # ---- learned GB arm (the headline): network trained on the GPU first
     learned_info = None
@@ -333,7 +353,7 @@ def run_b200(args):
     else:
         eng = make_engine(og, args, chain, rank, 0, stream)
         ms_per_step, clk = plain_ms, plain_clk
-    value = ws * args.replicas * args.dt * 1e-6 / (ms_per_step * 1e-3) * 86400.0
+    value = aggregate_ns_per_day(ws, args.replicas, args.dt, ms_per_step)
 
     force_ms = prof["force_pass"][0] / prof["force_pass"][1]
     born_ms = prof["born_pass"][0] / prof["born_pass"][1]
@@ -358,12 +378,8 @@ def run_b200(args):
         for r in range(args.replicas):
             hx[r] = eng.positions(r)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if ws > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = ws * args.replicas * args.dt * 1e-6 / e2e_s * 86400.0
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
+    e2e = aggregate_ns_per_day(ws, args.replicas, args.dt, e2e_s * 1e3)
 
     sasa_k = 0 if args.no_sasa else 2
     launches_plain = 9 + 2 + sasa_k
