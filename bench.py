@@ -364,27 +364,30 @@ def run_b200(args):
     force_tflops = 55 * pairs / (force_ms * 1e-3) / 1e12
     born_tflops = 60 * pairs / (born_ms * 1e-3) / 1e12
 
-    # ---- end to end through the C ABI with host buffers (headline arm)
+    # ---- end to end through the C ABI with host buffers (headline arm):
+    # every step the whole dynamic state goes host -> device from page-locked
+    # buffers (og_set_state: positions, velocities, the last forces, per-system
+    # counters), one step runs, and the state comes back (og_get_state)
     e2e_steps = max(3, min(args.steps, 20))
-    hx = [np.ascontiguousarray(eng.positions(r)) for r in range(args.replicas)]
-    hv = [np.ascontiguousarray(eng.velocities(r)) for r in range(args.replicas)]
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.int64): torch.int64, np.dtype(np.int32): torch.int32}
+    bufs = eng.state_buffers(alloc=lambda shape, dt: torch.empty(shape, dtype=tdt[np.dtype(dt)],
+                                                                 pin_memory=True).numpy())
+    state_bytes = sum(a.nbytes for a in bufs.values())
+    eng.get_state(out=bufs)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for r in range(args.replicas):
-            eng.set_positions(r, hx[r])
-            eng.set_velocities(r, hv[r])
+        eng.set_state(bufs)
         eng.step(1)
-        for r in range(args.replicas):
-            hx[r] = eng.positions(r)
+        eng.get_state(out=bufs)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws)
     e2e = aggregate_ns_per_day(ws, args.replicas, args.dt, e2e_s * 1e3)
 
+    # per step: BAOAB sub-steps and SHAKE (6), Born pass + finalize or
+    # descriptors + fused network (2), force, near field, bonded (3), SASA (2)
     sasa_k = 0 if args.no_sasa else 2
-    launches_plain = 9 + 2 + sasa_k
-    launches_learned = 7 + 2 + 5 + sasa_k  # descriptors, 3 GEMM layers, radii instead of Born pass + finalize
-    launches = launches_plain if args.plain_only else launches_learned
+    launches = 6 + 2 + 3 + sasa_k
     cfg = workload_config(args, chain)
     cfg["born"] = "plain OBC-II pass" if args.plain_only else "learned radii (network on tcgen05 GEMMs), plain-GB judge"
     line = {
@@ -414,8 +417,9 @@ def run_b200(args):
         "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / plain_ms) if "sasa" in prof else None,
         "born_pass_tflops": born_tflops,
         "pair_interactions_per_s": pairs / (ms_per_step * 1e-3) * ws,
-        "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": args.replicas * atoms * 6 * 8,
-                "d2h_bytes_per_step": args.replicas * atoms * 3 * 8},
+        "e2e": {"value": e2e, "unit": "ns/day", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes,
+                "path": "og_set_state (page-locked host state in) + og_step(1) + og_get_state (state out) per step"},
         "gpu_launches": args.steps * launches,
         "clocks": clk,
     }

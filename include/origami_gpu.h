@@ -45,7 +45,8 @@ typedef enum og_status {
   OG_E_NOMEM = 6,      /* device or host allocation failed */
   OG_E_STATE = 7,      /* call not valid in the engine's current state */
   OG_E_DATA = 8,       /* force-field / template table missing or malformed */
-  OG_E_UNSUPPORTED = 9 /* feature not built into this library */
+  OG_E_UNSUPPORTED = 9, /* feature not built into this library */
+  OG_E_IO = 10          /* a file could not be opened, read or written */
 } og_status;
 
 /* Human-readable text of the most recent error on this thread. */
@@ -247,6 +248,56 @@ og_status og_system_stats(og_engine* e, int32_t sys, int64_t* steps, int64_t* sh
 /* Instantaneous kinetic energy (langevin.rs:469) and temperature with
  * 3N degrees of freedom. */
 og_status og_kinetic(og_engine* e, int32_t sys, double* ke_kj_mol, double* temperature_k);
+
+/* ---- Whole-engine state, checkpoints and trajectory output.
+ * The reference writes trajectories as multi-MODEL PDB (io/src/pdb.rs:31
+ * write_pdb_trajectory) and has no binary checkpoint; both are here.
+ *
+ * og_state: the dynamic state of every system, systems in order, real atoms
+ * only (n_atoms = the sum of the systems' atom counts, og_engine_counts):
+ * positions and velocities (n_atoms x 3 doubles, A and A/ps), the forces of
+ * the last evaluation in the engine's fixed point (n_atoms x 3 int64, 2^32
+ * units per kJ/mol/A), and per system the step counter (which keys the
+ * O-step noise), SHAKE failure count, status word and temperature.  Restoring
+ * a state taken with og_get_state continues the run bit for bit.  Every
+ * pointer may be NULL: og_get_state skips that part; og_set_state keeps the
+ * engine's value, except that NULL forces (or new positions without forces)
+ * make the next step evaluate the forces first.  Host buffers may be
+ * pageable; page-locked buffers are copied by DMA without staging. */
+typedef struct og_state {
+  double* positions;
+  double* velocities;
+  int64_t* forces_fixed;
+  int64_t* steps;
+  int64_t* shake_failures;
+  int32_t* status;
+  double* temperature;
+} og_state;
+og_status og_engine_counts(const og_engine* e, int64_t* n_atoms, int32_t* n_systems);
+og_status og_get_state(og_engine* e, const og_state* out);
+og_status og_set_state(og_engine* e, const og_state* in);
+/* The state above (plus the learned-radius switch and judge phase) in a
+ * binary file: "OGCKPT01", u32 version 1, i32 systems, i64 atoms, i32 atoms
+ * per system, then the arrays in og_state order, little endian.  Loading
+ * requires an engine with the same systems' atom counts. */
+og_status og_save_checkpoint(og_engine* e, const char* path);
+og_status og_load_checkpoint(og_engine* e, const char* path);
+
+/* PDB output, record for record as io/src/pdb.rs: one model of a chain
+ * (write_pdb; xyz NULL = the chain's own positions), or a trajectory with
+ * one MODEL block per frame (write_pdb_trajectory).  A frame comes from host
+ * coordinates (og_trajectory_write) or from an engine system's device
+ * positions (og_trajectory_capture: the copy is queued on the engine's
+ * stream into page-locked memory and the call returns at once; the frame is
+ * formatted and written at a later capture, write or close, so writing
+ * overlaps the steps that follow).  The chain supplies names and residues;
+ * the system must have the chain's atom count. */
+typedef struct og_trajectory og_trajectory;
+og_status og_pdb_write(const og_chain* chain, const double* xyz, const char* title, const char* path);
+og_status og_trajectory_open(const og_chain* chain, const char* title, const char* path, og_trajectory** out);
+og_status og_trajectory_write(og_trajectory* t, const double* xyz);
+og_status og_trajectory_capture(og_trajectory* t, og_engine* e, int32_t sys);
+og_status og_trajectory_close(og_trajectory* t);
 
 /* Replica exchange (remd.rs:425-474): for each adjacent pair (a, a+1) with
  * a = parity, parity+2, ... of the temperature-sorted systems, Metropolis on

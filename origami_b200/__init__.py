@@ -121,6 +121,17 @@ class Chain:
             raise ValueError("position array has the wrong number of atoms")
         _check(lib().og_chain_set_positions(self._h, _dptr(x)))
 
+    def write_pdb(self, path: str, xyz: np.ndarray | None = None, title: str = "") -> None:
+        """One-model PDB of the chain (io/src/pdb.rs write_pdb); xyz defaults
+        to the chain's own positions."""
+        ptr = None
+        if xyz is not None:
+            x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+            if x.shape[0] != self.n_atoms:
+                raise ValueError("position array has the wrong number of atoms")
+            ptr = _dptr(x)
+        _check(lib().og_pdb_write(self._h, ptr, title.encode(), os.fsencode(path)))
+
     def topology_ptr(self) -> C.POINTER(F.og_topology):
         p = C.POINTER(F.og_topology)()
         _check(lib().og_chain_topology(self._h, C.byref(p)))
@@ -389,6 +400,62 @@ class Engine:
         _check(lib().og_compute_sasa(self._h, sys, codes[method], n_dots, _dptr(r)))
         return r
 
+    # ---- whole-engine state and checkpoints
+    STATE_PARTS = ("positions", "velocities", "forces_fixed", "steps", "shake_failures", "status", "temperature")
+
+    def counts(self) -> tuple[int, int]:
+        """(real atoms over all systems, systems)."""
+        n, s = C.c_int64(), C.c_int32()
+        _check(lib().og_engine_counts(self._h, C.byref(n), C.byref(s)))
+        return n.value, s.value
+
+    def state_buffers(self, alloc=np.empty) -> dict:
+        """Arrays shaped for og_state (alloc(shape, dtype) makes each one, e.g.
+        page-locked memory)."""
+        n, s = self.counts()
+        return {"positions": alloc((n, 3), np.float64), "velocities": alloc((n, 3), np.float64),
+                "forces_fixed": alloc((n, 3), np.int64), "steps": alloc((s,), np.int64),
+                "shake_failures": alloc((s,), np.int64), "status": alloc((s,), np.int32),
+                "temperature": alloc((s,), np.float64)}
+
+    @staticmethod
+    def _state_struct(d: dict) -> F.og_state:
+        st = F.og_state()
+        types = {"positions": (np.float64, F.c_double_p), "velocities": (np.float64, F.c_double_p),
+                 "forces_fixed": (np.int64, C.POINTER(C.c_int64)), "steps": (np.int64, C.POINTER(C.c_int64)),
+                 "shake_failures": (np.int64, C.POINTER(C.c_int64)), "status": (np.int32, F.c_int32_p),
+                 "temperature": (np.float64, F.c_double_p)}
+        for k, (dt, pt) in types.items():
+            a = d.get(k)
+            if a is None:
+                continue
+            if a.dtype != dt or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"state part {k!r} must be a C-contiguous {np.dtype(dt).name} array")
+            setattr(st, k, a.ctypes.data_as(pt))
+        return st
+
+    def get_state(self, out: dict | None = None, parts=STATE_PARTS) -> dict:
+        """The dynamic state of every system (og_get_state): filled into `out`
+        (e.g. page-locked arrays from state_buffers) or new arrays."""
+        d = out if out is not None else {k: v for k, v in self.state_buffers().items() if k in parts}
+        st = self._state_struct({k: d[k] for k in parts if k in d})
+        _check(lib().og_get_state(self._h, C.byref(st)))
+        return d
+
+    def set_state(self, state: dict) -> None:
+        """Restores any subset of a state taken with get_state (og_set_state)."""
+        st = self._state_struct(state)
+        _check(lib().og_set_state(self._h, C.byref(st)))
+        if state.get("temperature") is not None:
+            self._temps = [float(t) for t in state["temperature"]]
+
+    def save_checkpoint(self, path: str) -> None:
+        _check(lib().og_save_checkpoint(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path: str) -> None:
+        _check(lib().og_load_checkpoint(self._h, os.fsencode(path)))
+        self._temps = [float(t) for t in self.get_state(parts=("temperature",))["temperature"]]
+
     def energies(self, sys: int = 0) -> dict:
         e = F.og_energies()
         _check(lib().og_compute_energies(self._h, sys, C.byref(e)))
@@ -435,6 +502,45 @@ class Engine:
 
 
 # ------------------------------------------------------------------ drivers
+
+class Trajectory:
+    """Multi-MODEL PDB trajectory (io/src/pdb.rs write_pdb_trajectory): one
+    MODEL block per frame, from host coordinates (write) or from an engine
+    system's device positions (capture: queued on the engine's stream into
+    page-locked memory; written after the next capture or at close)."""
+
+    def __init__(self, chain: Chain, path: str, title: str = ""):
+        h = C.c_void_p()
+        _check(lib().og_trajectory_open(chain._h, title.encode(), os.fsencode(path), C.byref(h)))
+        self._h = h
+        self.n_atoms = chain.n_atoms
+
+    def write(self, xyz: np.ndarray) -> None:
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        if x.shape[0] != self.n_atoms:
+            raise ValueError("position array has the wrong number of atoms")
+        _check(lib().og_trajectory_write(self._h, _dptr(x)))
+
+    def capture(self, engine: "Engine", sys: int = 0) -> None:
+        _check(lib().og_trajectory_capture(self._h, engine._h, sys))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            h, self._h = self._h, None
+            _check(lib().og_trajectory_close(h))
+
+    def __enter__(self) -> "Trajectory":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 class Xoshiro256pp:
     """xoshiro256++ with SplitMix64 seeding and cached Box-Muller (dynamics/src/rng.rs)."""

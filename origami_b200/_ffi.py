@@ -17,7 +17,7 @@ LGB_N_PARAMS = 43537  # OG_LGB_N_PARAMS
 LGB_N_INPUT = 80      # OG_LGB_N_INPUT
 STATUS_NAMES = {
     0: "OG_OK", 1: "OG_E_BADARG", 2: "OG_E_NONFINITE", 3: "OG_E_SHAKE", 4: "OG_E_TIMEOUT",
-    5: "OG_E_CUDA", 6: "OG_E_NOMEM", 7: "OG_E_STATE", 8: "OG_E_DATA", 9: "OG_E_UNSUPPORTED",
+    5: "OG_E_CUDA", 6: "OG_E_NOMEM", 7: "OG_E_STATE", 8: "OG_E_DATA", 9: "OG_E_UNSUPPORTED", 10: "OG_E_IO",
 }
 
 
@@ -63,8 +63,26 @@ class og_kernel_time(C.Structure):
     _fields_ = [("name", C.c_char_p), ("ms", C.c_double), ("launches", C.c_int64)]
 
 
+class og_state(C.Structure):
+    _fields_ = [
+        ("positions", c_double_p), ("velocities", c_double_p), ("forces_fixed", C.POINTER(C.c_int64)),
+        ("steps", C.POINTER(C.c_int64)), ("shake_failures", C.POINTER(C.c_int64)), ("status", c_int32_p),
+        ("temperature", c_double_p),
+    ]
+
+
 # (name, restype, argtypes) of every exported symbol.
 SIGNATURES = [
+    ("og_engine_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), c_int32_p]),
+    ("og_get_state", C.c_int, [C.c_void_p, C.POINTER(og_state)]),
+    ("og_set_state", C.c_int, [C.c_void_p, C.POINTER(og_state)]),
+    ("og_save_checkpoint", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("og_load_checkpoint", C.c_int, [C.c_void_p, C.c_char_p]),
+    ("og_pdb_write", C.c_int, [C.c_void_p, c_double_p, C.c_char_p, C.c_char_p]),
+    ("og_trajectory_open", C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("og_trajectory_write", C.c_int, [C.c_void_p, c_double_p]),
+    ("og_trajectory_capture", C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    ("og_trajectory_close", C.c_int, [C.c_void_p]),
     ("og_last_error", C.c_char_p, []),
     ("og_status_string", C.c_char_p, [C.c_int]),
     ("og_version", C.c_char_p, []),

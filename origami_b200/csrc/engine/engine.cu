@@ -19,11 +19,13 @@
 #include <vector>
 
 #include "../../../include/origami_gpu.h"
+#include "../host/pdb.h"
 #include "../host/status.h"
 #include "common.cuh"
 #include "lgb.cuh"
 #include "pair_kernels.cuh"
 #include "sasa.cuh"
+#include "state.cuh"
 #include "tc_gemm.cuh"
 #include "step_kernels.cuh"
 
@@ -170,6 +172,11 @@ struct og_engine {
   DVec<double> born_r, born_r64, integral64, e_lj, e_coul, e_gb, e_self;
   DVec<unsigned long long> fx, fy, fz, born_sum;
   DVec<int32_t> atom_sys, local_idx, atom_valid, n_pairs;
+  // real atom (systems in order) -> padded index; AoS staging of og_state
+  DVec<int32_t> real_map;
+  int64_t n_real = 0;
+  DVec<double> stage_a, stage_b;
+  DVec<int64_t> stage_f;
   DVec<float> pq, lj, gb;  // tile-SoA, 4 columns per 32-atom tile
   DVec<double4> origin;
   DVec<ogk::SysState> sys_state;
@@ -712,6 +719,13 @@ og_status finalize_impl(og_engine* e) {
   OG_CUDA(e->rho.upload(hrho, st)); OG_CUDA(e->rho_tilde.upload(hrt, st)); OG_CUDA(e->srho.upload(hsr, st));
   OG_CUDA(e->atom_sys.upload(hsys, st)); OG_CUDA(e->local_idx.upload(hloc, st));
   OG_CUDA(e->atom_valid.upload(hvalid, st)); OG_CUDA(e->lj.upload(hlj, st));
+  {
+    std::vector<int32_t> hmap;
+    for (const auto& s : e->sys)
+      for (int k = 0; k < s.topo.n; ++k) hmap.push_back(s.atom_begin + k);
+    e->n_real = static_cast<int64_t>(hmap.size());
+    OG_CUDA(e->real_map.upload(hmap, st));
+  }
   std::vector<double> zeros(np, 0.0);
   OG_CUDA(e->vx.upload(zeros, st)); OG_CUDA(e->vy.upload(zeros, st)); OG_CUDA(e->vz.upload(zeros, st));
   OG_CUDA(e->rx.upload(zeros, st)); OG_CUDA(e->ry.upload(zeros, st)); OG_CUDA(e->rz.upload(zeros, st));
@@ -1531,6 +1545,224 @@ og_status og_kinetic(og_engine* e, int32_t s, double* ke, double* temp) {
   const double dof = 3.0 * e->sys[s].topo.n;
   if (ke) *ke = h[s];
   if (temp) *temp = dof > 0.0 ? 2.0 * h[s] / (dof * ogk::kBoltzmann) : 0.0;
+  return OG_OK;
+}
+
+// ---------------------------------------------------------------- og_state
+namespace {
+
+og_status ensure_stage(og_engine* e) {
+  const size_t n3 = 3 * static_cast<size_t>(e->n_real);
+  if (e->stage_a.n != n3) OG_CUDA(e->stage_a.alloc(n3));
+  if (e->stage_b.n != n3) OG_CUDA(e->stage_b.alloc(n3));
+  if (e->stage_f.n != n3) OG_CUDA(e->stage_f.alloc(n3));
+  return OG_OK;
+}
+
+}  // namespace
+
+og_status og_engine_counts(const og_engine* e, int64_t* n_atoms, int32_t* n_systems) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (n_atoms) *n_atoms = e->n_real;
+  if (n_systems) *n_systems = static_cast<int32_t>(e->sys.size());
+  return OG_OK;
+}
+
+og_status og_get_state(og_engine* e, const og_state* out) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!out) return og_fail(OG_E_BADARG, "null state");
+  if ((st = ensure_stage(e)) != OG_OK) return st;
+  const size_t bytes = sizeof(double) * 3 * static_cast<size_t>(e->n_real);
+  cudaStream_t s = e->stream;
+  if (out->positions) {
+    ogk::launch_gather_xyz(e->x.p, e->y.p, e->z.p, e->real_map.p, e->n_real, e->stage_a.p, s);
+    OG_CUDA(cudaMemcpyAsync(out->positions, e->stage_a.p, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if (out->velocities) {
+    ogk::launch_gather_xyz(e->vx.p, e->vy.p, e->vz.p, e->real_map.p, e->n_real, e->stage_b.p, s);
+    OG_CUDA(cudaMemcpyAsync(out->velocities, e->stage_b.p, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if (out->forces_fixed) {
+    ogk::launch_gather_fixed(e->fx.p, e->fy.p, e->fz.p, e->real_map.p, e->n_real, e->stage_f.p, s);
+    OG_CUDA(cudaMemcpyAsync(out->forces_fixed, e->stage_f.p, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  if ((st = launch_check("state gather")) != OG_OK) return st;
+  std::vector<ogk::SysState> hs;
+  if ((st = read_status(e, &hs)) != OG_OK) return st;  // also waits for the copies
+  for (size_t k = 0; k < hs.size(); ++k) {
+    if (out->steps) out->steps[k] = hs[k].steps;
+    if (out->shake_failures) out->shake_failures[k] = hs[k].shake_failures;
+    if (out->status) out->status[k] = hs[k].status;
+    if (out->temperature) out->temperature[k] = hs[k].temperature;
+  }
+  return OG_OK;
+}
+
+og_status og_set_state(og_engine* e, const og_state* in) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!in) return og_fail(OG_E_BADARG, "null state");
+  if ((st = ensure_stage(e)) != OG_OK) return st;
+  const size_t bytes = sizeof(double) * 3 * static_cast<size_t>(e->n_real);
+  cudaStream_t s = e->stream;
+  if (in->positions) {
+    OG_CUDA(cudaMemcpyAsync(e->stage_a.p, in->positions, bytes, cudaMemcpyHostToDevice, s));
+    ogk::launch_scatter_xyz(e->stage_a.p, e->real_map.p, e->n_real, e->x.p, e->y.p, e->z.p, s);
+  }
+  if (in->velocities) {
+    OG_CUDA(cudaMemcpyAsync(e->stage_b.p, in->velocities, bytes, cudaMemcpyHostToDevice, s));
+    ogk::launch_scatter_xyz(e->stage_b.p, e->real_map.p, e->n_real, e->vx.p, e->vy.p, e->vz.p, s);
+  }
+  if (in->forces_fixed) {
+    OG_CUDA(cudaMemcpyAsync(e->stage_f.p, in->forces_fixed, bytes, cudaMemcpyHostToDevice, s));
+    ogk::launch_scatter_fixed(e->stage_f.p, e->real_map.p, e->n_real, e->fx.p, e->fy.p, e->fz.p, s);
+  }
+  if ((st = launch_check("state scatter")) != OG_OK) return st;
+  if (in->steps || in->shake_failures || in->status || in->temperature) {
+    std::vector<ogk::SysState> hs;
+    if ((st = read_status(e, &hs)) != OG_OK) return st;
+    for (size_t k = 0; k < hs.size(); ++k) {
+      if (in->steps) hs[k].steps = in->steps[k];
+      if (in->shake_failures) hs[k].shake_failures = in->shake_failures[k];
+      if (in->status) hs[k].status = in->status[k];
+      if (in->temperature) {
+        if (!(in->temperature[k] >= 0.0)) return og_fail(OG_E_BADARG, "temperature must be >= 0");
+        hs[k].temperature = in->temperature[k];
+        hs[k].kbt = ogk::kBoltzmann * in->temperature[k];
+        e->sys[k].temperature = in->temperature[k];
+      }
+    }
+    OG_CUDA(cudaMemcpyAsync(e->sys_state.p, hs.data(), sizeof(ogk::SysState) * hs.size(), cudaMemcpyHostToDevice, s));
+  }
+  if (in->forces_fixed)
+    e->forces_valid = true;
+  else if (in->positions)
+    e->forces_valid = false;
+  OG_CUDA(cudaStreamSynchronize(s));  // the caller's buffers are free on return
+  return OG_OK;
+}
+
+// ------------------------------------------------------------ checkpoints
+namespace {
+
+constexpr char kCkptMagic[8] = {'O', 'G', 'C', 'K', 'P', 'T', '0', '1'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct HostState {
+  std::vector<double> x, v, temp;
+  std::vector<int64_t> f, steps, fails;
+  std::vector<int32_t> status;
+  explicit HostState(int64_t n, size_t n_sys)
+      : x(3 * n), v(3 * n), temp(n_sys), f(3 * n), steps(n_sys), fails(n_sys), status(n_sys) {}
+  og_state view() {
+    return og_state{x.data(), v.data(), f.data(), steps.data(), fails.data(), status.data(), temp.data()};
+  }
+};
+
+extern "C++" {
+template <typename T>
+bool put(FILE* f, const T* p, size_t n) { return std::fwrite(p, sizeof(T), n, f) == n; }
+template <typename T>
+bool get(FILE* f, T* p, size_t n) { return std::fread(p, sizeof(T), n, f) == n; }
+}
+
+}  // namespace
+
+og_status og_save_checkpoint(og_engine* e, const char* path) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!path) return og_fail(OG_E_BADARG, "null path");
+  const size_t n_sys = e->sys.size();
+  if (!e->forces_valid && (st = eval_forces(e)) != OG_OK) return st;
+  HostState h(e->n_real, n_sys);
+  const og_state v = h.view();
+  if ((st = og_get_state(e, &v)) != OG_OK) return st;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return og_fail(OG_E_IO, std::string("cannot open ") + path);
+  const int32_t ns = static_cast<int32_t>(n_sys);
+  const int64_t na = e->n_real;
+  std::vector<int32_t> counts;
+  for (const auto& s : e->sys) counts.push_back(s.topo.n);
+  const int32_t lgb_active = e->lgb_active ? 1 : 0;
+  const int64_t since = e->lgb_since_judge;
+  bool ok = put(f, kCkptMagic, 8) && put(f, &kCkptVersion, 1) && put(f, &ns, 1) && put(f, &na, 1) &&
+            put(f, counts.data(), n_sys) && put(f, h.x.data(), h.x.size()) && put(f, h.v.data(), h.v.size()) &&
+            put(f, h.f.data(), h.f.size()) && put(f, h.steps.data(), n_sys) && put(f, h.fails.data(), n_sys) &&
+            put(f, h.status.data(), n_sys) && put(f, h.temp.data(), n_sys) && put(f, &lgb_active, 1) &&
+            put(f, &since, 1);
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return og_fail(OG_E_IO, std::string("checkpoint write failed: ") + path);
+  return OG_OK;
+}
+
+og_status og_load_checkpoint(og_engine* e, const char* path) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (!path) return og_fail(OG_E_BADARG, "null path");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return og_fail(OG_E_IO, std::string("cannot open ") + path);
+  const size_t n_sys = e->sys.size();
+  char magic[8];
+  uint32_t version = 0;
+  int32_t ns = 0, lgb_active = 0;
+  int64_t na = 0, since = 0;
+  bool ok = get(f, magic, 8) && std::memcmp(magic, kCkptMagic, 8) == 0 && get(f, &version, 1) &&
+            version == kCkptVersion && get(f, &ns, 1) && get(f, &na, 1);
+  if (!ok) {
+    std::fclose(f);
+    return og_fail(OG_E_DATA, std::string("not an origami-b200 checkpoint: ") + path);
+  }
+  std::vector<int32_t> counts(ns > 0 ? ns : 0);
+  ok = static_cast<size_t>(ns) == n_sys && na == e->n_real && get(f, counts.data(), counts.size());
+  for (size_t k = 0; ok && k < n_sys; ++k) ok = counts[k] == e->sys[k].topo.n;
+  if (!ok) {
+    std::fclose(f);
+    return og_fail(OG_E_BADARG, "checkpoint systems differ from the engine's");
+  }
+  HostState h(na, n_sys);
+  ok = get(f, h.x.data(), h.x.size()) && get(f, h.v.data(), h.v.size()) && get(f, h.f.data(), h.f.size()) &&
+       get(f, h.steps.data(), n_sys) && get(f, h.fails.data(), n_sys) && get(f, h.status.data(), n_sys) &&
+       get(f, h.temp.data(), n_sys) && get(f, &lgb_active, 1) && get(f, &since, 1);
+  std::fclose(f);
+  if (!ok) return og_fail(OG_E_DATA, std::string("truncated checkpoint: ") + path);
+  const og_state v = h.view();
+  if ((st = og_set_state(e, &v)) != OG_OK) return st;
+  if (!lgb_active && e->lgb_active) {
+    e->lgb_active = false;  // the run had fallen back to plain GB
+    reset_graph(e);
+  }
+  e->lgb_since_judge = since;
+  return OG_OK;
+}
+
+// ---------------------------------------------------- trajectory capture
+og_status og_trajectory_capture(og_trajectory* t, og_engine* e, int32_t s) {
+  og_status st = check_sys(e, s);
+  if (st != OG_OK) return st;
+  if (!t) return og_fail(OG_E_BADARG, "null trajectory");
+  const SysHost& sh = e->sys[s];
+  if (sh.topo.n != t->layout.n_atoms) return og_fail(OG_E_BADARG, "system and chain atom counts differ");
+  const size_t bytes = sizeof(double) * 3 * static_cast<size_t>(sh.topo.n);
+  if (!t->staging) {
+    OG_CUDA(cudaMalloc(reinterpret_cast<void**>(&t->staging), bytes));
+    for (int k = 0; k < 2; ++k) {
+      OG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&t->pinned[k]), bytes, cudaHostAllocDefault));
+      OG_CUDA(cudaEventCreateWithFlags(&t->copied[k], cudaEventDisableTiming));
+    }
+  }
+  // the slot's previous frame (two captures ago) is written first; the
+  // frame captured last stays in flight
+  const int slot = static_cast<int>(t->captures & 1);
+  if (t->pending[slot] >= 0 && (st = og_trajectory_flush(t, t->captures - 1)) != OG_OK) return st;
+  int64_t first = 0;  // the system's first real atom
+  for (int32_t k = 0; k < s; ++k) first += e->sys[k].topo.n;
+  ogk::launch_gather_xyz(e->x.p, e->y.p, e->z.p, e->real_map.p + first, sh.topo.n, t->staging, e->stream);
+  OG_CUDA(cudaMemcpyAsync(t->pinned[slot], t->staging, bytes, cudaMemcpyDeviceToHost, e->stream));
+  OG_CUDA(cudaEventRecord(t->copied[slot], e->stream));
+  if ((st = launch_check("trajectory gather")) != OG_OK) return st;
+  t->pending[slot] = t->captures++;
   return OG_OK;
 }
 

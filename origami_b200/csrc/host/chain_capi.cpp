@@ -16,6 +16,7 @@
 #include <string>
 
 #include "../../../include/origami_gpu.h"
+#include "chain.h"
 #include "model.h"
 #include "status.h"
 
@@ -79,21 +80,6 @@ double gb_hct_scale(og::Element e) {  // energy/src/gb.rs:73-83
 }
 
 }  // namespace
-
-struct og_chain {
-  og::Structure s;
-  // Flattened arrays backing `topo`.
-  std::vector<double> charge, rmin, eps, rmin14, eps14, rho, scale, mass;
-  std::vector<int32_t> element, atom_type, residue_of;
-  std::vector<int32_t> bond_atoms, angle_atoms, dih_atoms, dih_start, term_n, imp_atoms;
-  std::vector<double> bond_k, bond_r0, angle_k, angle_t0, term_k, term_delta, imp_k, imp_psi0;
-  std::vector<int32_t> excl_atoms, cons_atoms;
-  std::vector<int8_t> excl_kind;
-  std::vector<double> cons_d;
-  int32_t missing = 0;
-  og_topology topo{};
-  bool dirty = true;
-};
 
 namespace {
 

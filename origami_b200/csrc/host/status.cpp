@@ -25,6 +25,7 @@ const char* og_status_string(int s) {
     case OG_E_STATE: return "invalid engine state";
     case OG_E_DATA: return "force-field or template data error";
     case OG_E_UNSUPPORTED: return "unsupported";
+    case OG_E_IO: return "file i/o error";
     default: return "unknown status";
   }
 }
