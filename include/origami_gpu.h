@@ -218,6 +218,17 @@ og_status og_get_velocities(og_engine* e, int32_t sys, double* v);
 og_status og_init_velocities(og_engine* e, int32_t sys, uint64_t seed, int32_t remove_com);
 og_status og_set_temperature(og_engine* e, int32_t sys, double temperature_k);
 
+/* External potential of co-translational folding (cotranslate.rs:119-154
+ * CylindricalTunnel): every real atom of every system whose projection on
+ * the axis origin + t * direction lies within [0, length_a] and whose
+ * distance d from the axis exceeds radius_a feels k_confine (d - radius_a)
+ * toward the axis (kJ/mol/A; direction used as given, a unit vector).  Added
+ * to og_compute_forces and every og_step force evaluation; not an energy
+ * term (the reference's ExternalPotential has none).  origin or direction
+ * NULL removes it. */
+og_status og_set_tunnel(og_engine* e, const double* origin, const double* direction, double radius_a,
+                        double length_a, double k_confine);
+
 /* Forces at the current positions of every system: replaces
  * total_force_with_scratch (forces.rs:78).  f_out (optional) receives
  * 3*n_atoms doubles for system `sys` (or nothing when NULL).  The same
@@ -255,7 +266,7 @@ og_status og_kinetic(og_engine* e, int32_t sys, double* ke_kj_mol, double* tempe
  *
  * og_state: the dynamic state of every system, systems in order, real atoms
  * only (n_atoms = the sum of the systems' atom counts, og_engine_counts):
- * positions and velocities (n_atoms x 3 doubles, A and A/ps), the forces of
+ * positions and velocities (n_atoms x 3 doubles, A and A/fs), the forces of
  * the last evaluation in the engine's fixed point (n_atoms x 3 int64, 2^32
  * units per kJ/mol/A), and per system the step counter (which keys the
  * O-step noise), SHAKE failure count, status word and temperature.  Restoring

@@ -74,6 +74,7 @@ class og_state(C.Structure):
 # (name, restype, argtypes) of every exported symbol.
 SIGNATURES = [
     ("og_engine_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), c_int32_p]),
+    ("og_set_tunnel", C.c_int, [C.c_void_p, c_double_p, c_double_p, C.c_double, C.c_double, C.c_double]),
     ("og_get_state", C.c_int, [C.c_void_p, C.POINTER(og_state)]),
     ("og_set_state", C.c_int, [C.c_void_p, C.POINTER(og_state)]),
     ("og_save_checkpoint", C.c_int, [C.c_void_p, C.c_char_p]),

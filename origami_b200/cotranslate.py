@@ -1,0 +1,160 @@
+"""Co-translational chain growth on the GPU (dynamics/src/cotranslate.rs).
+
+The driver alternates, as run_cotranslate (cotranslate.rs:174-313) does,
+between emitting the next residue -- appended with origami's NeRF builder,
+relieved by a short L-BFGS, new atoms seeded with Maxwell-Boltzmann
+velocities from the run's xoshiro stream (langevin.rs:417-447) -- and a
+BAOAB slice up to the next emission time (run_slice, cotranslate.rs:315-384:
+no SHAKE, the ribosome's exit tunnel as an external force, reference
+cutoffs).  A tail slice of tail_steps follows the last residue.
+
+Each slice runs in a one-system engine built from the grown chain's
+topology: the per-system tables (bonded terms, exclusion tile masks, SHAKE
+clusters) are rebuilt in O(atoms), and the tile work lists in O(tiles^2),
+where the reference rebuilds its O(N^2) exclusion matrix every slice
+(scratch.rs:233-251).  Positions and velocities carry over between slices;
+the engine's O-step noise is keyed by the run's global step count, so no
+slice repeats another's noise.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (BOLTZMANN_KJ_PER_MOL_K, Chain, Engine, LangevinOptions, Params, Xoshiro256pp, _check, _dptr, lib)
+from .minimize import MinimizeOptions, minimize_chain
+
+ACCEL_FACTOR = 1.0e-4  # langevin.rs ACCEL_FACTOR: kJ/mol/A/Da -> A/fs^2
+
+
+@dataclass
+class UniformRibosome:
+    """Residue i is emitted at i * interval_fs (cotranslate.rs:64-88)."""
+    sequence: str
+    interval_fs: float
+
+    def emission_time_fs(self, residue_idx: int) -> float:
+        return residue_idx * max(self.interval_fs, 0.0)
+
+
+@dataclass
+class CylindricalTunnel:
+    """Soft exit-tunnel confinement (cotranslate.rs:100-154); defaults as
+    CylindricalTunnel::default."""
+    axis_origin: tuple = (0.0, 0.0, 0.0)
+    axis_direction: tuple = (0.0, 0.0, 1.0)
+    radius_a: float = 12.0
+    length_a: float = 80.0
+    k_confine: float = 50.0
+
+    def apply_to(self, engine: Engine) -> None:
+        o = np.ascontiguousarray(self.axis_origin, dtype=np.float64)
+        d = np.ascontiguousarray(self.axis_direction, dtype=np.float64)
+        _check(lib().og_set_tunnel(engine._h, _dptr(o), _dptr(d), float(self.radius_a), float(self.length_a),
+                                   float(self.k_confine)))
+
+
+@dataclass
+class CotranslateFrame:
+    """cotranslate.rs:158-163."""
+    time_fs: float
+    residue_count: int
+    positions: np.ndarray
+    instantaneous_temperature_k: float
+
+
+# minimize after every append (cotranslate.rs:218-231)
+APPEND_MINIMIZE = MinimizeOptions(max_steps=200, gradient_tol=10.0, energy_tol=0.1, max_step_a=0.1)
+
+
+def seed_new_atom_velocities(chain: Chain, velocities: np.ndarray, temperature_k: float,
+                             rng: Xoshiro256pp) -> np.ndarray:
+    """Existing atoms keep their velocities; atoms added since get
+    sigma * gaussian per component, sigma = sqrt(kB T ACCEL / m), drawn x, y,
+    z per atom in atom order (langevin.rs:417-447)."""
+    n = chain.n_atoms
+    old = velocities.shape[0]
+    if n <= old:
+        return velocities
+    mass = chain.topology().mass
+    kbt = BOLTZMANN_KJ_PER_MOL_K * temperature_k
+    out = np.empty((n, 3))
+    out[:old] = velocities
+    for i in range(old, n):
+        sigma = math.sqrt(kbt * ACCEL_FACTOR / mass[i])
+        out[i] = [sigma * rng.gaussian(), sigma * rng.gaussian(), sigma * rng.gaussian()]
+    return out
+
+
+def _temperature(velocities: np.ndarray, mass: np.ndarray) -> float:
+    ke = 0.5 * float((mass[:, None] * velocities * velocities).sum()) / ACCEL_FACTOR
+    dof = 3.0 * velocities.shape[0]
+    return 2.0 * ke / (dof * BOLTZMANN_KJ_PER_MOL_K) if dof > 0 else 0.0
+
+
+def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: CylindricalTunnel | None = None,
+                    callback=None, params: Params | None = None) -> Chain | None:
+    """Grows the ribosome's sequence residue by residue with dynamics in
+    between (cotranslate.rs:174-313); returns the final chain (None for an
+    empty sequence).  callback(CotranslateFrame) receives every save_every-th
+    step of each slice, and the emission moment of a slice with no steps."""
+    seq = ribosome.sequence
+    if not seq:
+        return None
+    base = params or Params()
+    rng = Xoshiro256pp(opts.seed)
+    chain: Chain | None = None
+    velocities = np.zeros((0, 3))
+    clock_fs = 0.0
+    steps_done = 0
+    for i, aa in enumerate(seq):
+        clock_fs = max(clock_fs, ribosome.emission_time_fs(i))
+        if chain is None:
+            chain = Chain.build(aa)
+        else:
+            chain.append(aa)
+        minimize_chain(chain, params=Params(nb_cutoff=base.nb_cutoff, born_cutoff=base.born_cutoff,
+                                            gb_force_cutoff=base.gb_force_cutoff), opts=APPEND_MINIMIZE)
+        velocities = seed_new_atom_velocities(chain, velocities, opts.temperature_k, rng)
+        target = ribosome.emission_time_fs(i + 1) if i + 1 < len(seq) else clock_fs + tail_steps * opts.dt_fs
+        n_steps = int(round(max(target - clock_fs, 0.0) / opts.dt_fs))
+        if n_steps == 0:
+            if callback:
+                callback(CotranslateFrame(clock_fs, i + 1, chain.positions,
+                                          _temperature(velocities, chain.topology().mass)))
+            continue
+        clock_fs, steps_done, velocities = _run_slice(chain, velocities, opts, n_steps, external, base, clock_fs,
+                                                      steps_done, i + 1, callback)
+    return chain
+
+
+def _run_slice(chain: Chain, velocities: np.ndarray, opts: LangevinOptions, n_steps: int,
+               external: CylindricalTunnel | None, base: Params, clock_fs: float, steps_done: int,
+               residue_count: int, callback):
+    p = Params(nb_cutoff=base.nb_cutoff, born_cutoff=base.born_cutoff, gb_force_cutoff=base.gb_force_cutoff,
+               dt_fs=opts.dt_fs, friction_ps_inv=opts.friction_ps_inv, constrain_h_bonds=False,
+               include_sasa=opts.include_sasa, sasa_gamma_scale=base.sasa_gamma_scale, seed=opts.seed)
+    eng = Engine(p)
+    try:
+        eng.add_system(chain, chain.positions, opts.temperature_k)
+        eng.finalize()
+        if external is not None:
+            external.apply_to(eng)
+        eng.set_state({"velocities": np.ascontiguousarray(velocities, dtype=np.float64),
+                       "steps": np.array([steps_done], dtype=np.int64)})
+        chunk = opts.save_every if opts.save_every > 0 else n_steps
+        done = 0
+        while done < n_steps:
+            k = min(chunk, n_steps - done)
+            eng.step(k)
+            done += k
+            if callback and opts.save_every > 0 and done % opts.save_every == 0:
+                _, t_inst = eng.kinetic(0)
+                callback(CotranslateFrame(clock_fs + done * opts.dt_fs, residue_count, eng.positions(0), t_inst))
+        chain.positions = eng.positions(0)
+        velocities = eng.velocities(0)
+    finally:
+        eng.close()
+    return clock_fs + n_steps * opts.dt_fs, steps_done + n_steps, velocities

@@ -232,6 +232,9 @@ struct og_engine {
   int lgb_judge_interval = 500, lgb_judged = 0;
   double lgb_tol = 1e-3, lgb_last_err = -1.0;
   int64_t lgb_since_judge = 0;
+  // external potential: the cotranslation exit tunnel
+  bool tunnel_on = false;
+  ogk::TunnelParams tunnel{};
   double sasa_rmax = 0.0;
   // graph
   cudaGraph_t graph = nullptr;
@@ -480,6 +483,10 @@ struct og_engine {
     if (p.include_sasa) {
       Timer t(this, "sasa");
       ogk::launch_sasa_forces(sasa_args(false), stream);
+    }
+    if (tunnel_on) {
+      Timer t(this, "tunnel");
+      ogk::launch_tunnel(atoms(), tunnel, stream);
     }
   }
 
@@ -1338,6 +1345,23 @@ og_status og_set_temperature(og_engine* e, int32_t s, double t) {
   OG_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(e->sys_state.p + s) + offsetof(ogk::SysState, kbt), &kbt,
                           sizeof(double), cudaMemcpyHostToDevice, e->stream));
   OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+og_status og_set_tunnel(og_engine* e, const double* origin, const double* direction, double radius_a,
+                        double length_a, double k_confine) {
+  if (!e) return og_fail(OG_E_BADARG, "null engine");
+  if (!origin || !direction) {
+    e->tunnel_on = false;
+  } else {
+    if (!(radius_a >= 0.0) || !(length_a >= 0.0) || !std::isfinite(k_confine))
+      return og_fail(OG_E_BADARG, "tunnel radius and length must be >= 0 and k finite");
+    e->tunnel = ogk::TunnelParams{origin[0],    origin[1],    origin[2], direction[0], direction[1],
+                                  direction[2], radius_a, length_a, k_confine};
+    e->tunnel_on = true;
+  }
+  e->forces_valid = false;
+  if (e->finalized) reset_graph(e);
   return OG_OK;
 }
 

@@ -494,4 +494,29 @@ void launch_kinetic(const AtomArrays& a, const int32_t* begin, const int32_t* en
   if (n_sys > 0) k_kinetic<<<n_sys, kRedThreads, 0, s>>>(a, begin, end, out);
 }
 
+namespace {
+
+// One thread per atom; it owns its accumulators here (the force kernels
+// have finished in stream order), so a plain add suffices.
+__global__ void k_tunnel(AtomArrays a, TunnelParams t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_padded || a.atom_sys[i] < 0) return;
+  const double rx = a.x[i] - t.ox, ry = a.y[i] - t.oy, rz = a.z[i] - t.oz;
+  const double along = rx * t.dx + ry * t.dy + rz * t.dz;
+  if (along < 0.0 || along > t.length) return;
+  const double px = rx - t.dx * along, py = ry - t.dy * along, pz = rz - t.dz * along;
+  const double d = sqrt(px * px + py * py + pz * pz);
+  if (!(d > t.radius)) return;
+  const double s = -t.k * (d - t.radius) / d;
+  a.fx[i] += static_cast<unsigned long long>(__double2ll_rn(s * px * kForceScale));
+  a.fy[i] += static_cast<unsigned long long>(__double2ll_rn(s * py * kForceScale));
+  a.fz[i] += static_cast<unsigned long long>(__double2ll_rn(s * pz * kForceScale));
+}
+
+}  // namespace
+
+void launch_tunnel(const AtomArrays& a, const TunnelParams& t, cudaStream_t s) {
+  k_tunnel<<<blocks_for(a.n_padded, 256), 256, 0, s>>>(a, t);
+}
+
 }  // namespace ogk

@@ -115,6 +115,18 @@ void launch_segment_sum(const double* v, const int32_t* begin, const int32_t* en
 void launch_swap_systems(const AtomArrays& a, int32_t begin_a, int32_t begin_b, int32_t n, double scale_a,
                          double scale_b, cudaStream_t s);
 
+// Soft cylindrical exit tunnel (cotranslate.rs:119-154 CylindricalTunnel):
+// an atom whose projection on the axis (origin + t * direction, direction
+// used as given -- a unit vector) lies within [0, length] and whose distance
+// from the axis exceeds the radius feels k (d - radius) back toward the
+// axis; added to the fixed-point forces of every real atom.
+struct TunnelParams {
+  double ox, oy, oz;  // axis origin, A
+  double dx, dy, dz;  // axis direction
+  double radius, length, k;  // A, A, kJ/mol/A^2
+};
+void launch_tunnel(const AtomArrays& a, const TunnelParams& t, cudaStream_t s);
+
 // Kinetic energy per system: sum m v^2 / 2 / ACCEL (langevin.rs:469-475).
 void launch_kinetic(const AtomArrays& a, const int32_t* begin, const int32_t* end, int32_t n_sys, double* out,
                     cudaStream_t s);
