@@ -190,6 +190,10 @@ struct og_engine {
   DVec<int4> near;
   DVec<ogk::PairWork> work_f;   // far-field force: upper-triangle tile pairs
   DVec<int32_t> jlist_f;
+  // cutoff mode: i-blocks of the two lists, their culled j lists and ends
+  DVec<ogk::CutBlock> cut_b, cut_f;
+  DVec<int32_t> jlist_cut_b, jlist_cut_f, seg_end_b, seg_end_f;
+  int n_cut_b = 0, n_cut_f = 0;
   int n_work = 0, n_near = 0, n_work_f = 0;
   // bonded
   DVec<int2> bond_atoms, dih_terms;
@@ -457,7 +461,14 @@ struct og_engine {
     } else {
       {
         Timer t(this, "born_pass");
-        ogk::launch_born_pass(pa, stream);
+        ogk::PairArgs pb = pa;
+        if (!no_cutoff(p.born_cutoff)) {
+          ogk::launch_cut_lists(cut_b.p, n_cut_b, jlist.p, origin.p, p.born_cutoff, jlist_cut_b.p, seg_end_b.p,
+                                stream);
+          pb.jlist = jlist_cut_b.p;
+          pb.seg_end = seg_end_b.p;
+        }
+        ogk::launch_born_pass(pb, stream);
       }
       {
         Timer t(this, "born_finalize");
@@ -470,6 +481,12 @@ struct og_engine {
       pf.work = work_f.p;
       pf.n_work = n_work_f;
       pf.jlist = jlist_f.p;
+      if (!no_cutoff(p.nb_cutoff) && !no_cutoff(p.gb_force_cutoff)) {
+        ogk::launch_cut_lists(cut_f.p, n_cut_f, jlist_f.p, origin.p, std::max(p.nb_cutoff, p.gb_force_cutoff),
+                              jlist_cut_f.p, seg_end_f.p, stream);
+        pf.jlist = jlist_cut_f.p;
+        pf.seg_end = seg_end_f.p;
+      }
       ogk::launch_force_pass(pf, stream);
     }
     {
@@ -879,12 +896,14 @@ og_status finalize_impl(og_engine* e) {
   {
     const int W = ogk::force_warps_per_cta();
     const int chunk = 16;
-    auto build_list = [&](int first_offset, std::vector<ogk::PairWork>* hw, std::vector<int32_t>* hj) {
+    auto build_list = [&](int first_offset, std::vector<ogk::PairWork>* hw, std::vector<int32_t>* hj,
+                          std::vector<ogk::CutBlock>* hc) {
       for (const auto& s : e->sys) {
         for (int t0 = 0; t0 < s.n_tiles; t0 += W) {
           const int jb = static_cast<int>(hj->size());
           for (int t = t0 + first_offset; t < s.n_tiles; ++t) hj->push_back(s.tile_begin + t);
           const int je = static_cast<int>(hj->size());
+          hc->push_back(ogk::CutBlock{s.tile_begin + t0, std::min(W, s.n_tiles - t0), jb, je});
           for (int j0 = jb; j0 < je; j0 += chunk)
             hw->push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
         }
@@ -895,8 +914,17 @@ og_status finalize_impl(og_engine* e) {
     };
     std::vector<int32_t> hj, hjf;
     std::vector<ogk::PairWork> hw, hwf;
-    build_list(0, &hw, &hj);
-    build_list(1, &hwf, &hjf);
+    std::vector<ogk::CutBlock> hcb, hcf;
+    build_list(0, &hw, &hj, &hcb);
+    build_list(1, &hwf, &hjf, &hcf);
+    e->n_cut_b = static_cast<int>(hcb.size());
+    e->n_cut_f = static_cast<int>(hcf.size());
+    OG_CUDA(e->cut_b.upload(hcb, st));
+    OG_CUDA(e->cut_f.upload(hcf, st));
+    OG_CUDA(e->jlist_cut_b.alloc(hj.size()));
+    OG_CUDA(e->jlist_cut_f.alloc(hjf.size()));
+    OG_CUDA(e->seg_end_b.alloc(e->n_tiles));
+    OG_CUDA(e->seg_end_f.alloc(e->n_tiles));
     e->n_work = static_cast<int>(hw.size());
     OG_CUDA(e->work.upload(hw, st));
     OG_CUDA(e->jlist.upload(hj, st));

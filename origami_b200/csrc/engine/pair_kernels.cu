@@ -197,7 +197,9 @@ __global__ void __launch_bounds__(kWarps * 32, OG_BORN_MIN_BLOCKS) k_born(PairAr
   __shared__ __align__(8) uint64_t s_bar[2];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const PairWork w = a.work[blockIdx.x];
+  PairWork w = a.work[blockIdx.x];
+  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
+  if (w.j_begin >= w.j_end) return;  // chunk culled by the cutoff (block-uniform)
   const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar};
   const float* src[2] = {a.pq, a.gb};
   if (threadIdx.x == 0) {
@@ -337,7 +339,9 @@ __global__ void __launch_bounds__(kWarps * 32, OG_FORCE_MIN_BLOCKS) k_force(Pair
   __shared__ __align__(8) uint64_t s_bar[2];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const PairWork w = a.work[blockIdx.x];
+  PairWork w = a.work[blockIdx.x];
+  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
+  if (w.j_begin >= w.j_end) return;  // chunk culled by the cutoff (block-uniform)
   const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar};
   const float* src[3] = {a.pq, a.lj, a.gb};
   if (threadIdx.x == 0) {
@@ -453,6 +457,46 @@ OG_UNROLL(OG_FORCE_UNROLL)
 }  // namespace
 
 int force_warps_per_cta() { return kWarps; }
+
+namespace {
+
+// One warp per i-block; lanes test 32 j-tiles at a time against each of the
+// block's i-tile spheres and append the survivors in order.
+__global__ void k_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* jlist_all,
+                            const double4* origin, double cutoff, int32_t* jlist_out, int32_t* seg_end) {
+  const int b = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (b >= n_blocks) return;
+  const CutBlock cb = blocks[b];
+  int count = 0;
+  for (int p0 = cb.jb; p0 < cb.je; p0 += 32) {
+    const int p = p0 + lane;
+    bool keep = false;
+    int jt = 0;
+    if (p < cb.je) {
+      jt = jlist_all[p];
+      const double4 oj = origin[jt];
+      for (int k = 0; k < cb.n_i_tiles && !keep; ++k) {
+        const double4 oi = origin[cb.i_tile0 + k];
+        const double dx = oj.x - oi.x, dy = oj.y - oi.y, dz = oj.z - oi.z;
+        const double lim = oi.w + oj.w + cutoff + 1e-3;
+        keep = dx * dx + dy * dy + dz * dz <= lim * lim;
+      }
+    }
+    const unsigned kept = __ballot_sync(0xffffffffu, keep);
+    if (keep) jlist_out[cb.jb + count + __popc(kept & ((1u << lane) - 1u))] = jt;
+    count += __popc(kept);
+  }
+  if (lane == 0) seg_end[cb.i_tile0] = cb.jb + count;
+}
+
+}  // namespace
+
+void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* jlist_all, const double4* origin,
+                      double cutoff, int32_t* jlist_out, int32_t* seg_end, cudaStream_t s) {
+  if (n_blocks > 0)
+    k_cut_lists<<<(n_blocks + 3) / 4, 128, 0, s>>>(blocks, n_blocks, jlist_all, origin, cutoff, jlist_out, seg_end);
+}
 
 void launch_born_pass(const PairArgs& a, cudaStream_t s) {
   if (a.n_work > 0) k_born<<<a.n_work, kWarps * 32, 0, s>>>(a);

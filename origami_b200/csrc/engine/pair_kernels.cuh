@@ -36,6 +36,9 @@ struct PairArgs {
   const PairWork* work;
   int32_t n_work;
   const int32_t* jlist;
+  // cutoff mode: per i-block first tile, the end of its culled j range in
+  // jlist (the work items' j_end is clamped to it); NULL for all pairs
+  const int32_t* seg_end;
   const int32_t* mask_begin;  // per tile: first TileMaskRef, mask_begin[t+1] = end
   const TileMaskRef* mask_refs;
   const uint32_t* mask_ex;
@@ -65,6 +68,21 @@ struct PairArgs {
   const double* born_r64;
   double nb_c2_64, gb_c2_64, inv_rc3_64;
 };
+
+// One i-block of a pair work list: W i-tiles from i_tile0 against the j-tiles
+// jlist[jb, je).
+struct CutBlock {
+  int32_t i_tile0, n_i_tiles, jb, je;
+};
+// Cutoff-mode j lists, rebuilt from the tile origins every force evaluation:
+// for each i-block, the j-tiles of jlist_all[jb, je) whose bounding sphere
+// comes within `cutoff` of any of the block's tile spheres, kept in order and
+// compacted to the front of the same range of jlist_out; seg_end[i_tile0]
+// receives the new end.  No atom pair within the cutoff is dropped (sphere
+// bounds, FP64, 1e-3 A margin); the pair kernels still apply the cutoff per
+// pair.
+void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* jlist_all, const double4* origin,
+                      double cutoff, int32_t* jlist_out, int32_t* seg_end, cudaStream_t s);
 
 void launch_born_pass(const PairArgs& a, cudaStream_t s);
 // Far field (tiles without exclusion masks), FP32.

@@ -252,3 +252,23 @@ def test_nonfinite_positions_reported(origami):
     assert st == 2
     assert eng.stats(1)["diverged"] and not eng.stats(0)["diverged"]
     assert np.isfinite(eng.positions(0)).all()
+
+
+def test_cutoff_lists_on_long_chains(origami):
+    """Cutoff mode culls tile pairs by bounding spheres every evaluation (most
+    pairs of a 60-residue extended chain lie beyond 20 A): forces and Born
+    integrals of two batched systems still match the oracle's cutoff sums."""
+    seq = "ARNDCQEGHILKMFPSTWYV" * 3
+    chains = [origami.Chain.build(seq), helix(origami, seq)]
+    xs = [jitter(c.positions, 0.03, 11 + k) for k, c in enumerate(chains)]
+    eng = origami.Engine(origami.Params())
+    for c, x in zip(chains, xs):
+        eng.add_system(c, x)
+    eng.finalize()
+    for k, (c, x) in enumerate(zip(chains, xs)):
+        f = eng.total_force(k)
+        ref = Orc(c).total_force(x, 10.0, 20.0, 10.0)
+        assert rms_rel(f, ref) < 1e-5, (k, rms_rel(f, ref))
+        got = eng.born_integrals(k)
+        ref_i = Orc(c).born_integrals(x, 20.0)
+        assert np.max(np.abs(got - ref_i)) < 1e-6 * np.max(np.abs(ref_i))
