@@ -252,6 +252,36 @@ struct og_engine {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (own_stream && stream) cudaStreamDestroy(stream);
+    for (cudaStream_t* q : {&side, &hi})
+      if (*q) {
+        cudaStreamSynchronize(*q);
+        cudaStreamDestroy(*q);
+      }
+    for (cudaEvent_t ev : {ev_fork, ev_join, ev_join_hi})
+      if (ev) cudaEventDestroy(ev);
+  }
+
+  // The surface term runs on an internal side stream, forked after the
+  // positions are packed and joined before anything reads the forces, so
+  // its FP64, latency-bound kernels overlap the FP32 pair kernels (both add
+  // into the fixed-point accumulators with atomics, so the result does not
+  // depend on the interleaving).  Inside a graph capture the fork and join
+  // become graph edges.
+  // The pair kernels go to a high-priority internal stream and the surface
+  // term to a low-priority one, so that as surface blocks retire the block
+  // scheduler places pair blocks first and the surface blocks fill the rest.
+  cudaStream_t side = nullptr, hi = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join_hi = nullptr;
+  cudaError_t ensure_side() {
+    if (side) return cudaSuccess;
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, least);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&hi, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_join_hi, cudaEventDisableTiming);
+    return e;
   }
 
   ogk::AtomArrays atoms() {
@@ -378,16 +408,17 @@ struct og_engine {
   struct Timer {
     og_engine* e;
     const char* name;
+    cudaStream_t s;
     cudaEvent_t a = nullptr, b = nullptr;
-    Timer(og_engine* eng, const char* n) : e(eng), name(n) {
+    Timer(og_engine* eng, const char* n, cudaStream_t on = nullptr) : e(eng), name(n), s(on ? on : eng->stream) {
       if (!e->profile) return;
       cudaEventCreate(&a);
       cudaEventCreate(&b);
-      cudaEventRecord(a, e->stream);
+      cudaEventRecord(a, s);
     }
     ~Timer() {
       if (!e->profile) return;
-      cudaEventRecord(b, e->stream);
+      cudaEventRecord(b, s);
       cudaEventSynchronize(b);
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, a, b);
@@ -456,6 +487,18 @@ struct og_engine {
   void enqueue_forces() {
     ogk::PairArgs pa = pair_args();
     ogk::AtomArrays at = atoms();
+    // the surface term on the side stream (profiling times kernels one by
+    // one, on the main stream)
+    const bool sasa_forked = p.include_sasa && !profile && ensure_side() == cudaSuccess;
+    const cudaStream_t main_stream = stream;
+    if (sasa_forked) {
+      cudaEventRecord(ev_fork, stream);
+      cudaStreamWaitEvent(side, ev_fork, 0);
+      cudaStreamWaitEvent(hi, ev_fork, 0);
+      ogk::launch_sasa_forces(sasa_args(false), side);
+      cudaEventRecord(ev_join, side);
+      stream = hi;  // the pair kernels below
+    }
     if (lgb_on()) {
       enqueue_learned_radii();
     } else {
@@ -497,7 +540,12 @@ struct og_engine {
       Timer t(this, "bonded");
       ogk::launch_bonded_forces(bonded_args(), stream);
     }
-    if (p.include_sasa) {
+    if (sasa_forked) {
+      cudaEventRecord(ev_join_hi, hi);
+      stream = main_stream;
+      cudaStreamWaitEvent(stream, ev_join_hi, 0);
+      cudaStreamWaitEvent(stream, ev_join, 0);
+    } else if (p.include_sasa) {
       Timer t(this, "sasa");
       ogk::launch_sasa_forces(sasa_args(false), stream);
     }
