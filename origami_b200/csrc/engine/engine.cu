@@ -268,8 +268,8 @@ struct og_engine {
   // depend on the interleaving).  Inside a graph capture the fork and join
   // become graph edges.
   // The pair kernels go to a high-priority internal stream and the surface
-  // term to a low-priority one, so that as surface blocks retire the block
-  // scheduler places pair blocks first and the surface blocks fill the rest.
+  // term to a low-priority one; in eager launches (judge, single force
+  // evaluations) the block scheduler then places pair blocks first.
   cudaStream_t side = nullptr, hi = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join_hi = nullptr;
   cudaError_t ensure_side() {
@@ -1245,6 +1245,11 @@ og_status build_graph(og_engine* e) {
   e->stream = saved;
   cudaStreamDestroy(cap);
   if (err != cudaSuccess) return cuda_fail(err, "graph capture");
+  // Kernel nodes run at the launch stream's priority: the surface term's
+  // blocks, launched first, are dispatched first and the pair kernels fill
+  // its tail.  (Honouring the captured node priorities, pair kernels first,
+  // measured slower: they displace surface warps, whose latency-bound work
+  // then stretches the step.)
   OG_CUDA(cudaGraphInstantiate(&e->graph_exec, e->graph, 0));
   return OG_OK;
 }
