@@ -179,16 +179,6 @@ __device__ __forceinline__ D3 pos(const SasaArgs& a, int j) { return {a.x[j], a.
 // Unit radial direction of transition s of the circle being processed.
 __device__ __forceinline__ D3 tpoint(const WarpSmem& w, int s) { return {w.tx[s], w.ty[s], w.tz[s]}; }
 
-__device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
-  int s = v;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(kFull, s, o);
-    if (lane >= o) s += t;
-  }
-  *total = __shfl_sync(kFull, s, 31);
-  return s - v;
-}
-
 // Position of the n-th (0-based) set bit of mask, which has more than n.
 __device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
   int pos = 0;
@@ -311,26 +301,36 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
   // ---- drop caps whose circle lies inside another cap: alpha_k < alpha_m
   // and angle(axis_k, axis_m) < alpha_m - alpha_k, i.e. sigma - c_k c_m -
   // margin > s_k s_m, compared squared (both sides positive)
+  // Each lane tests two caps (k and k + 32) against the caps m in one pass,
+  // so a cap m's data is read once for both; survivors keep ascending order.
   int n_live = 0;
-  for (int k0 = 0; k0 < n_caps; k0 += 32) {
-    const int k = k0 + lane;
-    bool live = k < n_caps;
-    if (live) {
-      const double ck = w.cc[k], sk2 = 1.0 - ck * ck;
-      const D3 ak = {w.cx[k], w.cy[k], w.cz[k]};
-      for (int m = 0; m < n_caps; ++m) {
-        const double cm = w.cc[m];
-        if (m == k || !(ck > cm)) continue;
-        const double lhs = ak.x * w.cx[m] + ak.y * w.cy[m] + ak.z * w.cz[m] - cm * ck - 1e-6;
-        if (lhs > 0.0 && lhs * lhs > sk2 * (1.0 - cm * cm)) {
-          live = false;
-          break;
-        }
+  for (int k0 = 0; k0 < n_caps; k0 += 64) {
+    const int ka = k0 + lane, kb = k0 + 32 + lane;
+    bool la = ka < n_caps, lb = kb < n_caps;
+    const double ca = la ? w.cc[ka] : 0.0, cb = lb ? w.cc[kb] : 0.0;
+    const double sa2 = 1.0 - ca * ca, sb2 = 1.0 - cb * cb;
+    const D3 aa = la ? D3{w.cx[ka], w.cy[ka], w.cz[ka]} : D3{};
+    const D3 ab = lb ? D3{w.cx[kb], w.cy[kb], w.cz[kb]} : D3{};
+    for (int m = 0; m < n_caps && (la || lb); ++m) {
+      const double cm = w.cc[m];
+      const D3 am = {w.cx[m], w.cy[m], w.cz[m]};
+      const double sm2 = 1.0 - cm * cm;
+      if (la && m != ka && ca > cm) {
+        const double lhs = dot(aa, am) - cm * ca - 1e-6;
+        if (lhs > 0.0 && lhs * lhs > sa2 * sm2) la = false;
+      }
+      if (lb && m != kb && cb > cm) {
+        const double lhs = dot(ab, am) - cm * cb - 1e-6;
+        if (lhs > 0.0 && lhs * lhs > sb2 * sm2) lb = false;
       }
     }
-    const unsigned lv = __ballot_sync(kFull, live);
-    if (live) w.live[n_live + __popc(lv & ((1u << lane) - 1u))] = static_cast<uint8_t>(k);
-    n_live += __popc(lv);
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned lva = __ballot_sync(kFull, la);
+    if (la) w.live[n_live + __popc(lva & below)] = static_cast<uint8_t>(ka);
+    n_live += __popc(lva);
+    const unsigned lvb = __ballot_sync(kFull, lb);
+    if (lb) w.live[n_live + __popc(lvb & below)] = static_cast<uint8_t>(kb);
+    n_live += __popc(lvb);
   }
   __syncwarp();
 
@@ -453,8 +453,11 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
         const int k = w.live[b0 + j], m = w.live[lm];
         if (k != m) cnt = classify(cap_at(w, k), cap_at(w, m)).count;
       }
-      int tot;
-      const int off = warp_excl_scan(cnt, lane, &tot);
+      // prefix of the counts (0, 1 or 2) from two ballots
+      const unsigned c1 = __ballot_sync(kFull, cnt & 1), c2 = __ballot_sync(kFull, cnt & 2);
+      const unsigned below = (1u << lane) - 1u;
+      const int off = __popc(c1 & below) + 2 * __popc(c2 & below);
+      const int tot = __popc(c1) + 2 * __popc(c2);
       const unsigned packed = static_cast<unsigned>(p) | (static_cast<unsigned>(run + off + (cnt ? w.zpre[j] : 0)) << 16);
       const unsigned crossing = __ballot_sync(kFull, cnt != 0);
       const int n_new = __popc(crossing);
