@@ -1028,8 +1028,10 @@ og_status finalize_impl(og_engine* e) {
     }
     hmb[e->n_tiles] = static_cast<int32_t>(hmr.size());
   }
-  std::vector<int4> hnear;
-  for (const auto& kv : mask_of) hnear.push_back(make_int4(kv.first.first, kv.first.second, kv.second, 0));
+  std::vector<int4> hnear;  // unordered: the (i_tile <= j_tile) orientation's block
+  for (const auto& kv : mask_of)
+    if (kv.first.first <= kv.first.second)
+      hnear.push_back(make_int4(kv.first.first, kv.first.second, kv.second, 0));
   e->n_near = static_cast<int>(hnear.size());
   OG_CUDA(e->near.upload(hnear, st));
   OG_CUDA(e->mask_begin.upload(hmb, st));

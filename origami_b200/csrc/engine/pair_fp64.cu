@@ -8,69 +8,115 @@
 namespace ogk {
 
 // ------------------------------------------------------- FP64 near field
-// One warp per near-field (i-tile, j-tile) pair -- the tiles that carry
-// exclusion / 1-4 masks, i.e. the bonded neighbourhood where the large LJ and
-// Coulomb pair forces cancel against the bonded terms.  FP64 throughout, term
-// for term as forces_nonbonded.rs:196-232 + forces_gb.rs:82-111; the j atoms
-// are warp-uniform broadcast loads.
+// One warp per unordered near-field tile pair (i-tile <= j-tile) -- the
+// tiles that carry exclusion / 1-4 masks, i.e. the bonded neighbourhood
+// where the large LJ and Coulomb pair forces cancel against the bonded terms.
+// FP64 throughout, term for term as forces_nonbonded.rs:196-232 +
+// forces_gb.rs:82-111.  Each pair is evaluated once (Newton's third law):
+// the j-tile's atoms are staged in the warp's shared memory, lane l meets
+// partner (l + k) mod 32 at step k, so within a step every lane touches a
+// different partner and the j-side sums need no atomics.  On a diagonal tile
+// pair steps 1..16 cover every pair once (step 16 on the lower half-warp
+// only).  The pair coefficient is symmetric in i and j, so the j-side force
+// is exactly the negated i-side term.
 namespace {
 
-__global__ void __launch_bounds__(128) k_near64(PairArgs a, const int4* __restrict__ near, int n_near) {
-  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+constexpr int kNearWarps = 4;
+
+struct NearTile {
+  double x[kTile], y[kTile], z[kTile], q[kTile], r[kTile];
+  double rmin[kTile], eps[kTile], rmin14[kTile], eps14[kTile];
+  double fx[kTile], fy[kTile], fz[kTile];
+  int32_t valid[kTile];
+};
+
+__global__ void __launch_bounds__(kNearWarps * 32) k_near64(PairArgs a, const int4* __restrict__ near, int n_near) {
+  __shared__ NearTile tiles[kNearWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wid = blockIdx.x * kNearWarps + warp;
   if (wid >= n_near) return;
-  const int4 w = near[wid];  // i_tile, j_tile, mask offset
+  NearTile& t = tiles[warp];
+  const int4 w = near[wid];  // i_tile, j_tile (>= i_tile), mask block of (i_tile, j_tile)
   const int i = w.x * kTile + lane;
+  const int jl = w.y * kTile + lane;  // this lane's j atom, staged for the warp
+  t.x[lane] = a.x64[jl];
+  t.y[lane] = a.y64[jl];
+  t.z[lane] = a.z64[jl];
+  t.q[lane] = a.q64[jl];
+  t.r[lane] = a.born_r64[jl];
+  t.rmin[lane] = a.rmin64[jl];
+  t.eps[lane] = a.eps64[jl];
+  t.rmin14[lane] = a.rmin14_64[jl];
+  t.eps14[lane] = a.eps14_64[jl];
+  t.valid[lane] = a.atom_valid[jl];
+  t.fx[lane] = t.fy[lane] = t.fz[lane] = 0.0;
   const uint32_t ex = a.mask_ex[w.z * kTile + lane];
   const uint32_t m14 = a.mask_14[w.z * kTile + lane];
+  const bool valid_i = a.atom_valid[i] != 0;
   const double xi = a.x64[i], yi = a.y64[i], zi = a.z64[i], qi = a.q64[i], Ri = a.born_r64[i];
   const double rmi = a.rmin64[i], epi = a.eps64[i], rm14i = a.rmin14_64[i], ep14i = a.eps14_64[i];
   const double coul_kj = kCoulomb * kKcalToKj;
   const double gb_pref = (1.0 - 1.0 / kEpsWater) * kCoulomb * kKcalToKj;
+  const bool diag = w.x == w.y;
   double ax = 0.0, ay = 0.0, az = 0.0;
-  const int j0 = w.y * kTile;
-  for (int k = 0; k < kTile; ++k) {
-    const int j = j0 + k;
-    if (!a.atom_valid[j]) continue;
-    const double dx = a.x64[j] - xi, dy = a.y64[j] - yi, dz = a.z64[j] - zi;
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    if (r2 < 1e-18) continue;
-    const double qq = qi * a.q64[j];
-    double coeff = 0.0;
-    if (!((ex >> k) & 1u) && r2 <= a.nb_c2_64) {
-      const bool is14 = (m14 >> k) & 1u;
-      const double rmin = is14 ? rm14i + a.rmin14_64[j] : rmi + a.rmin64[j];
-      const double eps = sqrt(is14 ? ep14i * a.eps14_64[j] : epi * a.eps64[j]);
-      const double inv_r2 = 1.0 / r2;
-      const double ratio2 = rmin * rmin * inv_r2;
-      const double r6 = ratio2 * ratio2 * ratio2;
-      coeff += 12.0 * eps * inv_r2 * (r6 - r6 * r6) * kKcalToKj;
-      if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 / sqrt(r2) - a.inv_rc3_64);
-    }
-    if (qq != 0.0 && r2 <= a.gb_c2_64) {
-      const double r = sqrt(r2);
-      const double rp = Ri * a.born_r64[j];
-      const double e = exp(-r2 / (4.0 * rp));
-      const double f2 = r2 + rp * e;
-      const double f = sqrt(f2);
-      coeff += gb_pref * qq / f2 * ((2.0 * r - 0.5 * r * e) / (2.0 * f)) / r;
+  __syncwarp();
+  for (int k = diag ? 1 : 0; k < (diag ? 17 : kTile); ++k) {
+    const int p = (lane + k) & (kTile - 1);
+    double coeff = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+    if (valid_i && t.valid[p] && !(diag && k == 16 && lane >= 16)) {
+      dx = t.x[p] - xi;
+      dy = t.y[p] - yi;
+      dz = t.z[p] - zi;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double qq = qi * t.q[p];
+      if (r2 >= 1e-18) {
+        if (!((ex >> p) & 1u) && r2 <= a.nb_c2_64) {
+          const bool is14 = (m14 >> p) & 1u;
+          const double rmin = is14 ? rm14i + t.rmin14[p] : rmi + t.rmin[p];
+          const double eps = sqrt(is14 ? ep14i * t.eps14[p] : epi * t.eps[p]);
+          const double inv_r2 = 1.0 / r2;
+          const double ratio2 = rmin * rmin * inv_r2;
+          const double r6 = ratio2 * ratio2 * ratio2;
+          coeff += 12.0 * eps * inv_r2 * (r6 - r6 * r6) * kKcalToKj;
+          if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 / sqrt(r2) - a.inv_rc3_64);
+        }
+        if (qq != 0.0 && r2 <= a.gb_c2_64) {
+          const double r = sqrt(r2);
+          const double rp = Ri * t.r[p];
+          const double e = exp(-r2 / (4.0 * rp));
+          const double f2 = r2 + rp * e;
+          const double f = sqrt(f2);
+          coeff += gb_pref * qq / f2 * ((2.0 * r - 0.5 * r * e) / (2.0 * f)) / r;
+        }
+      }
     }
     ax += dx * coeff;
     ay += dy * coeff;
     az += dz * coeff;
+    t.fx[p] -= dx * coeff;
+    t.fy[p] -= dy * coeff;
+    t.fz[p] -= dz * coeff;
+    __syncwarp();
   }
-  if (a.atom_valid[i]) {
+  if (valid_i) {
     if (!(isfinite(ax) && isfinite(ay) && isfinite(az))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
     add_fixed(a.fx + i, ax, kForceScale);
     add_fixed(a.fy + i, ay, kForceScale);
     add_fixed(a.fz + i, az, kForceScale);
+  }
+  if (t.valid[lane]) {
+    const double bx = t.fx[lane], by = t.fy[lane], bz = t.fz[lane];
+    if (!(isfinite(bx) && isfinite(by) && isfinite(bz))) atomicOr(a.sys_nonfinite + a.atom_sys[jl], 1);
+    add_fixed(a.fx + jl, bx, kForceScale);
+    add_fixed(a.fy + jl, by, kForceScale);
+    add_fixed(a.fz + jl, bz, kForceScale);
   }
 }
 
 }  // namespace
 
 void launch_near_force64(const PairArgs& a, const int4* near, int n_near, cudaStream_t s) {
-  if (n_near > 0) k_near64<<<(n_near * 32 + 127) / 128, 128, 0, s>>>(a, near, n_near);
+  if (n_near > 0) k_near64<<<(n_near + kNearWarps - 1) / kNearWarps, kNearWarps * 32, 0, s>>>(a, near, n_near);
 }
 
 // ----------------------------------------------------------------- FP64 path

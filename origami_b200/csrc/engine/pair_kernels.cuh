@@ -87,8 +87,9 @@ void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* j
 void launch_born_pass(const PairArgs& a, cudaStream_t s);
 // Far field (tiles without exclusion masks), FP32.
 void launch_force_pass(const PairArgs& a, cudaStream_t s);
-// Near field: near[k] = (i_tile, j_tile, mask block, 0) for every ordered tile
-// pair that carries masks, FP64.
+// Near field: near[k] = (i_tile, j_tile, mask block of (i_tile, j_tile), 0)
+// for every unordered tile pair (i_tile <= j_tile) that carries masks, FP64;
+// each pair once, both atoms' forces.
 void launch_near_force64(const PairArgs& a, const int4* near, int n_near, cudaStream_t s);
 
 // FP64 energy evaluation, one thread per i atom over every j of its system.
