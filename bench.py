@@ -12,8 +12,9 @@ Metric: aggregate ns/day over all replicas (and GPUs).
 
 Timing: CUDA events on the engine's stream (torch's current stream), one
 event pair per step with a 256 MiB L2 flush before each; under torchrun the
-max over ranks.  `e2e` is the same metric through the C ABI with host
-positions/velocities copied in and positions copied out every step.
+max over ranks.  `e2e` is the same metric through the C ABI with the whole
+dynamic state copied in from page-locked host buffers and back out every
+step (og_set_state / og_step / og_get_state).
 """
 from __future__ import annotations
 
@@ -411,7 +412,7 @@ def run_b200(args):
         "dominant_kernel": {
             "kernel": "k_sasa_boundary + k_sasa_terms (PowerSasa, FP64)",
             "ms_per_step": (prof["sasa"][0] / prof["sasa"][1]) if "sasa" in prof else None,
-            "bound": "FP64 dependency latency at 16 warps per SM (ncu: issue active 43.5 %, FP64 pipe 15 %, "
+            "bound": "FP64 dependency latency at 16 warps per SM (ncu: issue active 45 %, FP64 pipe 16 %, "
                      "DRAM 0.02 %); data-dependent geometry, no flop or byte roofline",
             "profile": "profiles/sasa_boundary_4x4694_extended.md"},
         "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / plain_ms) if "sasa" in prof else None,
