@@ -56,7 +56,7 @@ struct LgbDescArgs {
   const double* rho_tilde;     // rho - offset
   const double* srho;          // HCT scale * rho~
   const int2* sys_tiles;       // per system: (first tile, tile count)
-  const double4* origin;       // per tile: first atom, w = bounding radius
+  const double4* origin;       // per tile: centroid, w = bounding radius
   int32_t n_padded;
   float* xin;                  // n_padded x 80 network inputs (padding rows 0)
   double* r_cfa;               // n_padded (padding: 1)

@@ -48,7 +48,7 @@ struct SasaArgs {
   int32_t n_tasks;
   const int32_t* atom_sys;    // -1 for padding
   const int2* sys_tiles;      // per system: (first tile, tile count)
-  const double4* origin;      // per tile: first atom, w = bounding radius
+  const double4* origin;      // per tile: centroid, w = bounding radius
   double r_max;               // largest SASA radius of any atom
   unsigned long long* fx;     // fixed-point forces (kForceScale)
   unsigned long long* fy;

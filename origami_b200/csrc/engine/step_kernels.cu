@@ -23,14 +23,21 @@ __device__ __forceinline__ bool atom_live(const AtomArrays& a, int i, int* sys) 
 // ------------------------------------------------------------------- pack
 __device__ __forceinline__ void pack_atom(const AtomArrays& a, int i) {
   const int tile = i >> 5;
-  const int first = tile << 5;
-  const bool first_real = a.atom_sys[first] >= 0;
-  const double ox = first_real ? a.x[first] : 0.0;
-  const double oy = first_real ? a.y[first] : 0.0;
-  const double oz = first_real ? a.z[first] : 0.0;
-  // origin.w = radius of the tile's bounding sphere about its first atom
-  // (the SASA neighbour search culls tiles with it).  The whole warp is one
+  // The tile's origin is the centroid of its real atoms and origin.w the
+  // radius of its bounding sphere about it: the reference frame of the FP32
+  // coordinates and the sphere every tile-level cull tests (cutoff lists,
+  // descriptor partners, the SASA neighbour search).  The whole warp is one
   // tile: n_padded is a multiple of 32 and launches use whole warps.
+  const bool real = a.atom_sys[i] >= 0;
+  double sx = real ? a.x[i] : 0.0, sy = real ? a.y[i] : 0.0, sz = real ? a.z[i] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    sz += __shfl_xor_sync(0xffffffffu, sz, o);
+  }
+  const int n_real = __popc(__ballot_sync(0xffffffffu, real));
+  const double inv_n = n_real > 0 ? 1.0 / n_real : 0.0;
+  const double ox = sx * inv_n, oy = sy * inv_n, oz = sz * inv_n;
   double rad = 0.0;
   if (a.atom_sys[i] >= 0) {
     const double dx = a.x[i] - ox, dy = a.y[i] - oy, dz = a.z[i] - oz;
