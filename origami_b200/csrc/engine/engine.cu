@@ -219,7 +219,7 @@ struct og_engine {
   DVec<int2> sys_tiles;
   DVec<ogk::SasaArcTerm> sasa_arc_terms;
   DVec<ogk::SasaVertexTerm> sasa_vertex_terms;
-  DVec<int32_t> sasa_counts;
+  DVec<int32_t> sasa_counts, sasa_overflow;
   int sasa_term_cap = 0;
   int n_sasa_tasks = 0, n_sasa_all = 0, n_sr_dots = 0;
   // learned Born radii: descriptor class per atom, network input, Coulomb-
@@ -374,6 +374,8 @@ struct og_engine {
     a.vertex_terms = sasa_vertex_terms.p;
     a.counts = sasa_counts.p;
     a.term_cap = sasa_term_cap;
+    a.overflow = sasa_overflow.p;
+    a.overflow_cap = static_cast<int32_t>(sasa_overflow.n);
     return a;
   }
 
@@ -616,8 +618,9 @@ og_status read_status(og_engine* e, std::vector<ogk::SysState>* out) {
   if (err_flag & ogk::kStatusTimeout) return og_fail(OG_E_TIMEOUT, "a pair-kernel pipeline wait timed out");
   for (const auto& s : *out)
     if (s.status & ogk::kStatusSasaOverflow)
-      return og_fail(OG_E_UNSUPPORTED, "an atom's SASA arrangement exceeds the kernel's capacity (caps, "
-                                       "transitions per cap or arcs); its surface term was not evaluated");
+      return og_fail(OG_E_UNSUPPORTED, "an atom's SASA arrangement exceeds the kernels' largest capacity (254 "
+                                       "caps, 254 transitions per circle, 128 arcs, or the term buffers); its "
+                                       "surface term was not evaluated");
   return OG_OK;
 }
 
@@ -860,8 +863,11 @@ og_status finalize_impl(og_engine* e) {
       e->sasa_term_cap = 16 * e->n_sasa_tasks + 1024;
       OG_CUDA(e->sasa_arc_terms.alloc(e->sasa_term_cap));
       OG_CUDA(e->sasa_vertex_terms.alloc(e->sasa_term_cap));
-      OG_CUDA(e->sasa_counts.alloc(2));
     }
+    // counters and the queue of atoms beyond the default arrangement
+    // capacities: used by the force path and by area queries alike
+    OG_CUDA(e->sasa_counts.alloc(3));
+    OG_CUDA(e->sasa_overflow.alloc(std::max(1, std::max(e->n_sasa_all, e->n_sasa_tasks))));
     // Component probes: Fibonacci points, golden angle pi (3 - sqrt 5),
     // joined when their dot product exceeds cos(2.5 sqrt(4 pi / N))
     // (arrangement.rs:327-391).

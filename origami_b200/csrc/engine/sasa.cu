@@ -138,19 +138,26 @@ __device__ int identify_root_sign(Cap c1, Cap c2, D3 ref) {
 }
 
 // ------------------------------------------------------ per-warp storage
-struct WarpSmem {
+// Capacities: caps (neighbour spheres cutting atom i's sphere), transitions
+// of one batch of circles, exposed arcs (and vertices).  Indices into caps
+// and transitions are bytes, so both stay below 255 (0xFF marks a circle's
+// pseudo entry).
+template <int kCaps_, int kTrans_, int kArcs_>
+struct WarpSmemT {
+  static constexpr int kCaps = kCaps_, kTrans = kTrans_, kArcs = kArcs_;
+  static_assert(kCaps <= 254 && kTrans <= 254, "byte-sized cap and transition indices");
   // caps (indices in neighbour order, i.e. ascending atom index)
-  double cx[kSasaMaxCaps], cy[kSasaMaxCaps], cz[kSasaMaxCaps], cc[kSasaMaxCaps];
-  int32_t owner[kSasaMaxCaps];
-  uint8_t live[kSasaMaxCaps];
+  double cx[kCaps], cy[kCaps], cz[kCaps], cc[kCaps];
+  int32_t owner[kCaps];
+  uint8_t live[kCaps];
   // transitions of each live circle (low 16 bits) and kContained
-  int32_t tcnt[kSasaMaxCaps];
+  int32_t tcnt[kCaps];
   // transitions of the batch of circles being processed: sort key, unit
   // radial direction, the other cap, the batch circle, the sorted order
-  double ta[kSasaMaxTrans], tx[kSasaMaxTrans], ty[kSasaMaxTrans], tz[kSasaMaxTrans];
-  uint8_t tother[kSasaMaxTrans];
-  uint8_t tseg[kSasaMaxTrans];
-  uint8_t torder[kSasaMaxTrans];
+  double ta[kTrans], tx[kTrans], ty[kTrans], tz[kTrans];
+  uint8_t tother[kTrans];
+  uint8_t tseg[kTrans];
+  uint8_t torder[kTrans];
   // per batch circle: first entry, entries kept after de-duplication,
   // transition-free circles before it, sin(alpha) and 1 / sin(alpha)
   uint16_t sbeg[kSasaBatch + 1];
@@ -160,24 +167,32 @@ struct WarpSmem {
   // order, its sorted position, and per batch circle the mode (0: burial
   // depth by toggles, 1: explicit midpoint tests) and the depth before its
   // first transition
-  int8_t ttog[kSasaMaxTrans], tdep[kSasaMaxTrans];
-  uint8_t trank[kSasaMaxTrans];
+  int8_t ttog[kTrans], tdep[kTrans];
+  uint8_t trank[kTrans];
   int32_t bmode[kSasaBatch];
   int32_t bbase[kSasaBatch];
   // exposed arcs
-  double a_theta[kSasaMaxArcs], a_sx[kSasaMaxArcs], a_sy[kSasaMaxArcs], a_sz[kSasaMaxArcs];
-  uint8_t a_cap[kSasaMaxArcs], a_full[kSasaMaxArcs], a_vis[kSasaMaxArcs];
-  int16_t a_own[kSasaMaxArcs], a_vs[kSasaMaxArcs], a_ve[kSasaMaxArcs];
+  double a_theta[kArcs], a_sx[kArcs], a_sy[kArcs], a_sz[kArcs];
+  uint8_t a_cap[kArcs], a_full[kArcs], a_vis[kArcs];
+  int16_t a_own[kArcs], a_vs[kArcs], a_ve[kArcs];
   // vertices (one per arc that is not a full circle)
-  double v_x[kSasaMaxArcs], v_y[kSasaMaxArcs], v_z[kSasaMaxArcs];
-  uint8_t v_in[kSasaMaxArcs], v_out[kSasaMaxArcs];
-  int8_t v_sign[kSasaMaxArcs];
+  double v_x[kArcs], v_y[kArcs], v_z[kArcs];
+  uint8_t v_in[kArcs], v_out[kArcs];
+  int8_t v_sign[kArcs];
 };
 
-__device__ __forceinline__ Cap cap_at(const WarpSmem& w, int k) { return {{w.cx[k], w.cy[k], w.cz[k]}, w.cc[k]}; }
+// The boundary kernels' storage: four warps per block at the default
+// capacities; atoms that exceed them are queued for one warp per block at
+// the large ones.
+using WarpSmem = WarpSmemT<kSasaMaxCaps, kSasaMaxTrans, kSasaMaxArcs>;
+using WarpSmemBig = WarpSmemT<kSasaBigCaps, kSasaBigTrans, kSasaBigArcs>;
+
+template <class W>
+__device__ __forceinline__ Cap cap_at(const W& w, int k) { return {{w.cx[k], w.cy[k], w.cz[k]}, w.cc[k]}; }
 __device__ __forceinline__ D3 pos(const SasaArgs& a, int j) { return {a.x[j], a.y[j], a.z[j]}; }
 // Unit radial direction of transition s of the circle being processed.
-__device__ __forceinline__ D3 tpoint(const WarpSmem& w, int s) { return {w.tx[s], w.ty[s], w.tz[s]}; }
+template <class W>
+__device__ __forceinline__ D3 tpoint(const W& w, int s) { return {w.tx[s], w.ty[s], w.tz[s]}; }
 
 // Position of the n-th (0-based) set bit of mask, which has more than n.
 __device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
@@ -235,7 +250,8 @@ __device__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D
 
 // Builds caps and the exposed boundary of atom i in w.  Returns the outcome;
 // for kBounded, *n_arcs / *n_verts are the boundary sizes (possibly zero).
-__device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, int* n_arcs_out, int* n_verts_out,
+template <class W>
+__device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_arcs_out, int* n_verts_out,
                               int* n_live_out) {
   const int sys = a.atom_sys[i];
   const D3 pi = pos(a, i);
@@ -282,7 +298,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
       const unsigned caps = __ballot_sync(kFull, is_cap);
       if (is_cap) {
         const int slot = n_caps + __popc(caps & ((1u << lane) - 1u));
-        if (slot < kSasaMaxCaps) {
+        if (slot < W::kCaps) {
           w.cx[slot] = ax;
           w.cy[slot] = ay;
           w.cz[slot] = az;
@@ -294,7 +310,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     }
   }
   if (__any_sync(kFull, enclosed)) return kBuried;
-  if (n_caps > kSasaMaxCaps) return kInvalid;
+  if (n_caps > W::kCaps) return kInvalid;
   if (n_caps == 0) return kExposed;
   __syncwarp();
 
@@ -375,7 +391,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
     int b1 = b0, total = 0;
     while (b1 < n_live && b1 - b0 < kSasaBatch) {
       const int sz = max(w.tcnt[b1] & kCountMask, 1);
-      if (total + sz > kSasaMaxTrans) break;
+      if (total + sz > W::kTrans) break;
       total += sz;
       ++b1;
     }
@@ -625,7 +641,7 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
       }
       const unsigned ex = __ballot_sync(kFull, exposed);
       const unsigned exv = __ballot_sync(kFull, exposed && !full);
-      if (n_arcs + __popc(ex) > kSasaMaxArcs) {
+      if (n_arcs + __popc(ex) > W::kArcs) {
         bad = true;
         break;
       }
@@ -675,7 +691,8 @@ __device__ int build_boundary(const SasaArgs& a, WarpSmem& w, int i, int lane, i
 }
 
 // Vertex signs and arc->vertex links (build_atom_cache).
-__device__ void link_boundary(WarpSmem& w, int n_arcs, int n_verts, int lane) {
+template <class W>
+__device__ void link_boundary(W& w, int n_arcs, int n_verts, int lane) {
   for (int v = lane; v < n_verts; v += 32)
     w.v_sign[v] = static_cast<int8_t>(
         identify_root_sign(cap_at(w, w.v_in[v]), cap_at(w, w.v_out[v]), {w.v_x[v], w.v_y[v], w.v_z[v]}));
@@ -703,21 +720,35 @@ __device__ __forceinline__ void scatter(const SasaArgs& a, int x, D3 g, double s
   if (g.z != 0.0) add_fixed(a.fz + x, g.z * scale, kForceScale);
 }
 
+// An atom whose arrangement exceeds the default capacities goes to the
+// overflow queue (counts[2], overflow[]) for the large-capacity kernel; past
+// the large capacities it is reported (kStatusSasaOverflow).
+// Returns whether the atom was queued (warp-uniform).
+__device__ __forceinline__ bool overflow_atom(const SasaArgs& a, int i, int sys, int lane, bool big) {
+  int queued = 0;
+  if (lane == 0) {
+    if (!big) {
+      const int q = atomicAdd(&a.counts[2], 1);
+      if (q < a.overflow_cap) {
+        a.overflow[q] = i;
+        queued = 1;
+      }
+    }
+    if (!queued) atomicOr(&a.sys[sys].status, kStatusSasaOverflow);
+  }
+  return __shfl_sync(kFull, queued, 0) != 0;
+}
+
 // Force path, stage 1: the boundary of atom i as term records
 // (build_atom_cache + arc_other_cap_and_sign, analytical.rs:101-214, 655-670).
-__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  const int task = blockIdx.x * kWarps + warp;
-  if (task >= a.n_tasks) return;
-  const int i = a.tasks[task];
+template <class W>
+__device__ void boundary_task(const SasaArgs& a, W& w, int i, int lane, bool big) {
   const int sys = a.atom_sys[i];
   if (a.sys[sys].status & kStatusDiverged) return;
   int n_arcs = 0, n_verts = 0, n_live = 0;
   const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live);
   if (outcome == kInvalid) {
-    if (lane == 0) atomicOr(&a.sys[sys].status, kStatusSasaOverflow);
+    overflow_atom(a, i, sys, lane, big);
     return;
   }
   if (outcome != kBounded || n_arcs == 0) return;
@@ -757,6 +788,24 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
     a.vertex_terms[vert_base + v] = SasaVertexTerm{i, w.owner[w.v_in[v]], w.owner[w.v_out[v]], w.v_sign[v]};
 }
 
+__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+  const int task = blockIdx.x * kWarps + warp;
+  if (task >= a.n_tasks) return;
+  boundary_task(a, w, a.tasks[task], lane, false);
+}
+
+// The queued atoms, one warp per block at the large capacities (persistent:
+// the queue length is known only on the device).
+__global__ void __launch_bounds__(32) k_sasa_boundary_big(SasaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmemBig& w = *reinterpret_cast<WarpSmemBig*>(smem_raw);
+  const int n = min(a.counts[2], a.overflow_cap);
+  for (int q = blockIdx.x; q < n; q += gridDim.x) boundary_task(a, w, a.overflow[q], threadIdx.x, true);
+}
+
 // Force path, stage 2: one term per thread, F_x += gamma_i R_i^2 dTerm/dr_x.
 __global__ void __launch_bounds__(128) k_sasa_terms(SasaArgs a) {
   const int n_arc = min(a.counts[0], a.term_cap), n_vert = min(a.counts[1], a.term_cap);
@@ -794,7 +843,8 @@ __global__ void __launch_bounds__(128) k_sasa_terms(SasaArgs a) {
 
 // Face walk with tangent disambiguation (area.rs:140-222): loop count and
 // the exterior-angle sum of the continuation actually taken.
-__device__ void walk_faces(WarpSmem& w, int n_arcs, int lane, int* loops_out, double* vsum_out) {
+template <class W>
+__device__ void walk_faces(W& w, int n_arcs, int lane, int* loops_out, double* vsum_out) {
   for (int e = lane; e < n_arcs; e += 32) w.a_vis[e] = 0;
   __syncwarp();
   int loops = 0;
@@ -862,7 +912,9 @@ __device__ void walk_faces(WarpSmem& w, int n_arcs, int lane, int* loops_out, do
 // then connected components of the fixed probe graph restricted to them by
 // minimum-label propagation (the component count does not depend on how
 // the components are found).
-__device__ int count_components(const SasaArgs& a, WarpSmem& w, int n_live, int lane) {
+template <class W>
+__device__ int count_components(const SasaArgs& a, W& w, int n_live, int lane) {
+  static_assert(sizeof(w.ta) >= kSasaProbes * sizeof(int16_t) && sizeof(w.tx) >= kSasaProbes, "probe scratch");
   volatile int16_t* lab = reinterpret_cast<int16_t*>(w.ta);
   uint8_t* acc = reinterpret_cast<uint8_t*>(w.tx);
   bool any = false;
@@ -899,13 +951,8 @@ __device__ int count_components(const SasaArgs& a, WarpSmem& w, int n_live, int 
   return roots;
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_sasa_areas(SasaArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  const int task = blockIdx.x * kWarps + warp;
-  if (task >= a.n_tasks) return;
-  const int i = a.tasks[task];
+template <class W>
+__device__ void areas_task(const SasaArgs& a, W& w, int i, int lane, bool big) {
   const int sys = a.atom_sys[i];
   const double ri = a.radius[i];
   const double four_pi_r2 = 4.0 * kPi * ri * ri;
@@ -913,7 +960,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_sasa_areas(SasaArgs a) {
   const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live);
   double area = 0.0;
   if (outcome == kInvalid) {
-    if (lane == 0) atomicOr(&a.sys[sys].status, kStatusSasaOverflow);
+    if (overflow_atom(a, i, sys, lane, big)) return;  // the large-capacity kernel writes its area
     area = NAN;
   } else if (outcome == kExposed) {
     area = four_pi_r2;
@@ -937,10 +984,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_sasa_areas(SasaArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(kWarps * 32) k_sasa_areas(SasaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+  const int task = blockIdx.x * kWarps + warp;
+  if (task >= a.n_tasks) return;
+  areas_task(a, w, a.tasks[task], lane, false);
+}
+
+__global__ void __launch_bounds__(32) k_sasa_areas_big(SasaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSmemBig& w = *reinterpret_cast<WarpSmemBig*>(smem_raw);
+  const int n = min(a.counts[2], a.overflow_cap);
+  for (int q = blockIdx.x; q < n; q += gridDim.x) areas_task(a, w, a.overflow[q], threadIdx.x, true);
+}
+
 // Shrake-Rupley: one warp per atom, neighbours staged in shared memory,
 // lanes over test points.
+constexpr int kSrMaxNeighbours = 254;
 struct SrSmem {
-  double nx[kSasaMaxCaps], ny[kSasaMaxCaps], nz[kSasaMaxCaps], nr2[kSasaMaxCaps];
+  double nx[kSrMaxNeighbours], ny[kSrMaxNeighbours], nz[kSrMaxNeighbours], nr2[kSrMaxNeighbours];
 };
 
 __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const double* dots, int n_dots) {
@@ -974,7 +1038,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const
       const unsigned m = __ballot_sync(kFull, nb);
       if (nb) {
         const int slot = n_nb + __popc(m & ((1u << lane) - 1u));
-        if (slot < kSasaMaxCaps) {
+        if (slot < kSrMaxNeighbours) {
           w.nx[slot] = a.x[j];
           w.ny[slot] = a.y[j];
           w.nz[slot] = a.z[j];
@@ -984,7 +1048,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const
       n_nb += __popc(m);
     }
   }
-  if (n_nb > kSasaMaxCaps) {
+  if (n_nb > kSrMaxNeighbours) {
     if (lane == 0) {
       atomicOr(&a.sys[sys].status, kStatusSasaOverflow);
       a.area[i] = NAN;
@@ -1012,6 +1076,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const
 }
 
 constexpr size_t kWarpSmemBytes = sizeof(WarpSmem) * kWarps;
+constexpr size_t kBigSmemBytes = sizeof(WarpSmemBig);
+constexpr int kBigGrid = 148 * 4;  // persistent one-warp blocks for the queue
 // four resident CTAs per SM (228 KB, 1 KB reserved per CTA)
 static_assert(4 * (kWarpSmemBytes + 1024) <= 228 * 1024, "boundary kernel no longer fits four CTAs per SM");
 
@@ -1020,21 +1086,31 @@ static_assert(4 * (kWarpSmemBytes + 1024) <= 228 * 1024, "boundary kernel no lon
 cudaError_t sasa_prepare() {
   cudaError_t e = cudaFuncSetAttribute(k_sasa_boundary, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(kWarpSmemBytes));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_sasa_areas, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              static_cast<int>(kWarpSmemBytes));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sasa_areas, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kWarpSmemBytes));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sasa_boundary_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kBigSmemBytes));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_sasa_areas_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kBigSmemBytes));
+  return e;
 }
 
 void launch_sasa_forces(const SasaArgs& a, cudaStream_t s) {
   if (a.n_tasks <= 0) return;
-  cudaMemsetAsync(a.counts, 0, 2 * sizeof(int32_t), s);
+  cudaMemsetAsync(a.counts, 0, 3 * sizeof(int32_t), s);
   k_sasa_boundary<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  k_sasa_boundary_big<<<kBigGrid, 32, kBigSmemBytes, s>>>(a);
   k_sasa_terms<<<148 * 8, 128, 0, s>>>(a);
 }
 
 void launch_sasa_areas(const SasaArgs& a, cudaStream_t s) {
   if (a.n_tasks <= 0) return;
+  cudaMemsetAsync(a.counts + 2, 0, sizeof(int32_t), s);
   k_sasa_areas<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  k_sasa_areas_big<<<kBigGrid, 32, kBigSmemBytes, s>>>(a);
 }
 
 void launch_shrake_rupley(const SasaArgs& a, const double* dots, int n_dots, cudaStream_t s) {

@@ -16,9 +16,15 @@ namespace ogk {
 // OG_E_UNSUPPORTED) instead of producing a wrong force.  Protein atoms reach
 // about 90 caps, 46 of them left after contained caps are dropped, 72
 // transitions on one circle and 19 exposed arcs.
+// Arrangement capacities per atom: the default kernels' (four warps per
+// block) and the large ones for the atoms that exceed them (caps cutting the
+// atom's sphere, transitions of one batch of circles, exposed arcs).
 constexpr int kSasaMaxCaps = 128;
 constexpr int kSasaMaxTrans = 128;
 constexpr int kSasaMaxArcs = 48;
+constexpr int kSasaBigCaps = 254;
+constexpr int kSasaBigTrans = 254;
+constexpr int kSasaBigArcs = 128;
 constexpr int kStatusSasaOverflow = 8;
 
 // Probes of the accessible-component count (arrangement.rs:327-391).
@@ -60,11 +66,15 @@ struct SasaArgs {
   const int16_t* probe_adj;
   SysState* sys;
   // force path: term records of every atom's boundary, appended through
-  // counts[0] (arcs) and counts[1] (vertices), capacity `term_cap` each
+  // counts[0] (arcs) and counts[1] (vertices), capacity `term_cap` each;
+  // counts[2] counts the atoms queued in overflow[] (capacity overflow_cap)
+  // for the large-capacity kernels
   SasaArcTerm* arc_terms;
   SasaVertexTerm* vertex_terms;
   int32_t* counts;
   int32_t term_cap;
+  int32_t* overflow;
+  int32_t overflow_cap;
 };
 
 // F_x += gamma_i R_i^2 (sum_arcs [theta dcos + cos_alpha dtheta] + sum_vertices

@@ -141,6 +141,55 @@ def test_sasa_forces_random_clusters_match_oracle(origami):
         assert np.abs(df - f_ref).max() < 1e-6, k
 
 
+def dense_shell_cluster(seed, n_shell):
+    """A carbon at the origin under a dense half-shell of n_shell atoms
+    between 2.4 and 5.4 A on the z > 1 side (at least 0.9 A apart): the
+    centre's sphere is cut by every shell atom -- more caps than the default
+    kernels hold -- and its other side stays exposed."""
+    rng = np.random.default_rng(seed)
+    pts = [np.zeros(3)]
+    while len(pts) < n_shell + 1:
+        d = rng.normal(size=3)
+        d[2] = abs(d[2])
+        p = d / np.linalg.norm(d) * rng.uniform(2.4, 5.4)
+        if p[2] < 1.0:
+            continue
+        if all(np.linalg.norm(p - q) > 0.9 for q in pts[1:]):
+            pts.append(p)
+    el = rng.choice([0, 0, 1, 1, 2, 3, 5], n_shell + 1)
+    el[0] = 1
+    return np.array(pts), el
+
+
+def test_dense_atoms_beyond_default_capacity_match_oracle(origami):
+    """Atoms whose arrangement exceeds the default per-atom capacities (here
+    the centre, with 140 caps) are queued for the large-capacity kernels:
+    forces, areas and the surface energy still match the oracle, and the
+    shell atoms below the limit take the default path in the same launch."""
+    x, el = dense_shell_cluster(5, 140)
+    o = oracle()
+    r = np.array([o.orc_sasa_radius(int(e)) for e in el])
+    g = np.array([o.orc_sasa_gamma(int(e), 1.0) for e in el])
+    d = np.linalg.norm(x - x[0], axis=1)
+    assert ((d > 0) & (d < r[0] + r)).sum() > 128
+    t = cluster_topology(origami, el)
+    on, off = origami.Params(), origami.Params()
+    on.include_sasa = True
+    e_on, e_off = origami.Engine(on), origami.Engine(off)
+    e_on.add_system(t, x)
+    e_off.add_system(t, x)
+    e_on.finalize()
+    e_off.finalize()
+    df = e_on.total_force(0) - e_off.total_force(0)
+    f_ref = oracle_sasa_forces(x, r, g)
+    assert np.abs(df - f_ref).max() < 1e-6, np.abs(df - f_ref).max()
+    ref = oracle_areas(x, r)
+    got = e_off.sasa_areas(0, "powersasa")
+    assert np.all(np.abs(got - ref) <= 1e-9 * 4 * math.pi * r**2), np.abs(got - ref).max()
+    sr = e_off.sasa_areas(0, "shrake_rupley", 960)
+    np.testing.assert_allclose(sr, oracle_sr(x, r, 960), rtol=0, atol=1e-9)
+
+
 @pytest.mark.parametrize("scale", [1.0, 0.25])
 def test_sasa_forces_match_oracle(origami, scale):
     for name, ch, x in generic_chains(origami):
