@@ -165,7 +165,9 @@ typedef struct og_params {
    * 0.005 kcal/mol/A^2 on C and S times sasa_gamma_scale (the reference's
    * ORIGAMI_SASA_GAMMA_SCALE, analytical.rs:607), applied to the energy as
    * well as the force so the two stay consistent (the reference scales the
-   * force only). */
+   * force only).  An atom's arrangement may hold up to 254 cutting spheres,
+   * 254 circle transitions per batch and 128 exposed arcs; beyond that the
+   * step returns OG_E_UNSUPPORTED (the reference has no limit). */
   int32_t include_sasa;
   double sasa_gamma_scale;
   /* Born radii: 0 = plain OBC-II descreening pass, 1 = learned radii. */
