@@ -164,11 +164,10 @@ struct WarpSmemT {
   uint8_t skept[kSasaBatch], zpre[kSasaBatch];
   double bsk[kSasaBatch], binv[kSasaBatch];
   // crossing toggle of each transition, the toggles up to it in angular
-  // order, its sorted position, and per batch circle the mode (0: burial
+  // order, and per batch circle the mode (0: burial
   // depth by toggles, 1: explicit midpoint tests) and the depth before its
   // first transition
   int8_t ttog[kTrans], tdep[kTrans];
-  uint8_t trank[kTrans];
   int32_t bmode[kSasaBatch];
   int32_t bbase[kSasaBatch];
   // exposed arcs
@@ -525,12 +524,26 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
           rank += before;
           dep += before ? w.ttog[t] : 0;
         }
-        if (w.ttog[sl] == 0) atomicOr(&w.bmode[j], 1);
+        const int tg = w.ttog[sl];
+        if (tg == 0) {
+          atomicOr(&w.bmode[j], 1);
+        } else if (tg == -1) {
+          // burial depth (below): a leaving crossing wraps around the start
+          // of the circle when its pair's entering crossing -- the
+          // neighbouring slot of the same circle and cap -- sorts after it
+          const int m = w.tother[sl];
+          const int q = (sl + 1 < se && w.tother[sl + 1] == m) ? sl + 1 : sl - 1;
+          if (q < sb || w.ttog[q] != 1 || w.tother[q] != m) {
+            atomicOr(&w.bmode[j], 1);
+          } else {
+            const double aq = w.ta[q];
+            if (!((aq < as) || (aq == as && q < sl))) atomicAdd(&w.bbase[j], 1);
+          }
+        }
       }
       rank = min(rank, se - sb - 1);
       // the crossings up to and including this one, in angular order
       w.tdep[sl] = static_cast<int8_t>(dep + w.ttog[sl]);
-      w.trank[sl] = static_cast<uint8_t>(rank);
       w.torder[sb + rank] = static_cast<uint8_t>(sl);
     }
     if (__any_sync(kFull, nonfinite)) {
@@ -556,19 +569,9 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     // crossing cap once, so the depth just after a transition is the toggles
     // up to it plus the depth before the first transition -- the number of
     // caps whose leaving crossing comes before their entering one in angular
-    // order.  A segment is exposed where the depth is 0.  The other circles
-    // test every segment's midpoint against every cap.
-    for (int sl = lane; sl < n_tr; sl += 32) {
-      if (w.ttog[sl] != -1) continue;
-      const int j = w.tseg[sl], m = w.tother[sl];
-      // the pair's other transition is the neighbouring slot with the same
-      // circle and cap
-      const int q = (sl + 1 < n_tr && w.tother[sl + 1] == m && w.tseg[sl + 1] == j) ? sl + 1 : sl - 1;
-      if (q < 0 || w.ttog[q] != 1 || w.tother[q] != m || w.tseg[q] != j)
-        atomicOr(&w.bmode[j], 1);
-      else if (w.trank[sl] < w.trank[q])
-        atomicAdd(&w.bbase[j], 1);
-    }
+    // order, counted during the sort.  A segment is exposed where the depth
+    // is 0.  The other circles test every segment's midpoint against every
+    // cap.
     __syncwarp();
     if (__any_sync(kFull, dup)) {
       if (lane == 0) {
