@@ -152,3 +152,18 @@ def origami():
 @pytest.fixture(scope="session")
 def gpu_available():
     return have_gpu()
+
+
+# The reference's known answers (tests/golden/known_answers.json, written by
+# tests/golden/make_known_answers.py from the reference's tests, constants
+# and README, each value with its source line).
+_KNOWN = None
+
+
+def known(key: str):
+    global _KNOWN
+    if _KNOWN is None:
+        import json
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "known_answers.json")) as f:
+            _KNOWN = json.load(f)
+    return _KNOWN[key]["value"]

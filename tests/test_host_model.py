@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import ROOT, oracle
+from conftest import ROOT, oracle, known
 
 REF = "/root/reference"
 
@@ -39,7 +39,7 @@ def test_all_twenty_residue_atom_count(origami):
 
 def test_agaga_has_44_atoms(origami):
     # dynamics/tests/cotranslate_acceptance.rs:47-49
-    assert origami.Chain.build("AGAGA").n_atoms == 44
+    assert origami.Chain.build("AGAGA").n_atoms == known("cotranslate_agaga_atoms") == 44
 
 
 def test_backbone_bond_lengths(origami):
@@ -48,12 +48,12 @@ def test_backbone_bond_lengths(origami):
     x = ch.positions
     for r in range(20):
         n, ca, c, o = (index_of(ch, r, a) for a in ("N", "CA", "C", "O"))
-        assert abs(np.linalg.norm(x[ca] - x[n]) - 1.458) < 1e-6
-        assert abs(np.linalg.norm(x[c] - x[ca]) - 1.525) < 1e-6
-        assert abs(np.linalg.norm(x[o] - x[c]) - 1.231) < 1e-6
+        assert abs(np.linalg.norm(x[ca] - x[n]) - known("backbone_n_ca_a")) < 1e-6
+        assert abs(np.linalg.norm(x[c] - x[ca]) - known("backbone_ca_c_a")) < 1e-6
+        assert abs(np.linalg.norm(x[o] - x[c]) - known("backbone_c_o_a")) < 1e-6
         if r > 0:
             pc = index_of(ch, r - 1, "C")
-            assert abs(np.linalg.norm(x[n] - x[pc]) - 1.329) < 1e-6
+            assert abs(np.linalg.norm(x[n] - x[pc]) - known("backbone_peptide_c_n_a")) < 1e-6
 
 
 def test_no_clashes_in_extended_chain(origami):

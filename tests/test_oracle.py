@@ -10,14 +10,14 @@ import math
 import numpy as np
 import pytest
 
-from conftest import Orc, dp, oracle
+from conftest import Orc, dp, known, oracle
 
 TRP_CAGE = "NLYIQWLKDGGPSSGRPPPS"
 
 
 def test_coulomb_known_value():
-    # energy/src/nonbonded.rs known_coulomb_value: -332.0637/5 * 4.184 = -277.871 kJ/mol
-    assert abs(-332.0637 / 5.0 * 4.184 - (-277.871)) < 0.01
+    # energy/src/nonbonded.rs known_coulomb_value: +1e and -1e at 5 A
+    assert abs(-332.0637 / 5.0 * 4.184 - known("coulomb_unit_pair_5A_kj")) < 0.01
 
 
 def test_extended_trp_cage_pins(origami):
@@ -26,8 +26,10 @@ def test_extended_trp_cage_pins(origami):
     # recorded for earlier revisions of the force field, so the pins are loose).
     orc = Orc(origami.Chain.build(TRP_CAGE))
     e = orc.energy_terms()
-    assert abs(e["bond"] - 23494.0) / 23494.0 < 1e-3, e["bond"]
-    assert abs(e["total"] - 47506.0) / 47506.0 < 1e-2, e["total"]
+    bond, total = known("trp_cage_extended_bond_kj"), known("trp_cage_extended_total_kj")
+    assert total == known("readme_extended_total_kj")
+    assert abs(e["bond"] - bond) / bond < 1e-3, e["bond"]
+    assert abs(e["total"] - total) / total < 1e-2, e["total"]
 
 
 def test_born_radii_floor(origami):

@@ -18,7 +18,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import dp, oracle
+from conftest import dp, oracle, known
 
 TRP = "NLYIQWLKDGGPSSGRPPPS"
 
@@ -60,8 +60,10 @@ def area_gradient(x, r, i):
 
 
 def test_isolated_carbon_full_sphere():
-    a = areas(np.zeros((1, 3)), np.array([1.7 + 1.4]))
-    assert abs(a[0] - 4 * math.pi * 3.1**2) < 1e-6
+    # energy/src/sasa.rs isolated_carbon_full_sphere: 4 pi (vdW_C + probe)^2
+    rc = known("sasa_isolated_carbon_vdw_a") + known("sasa_probe_radius_a")
+    a = areas(np.zeros((1, 3)), np.array([rc]))
+    assert abs(a[0] - 4 * math.pi * rc**2) < 1e-6
 
 
 def test_single_cap_closed_form():
