@@ -386,9 +386,12 @@ def run_b200(args):
     e2e = aggregate_ns_per_day(ws, args.replicas, args.dt, e2e_s * 1e3)
 
     # per step: BAOAB sub-steps and SHAKE (6), Born pass + finalize or
-    # descriptors + fused network (2), force, near field, bonded (3), SASA (2)
-    sasa_k = 0 if args.no_sasa else 2
-    launches = 6 + 2 + 3 + sasa_k
+    # descriptors + fused network (2), force, near field, bonded (3), SASA
+    # (boundary, its large-capacity queue, terms: 3), and in cutoff mode the
+    # culled work lists (force; plus Born in the plain arm)
+    sasa_k = 0 if args.no_sasa else 3
+    cut_k = 0 if not args.cutoff else (2 if args.plain_only else 1)
+    launches = 6 + 2 + 3 + sasa_k + cut_k
     cfg = workload_config(args, chain)
     cfg["born"] = "plain OBC-II pass" if args.plain_only else "learned radii (network on tcgen05 GEMMs), plain-GB judge"
     line = {
