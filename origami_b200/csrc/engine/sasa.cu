@@ -50,6 +50,9 @@ constexpr int kSasaBatch = 32;        // circles per arrangement batch
 constexpr uint8_t kNoOther = 0xFF;    // pseudo entry of a transition-free circle
 constexpr int32_t kContained = 1 << 16;  // circle inside a cap it does not cross
 constexpr int32_t kCountMask = kContained - 1;
+// crossing masks: one bit per live circle below 63, bit 63 for kContained
+constexpr int kMaskCircles = 63;
+constexpr uint64_t kMaskContained = 1ull << 63;
 constexpr double kPi = 3.14159265358979323846;
 
 __device__ __forceinline__ D3 normalize(D3 a) { return a / norm(a); }
@@ -146,12 +149,18 @@ template <int kCaps_, int kTrans_, int kArcs_>
 struct WarpSmemT {
   static constexpr int kCaps = kCaps_, kTrans = kTrans_, kArcs = kArcs_;
   static_assert(kCaps <= 254 && kTrans <= 254, "byte-sized cap and transition indices");
+  static_assert(kCaps / 2 >= kMaskCircles, "a crossing mask for every circle of mask mode");
   // caps (indices in neighbour order, i.e. ascending atom index)
   double cx[kCaps], cy[kCaps], cz[kCaps], cc[kCaps];
   int32_t owner[kCaps];
   uint8_t live[kCaps];
-  // transitions of each live circle (low 16 bits) and kContained
-  int32_t tcnt[kCaps];
+  // per live circle either its transitions (low 16 bits) and kContained,
+  // or -- up to kMaskCircles live circles, no tangent pair -- the mask of
+  // the live circles it crosses (bit lm) and kMaskContained
+  union {
+    int32_t tcnt[kCaps];
+    uint64_t xmask[kCaps / 2];
+  };
   // transitions of the batch of circles being processed: sort key, unit
   // radial direction, the other cap, the batch circle, the sorted order
   double ta[kTrans], tx[kTrans], ty[kTrans], tz[kTrans];
@@ -206,6 +215,22 @@ __device__ __forceinline__ int nth_set_bit(unsigned mask, int n) {
     }
   }
   return pos;
+}
+
+// Transitions of live circle li (low 16 bits) and kContained: in mask mode
+// every crossing pair has two transitions.
+template <class W>
+__device__ __forceinline__ int32_t circle_tally(const W& w, int li, bool masks) {
+  if (!masks) return w.tcnt[li];
+  const uint64_t mk = w.xmask[li];
+  return 2 * __popcll(mk & ~kMaskContained) | ((mk & kMaskContained) ? kContained : 0);
+}
+
+// Sets bit b of circle li's crossing mask by a 32-bit atomic on the word
+// holding it (little-endian halves), which shared memory does natively.
+template <class W>
+__device__ __forceinline__ void mask_or(W& w, int li, int b) {
+  atomicOr(reinterpret_cast<unsigned*>(&w.xmask[li]) + (b >> 5), 1u << (b & 31));
 }
 
 enum Outcome { kExposed = 0, kBuried = 1, kBounded = 2, kInvalid = 3 };
@@ -358,30 +383,55 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
   // order, the reference's order.  A circle without transitions takes one
   // pseudo entry (its probe test).  A circle that lies inside a cap without
   // crossing its rim (possible only within the culling margin) is marked
-  // kContained.
-  for (int li = lane; li < n_live; li += 32) w.tcnt[li] = 0;
-  __syncwarp();
+  // kContained.  With at most kMaskCircles live circles the pass records
+  // which circles cross (masks), so that the writing pass visits only
+  // crossing pairs; a tangent pair (one transition) sends the atom back to
+  // plain counts.
   // p / n_live by a float reciprocal: exact here, since p + 0.5 keeps the
   // quotient at least 0.5 / n_live from an integer, far above the rounding
   const float inv_live = 1.0f / static_cast<float>(n_live);
-  // the counts are symmetric (circle k crosses cap m where circle m crosses
-  // cap k), so each unordered pair is classified once: row li, columns lm > li
-  const int n_pairs = n_live * n_live;
-  for (int p = lane; p < n_pairs; p += 32) {
-    const int li = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live), lm = p - li * n_live;
-    if (lm <= li) continue;
-    const Cap ck = cap_at(w, w.live[li]), cm = cap_at(w, w.live[lm]);
-    const PairClass pc = classify(ck, cm);
-    if (pc.count) {
-      atomicAdd(&w.tcnt[li], pc.count);
-      atomicAdd(&w.tcnt[lm], pc.count);
+  bool masks = n_live <= kMaskCircles;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (masks) {
+      for (int li = lane; li < n_live; li += 32) w.xmask[li] = 0;
     } else {
-      // a circle inside the other cap without crossing its rim
-      if (ck.c * pc.sigma - cm.c > -1e-9) atomicOr(&w.tcnt[li], kContained);
-      if (cm.c * pc.sigma - ck.c > -1e-9) atomicOr(&w.tcnt[lm], kContained);
+      for (int li = lane; li < n_live; li += 32) w.tcnt[li] = 0;
     }
+    __syncwarp();
+    // the counts are symmetric (circle k crosses cap m where circle m
+    // crosses cap k), so each unordered pair is classified once: row li,
+    // columns lm > li
+    const int n_pairs = n_live * n_live;
+    bool tangent = false;
+    for (int p = lane; p < n_pairs; p += 32) {
+      const int li = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live), lm = p - li * n_live;
+      if (lm <= li) continue;
+      const Cap ck = cap_at(w, w.live[li]), cm = cap_at(w, w.live[lm]);
+      const PairClass pc = classify(ck, cm);
+      // a circle inside the other cap without crossing its rim
+      const bool in_m = !pc.count && ck.c * pc.sigma - cm.c > -1e-9;
+      const bool in_k = !pc.count && cm.c * pc.sigma - ck.c > -1e-9;
+      if (masks) {
+        tangent |= pc.count == 1;
+        if (pc.count == 2) {
+          mask_or(w, li, lm);
+          mask_or(w, lm, li);
+        }
+        if (in_m) mask_or(w, li, 63);
+        if (in_k) mask_or(w, lm, 63);
+      } else {
+        if (pc.count) {
+          atomicAdd(&w.tcnt[li], pc.count);
+          atomicAdd(&w.tcnt[lm], pc.count);
+        }
+        if (in_m) atomicOr(&w.tcnt[li], kContained);
+        if (in_k) atomicOr(&w.tcnt[lm], kContained);
+      }
+    }
+    __syncwarp();
+    if (!masks || !__any_sync(kFull, tangent)) break;
+    masks = false;
   }
-  __syncwarp();
 
   int n_arcs = 0, n_verts = 0;
   bool bad = false;
@@ -389,7 +439,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     // the batch: consecutive live circles whose (padded) lists fit
     int b1 = b0, total = 0;
     while (b1 < n_live && b1 - b0 < kSasaBatch) {
-      const int sz = max(w.tcnt[b1] & kCountMask, 1);
+      const int sz = max(circle_tally(w, b1, masks) & kCountMask, 1);
       if (total + sz > W::kTrans) break;
       total += sz;
       ++b1;
@@ -402,7 +452,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     if (lane == 0) {
       int s0 = 0, z = 0;
       for (int j = 0; j < nb; ++j) {
-        const int c = w.tcnt[b0 + j] & kCountMask;
+        const int c = circle_tally(w, b0 + j, masks) & kCountMask;
         w.sbeg[j] = static_cast<uint16_t>(s0);
         w.zpre[j] = static_cast<uint8_t>(z);
         s0 += max(c, 1);
@@ -415,7 +465,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       const double sk = sqrt(fmax(1.0 - c * c, 0.0));
       w.bsk[j] = sk;
       w.binv[j] = sk > 0.0 ? 1.0 / sk : 0.0;
-      w.bmode[j] = (w.tcnt[b0 + j] & kContained) ? 1 : 0;
+      w.bmode[j] = (circle_tally(w, b0 + j, masks) & kContained) ? 1 : 0;
       w.bbase[j] = 0;
     }
     __syncwarp();
@@ -423,82 +473,138 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     // transitions: pairs (batch circle j, live circle m), j-major, m ascending
     // (the reference's push order), kept as unit radial directions u
     // (p = axis cos(alpha) + u sin(alpha)) with a pseudo-angle sort key.
-    // Pairs are classified 32 at a time; those that cross, with their
+    // In mask mode the crossing pairs are read from the masks.  Otherwise
+    // pairs are classified 32 at a time; those that cross, with their
     // output positions, go to a warp queue (one entry per lane) whose full
     // rounds build the points with every lane busy.
-    int run = 0, queued = 0;
-    unsigned qentry = 0;  // pair index | output position << 16
-    const int np = nb * n_live;
-    auto drain = [&](int n_entries) {
-      if (lane < n_entries) {
-        const int pidx = static_cast<int>(qentry & 0xFFFFu), base = static_cast<int>(qentry >> 16);
-        const int j = __float2int_rz((static_cast<float>(pidx) + 0.5f) * inv_live), m = w.live[pidx - j * n_live];
-        const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
-        const PairClass pc = classify(ck, cm);
-        D3 pt{}, qt{};
-        transition_points(ck, cm, pc, &pt, &qt);
-        const double inv = w.binv[j];
-        const D3 h = helper_axis(ck.axis);
-        const D3 fu = h - ck.axis * dot(h, ck.axis);  // the angle is scale-free
-        const D3 fv = cross(ck.axis, fu);
-        for (int e = 0; e < pc.count; ++e) {
-          const int sl = base + e;
-          if (sl >= w.sbeg[j + 1]) break;  // never expected: the counts agree
-          const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
-          w.ta[sl] = pseudo_angle(dot(u, fu), dot(u, fv));
-          w.tx[sl] = u.x;
-          w.ty[sl] = u.y;
-          w.tz[sl] = u.z;
-          w.tother[sl] = static_cast<uint8_t>(m);
-          w.tseg[sl] = static_cast<uint8_t>(j);
-          // crossing direction: moving counter-clockwise (along axis x u)
-          // the point enters cap m where the rate is positive and leaves it
-          // where negative; a tangent or a shallow crossing gets 0
-          const double rate = dot(cross(ck.axis, u), cm.axis);
-          w.ttog[sl] = pc.count == 1 ? 0 : (rate > 1e-4 ? 1 : (rate < -1e-4 ? -1 : 0));
-        }
+    int run = 0;
+    bool mismatch = false;
+    // the transitions of batch circle j with cap m from slot base on
+    // batch circle j's transitions on its crossing with cap m, the points
+    // in the order of the pair (circle j, cap m), from slot base on
+    auto put = [&](int j, int m, int count, D3 pt, D3 qt, int base) {
+      const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
+      const double inv = w.binv[j];
+      const D3 h = helper_axis(ck.axis);
+      const D3 fu = h - ck.axis * dot(h, ck.axis);  // the angle is scale-free
+      const D3 fv = cross(ck.axis, fu);
+      for (int e = 0; e < count; ++e) {
+        const int sl = base + e;
+        if (sl >= w.sbeg[j + 1]) break;  // never expected: the counts agree
+        const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
+        w.ta[sl] = pseudo_angle(dot(u, fu), dot(u, fv));
+        w.tx[sl] = u.x;
+        w.ty[sl] = u.y;
+        w.tz[sl] = u.z;
+        w.tother[sl] = static_cast<uint8_t>(m);
+        w.tseg[sl] = static_cast<uint8_t>(j);
+        // crossing direction: moving counter-clockwise (along axis x u)
+        // the point enters cap m where the rate is positive and leaves it
+        // where negative; a tangent or a shallow crossing gets 0
+        const double rate = dot(cross(ck.axis, u), cm.axis);
+        w.ttog[sl] = count == 1 ? 0 : (rate > 1e-4 ? 1 : (rate < -1e-4 ? -1 : 0));
       }
     };
-    for (int p0 = 0; p0 < np; p0 += 32) {
-      const int p = p0 + lane;
-      int cnt = 0, j = 0;
-      if (p < np) {
-        j = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live);
-        const int lm = p - j * n_live;
-        const int k = w.live[b0 + j], m = w.live[lm];
-        if (k != m) cnt = classify(cap_at(w, k), cap_at(w, m)).count;
+    if (masks) {
+      // the crossing pairs straight from the masks, 32 at a time: entry e
+      // belongs to the batch circle whose inclusive prefix of crossing
+      // partners first exceeds e, and is its r-th partner in ascending live
+      // order, with slots sbeg[j] + 2r and + 2r + 1.  (Sharing one
+      // intersection between the pairs (k, m) and (m, k) of two batch
+      // circles was measured slower: the lane holding both does two
+      // circles' slot work while the others wait.)
+      const uint64_t mj = lane < nb ? (w.xmask[b0 + lane] & ~kMaskContained) : 0ull;
+      int incl = __popcll(mj);
+      for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += v;
       }
-      // prefix of the counts (0, 1 or 2) from two ballots
-      const unsigned c1 = __ballot_sync(kFull, cnt & 1), c2 = __ballot_sync(kFull, cnt & 2);
-      const unsigned below = (1u << lane) - 1u;
-      const int off = __popc(c1 & below) + 2 * __popc(c2 & below);
-      const int tot = __popc(c1) + 2 * __popc(c2);
-      const unsigned packed = static_cast<unsigned>(p) | (static_cast<unsigned>(run + off + (cnt ? w.zpre[j] : 0)) << 16);
-      const unsigned crossing = __ballot_sync(kFull, cnt != 0);
-      const int n_new = __popc(crossing);
-      // lanes queued .. 31 take the first new entries
-      int t = lane - queued;
-      unsigned v = __shfl_sync(kFull, packed, (t >= 0 && t < n_new) ? nth_set_bit(crossing, t) : lane);
-      if (t >= 0 && t < n_new) qentry = v;
-      if (queued + n_new >= 32) {
-        drain(32);
-        // the rest start the next queue
-        t = lane + (32 - queued);
-        v = __shfl_sync(kFull, packed, t < n_new ? nth_set_bit(crossing, t) : lane);
-        if (t < n_new) qentry = v;
-        queued = queued + n_new - 32;
-      } else {
-        queued += n_new;
+      const int n_ent = __shfl_sync(kFull, incl, 31);
+      for (int e0 = 0; e0 < n_ent; e0 += 32) {
+        const int e = e0 + lane;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          if (__shfl_sync(kFull, incl, j + step - 1) <= e) j += step;
+        }
+        const uint64_t mk = __shfl_sync(kFull, mj, j);
+        const int r = e - (__shfl_sync(kFull, incl, j) - __popcll(mk));
+        if (e < n_ent) {
+          const unsigned lo = static_cast<unsigned>(mk);
+          const int clo = __popc(lo);
+          const int lm = r < clo ? nth_set_bit(lo, r) : 32 + nth_set_bit(static_cast<unsigned>(mk >> 32), r - clo);
+          const int m = w.live[lm];
+          const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
+          const PairClass pc = classify(ck, cm);
+          if (pc.count != 2) mismatch = true;  // never expected: classify is symmetric
+          D3 pt{}, qt{};
+          transition_points(ck, cm, pc, &pt, &qt);
+          put(j, m, pc.count, pt, qt, w.sbeg[j] + 2 * r);
+        }
       }
-      run += tot;
+      run = 2 * n_ent;
+    } else {
+      int queued = 0;
+      unsigned qentry = 0;  // pair index | output position << 16
+      const int np = nb * n_live;
+      auto drain = [&](int n_entries) {
+        if (lane < n_entries) {
+          const int pidx = static_cast<int>(qentry & 0xFFFFu), base = static_cast<int>(qentry >> 16);
+          const int j = __float2int_rz((static_cast<float>(pidx) + 0.5f) * inv_live);
+          const int m = w.live[pidx - j * n_live];
+          const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
+          const PairClass pc = classify(ck, cm);
+          D3 pt{}, qt{};
+          transition_points(ck, cm, pc, &pt, &qt);
+          put(j, m, pc.count, pt, qt, base);
+        }
+      };
+      for (int p0 = 0; p0 < np; p0 += 32) {
+        const int p = p0 + lane;
+        int cnt = 0, j = 0;
+        if (p < np) {
+          j = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live);
+          const int lm = p - j * n_live;
+          const int k = w.live[b0 + j], m = w.live[lm];
+          if (k != m) cnt = classify(cap_at(w, k), cap_at(w, m)).count;
+        }
+        // prefix of the counts (0, 1 or 2) from two ballots
+        const unsigned c1 = __ballot_sync(kFull, cnt & 1), c2 = __ballot_sync(kFull, cnt & 2);
+        const unsigned below = (1u << lane) - 1u;
+        const int off = __popc(c1 & below) + 2 * __popc(c2 & below);
+        const int tot = __popc(c1) + 2 * __popc(c2);
+        const unsigned packed =
+            static_cast<unsigned>(p) | (static_cast<unsigned>(run + off + (cnt ? w.zpre[j] : 0)) << 16);
+        const unsigned crossing = __ballot_sync(kFull, cnt != 0);
+        const int n_new = __popc(crossing);
+        // lanes queued .. 31 take the first new entries
+        int t = lane - queued;
+        unsigned v = __shfl_sync(kFull, packed, (t >= 0 && t < n_new) ? nth_set_bit(crossing, t) : lane);
+        if (t >= 0 && t < n_new) qentry = v;
+        if (queued + n_new >= 32) {
+          drain(32);
+          // the rest start the next queue
+          t = lane + (32 - queued);
+          v = __shfl_sync(kFull, packed, t < n_new ? nth_set_bit(crossing, t) : lane);
+          if (t < n_new) qentry = v;
+          queued = queued + n_new - 32;
+        } else {
+          queued += n_new;
+        }
+        run += tot;
+      }
+      drain(queued);
     }
-    drain(queued);
-    if (run + w.zpre[nb - 1] + ((w.tcnt[b1 - 1] & kCountMask) == 0 ? 1 : 0) != w.sbeg[nb]) {
+    if (__any_sync(kFull, mismatch)) {
+      bad = true;
+      break;
+    }
+    if (run + w.zpre[nb - 1] + ((circle_tally(w, b1 - 1, masks) & kCountMask) == 0 ? 1 : 0) != w.sbeg[nb]) {
       bad = true;  // the two passes disagree: never expected, but never written past
       break;
     }
     for (int j = lane; j < nb; j += 32) {
-      if ((w.tcnt[b0 + j] & kCountMask) != 0) continue;
+      if ((circle_tally(w, b0 + j, masks) & kCountMask) != 0) continue;
       const int sl = w.sbeg[j];
       w.tseg[sl] = static_cast<uint8_t>(j);
       w.tother[sl] = kNoOther;

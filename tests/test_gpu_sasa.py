@@ -167,11 +167,18 @@ def test_dense_atoms_beyond_default_capacity_match_oracle(origami):
     forces, areas and the surface energy still match the oracle, and the
     shell atoms below the limit take the default path in the same launch."""
     x, el = dense_shell_cluster(5, 140)
+    r = np.array([oracle().orc_sasa_radius(int(e)) for e in el])
+    d = np.linalg.norm(x - x[0], axis=1)
+    assert ((d > 0) & (d < r[0] + r)).sum() > 128
+    check_cluster(origami, x, el)
+
+
+def check_cluster(origami, x, el, forces=True):
+    """Surface forces (unless forces is False), analytical areas and
+    Shrake-Rupley areas of one uncharged cluster against the oracle."""
     o = oracle()
     r = np.array([o.orc_sasa_radius(int(e)) for e in el])
     g = np.array([o.orc_sasa_gamma(int(e), 1.0) for e in el])
-    d = np.linalg.norm(x - x[0], axis=1)
-    assert ((d > 0) & (d < r[0] + r)).sum() > 128
     t = cluster_topology(origami, el)
     on, off = origami.Params(), origami.Params()
     on.include_sasa = True
@@ -180,14 +187,56 @@ def test_dense_atoms_beyond_default_capacity_match_oracle(origami):
     e_off.add_system(t, x)
     e_on.finalize()
     e_off.finalize()
-    df = e_on.total_force(0) - e_off.total_force(0)
-    f_ref = oracle_sasa_forces(x, r, g)
-    assert np.abs(df - f_ref).max() < 1e-6, np.abs(df - f_ref).max()
+    if forces:
+        df = e_on.total_force(0) - e_off.total_force(0)
+        f_ref = oracle_sasa_forces(x, r, g)
+        assert np.abs(df - f_ref).max() < 1e-6, np.abs(df - f_ref).max()
     ref = oracle_areas(x, r)
     got = e_off.sasa_areas(0, "powersasa")
     assert np.all(np.abs(got - ref) <= 1e-9 * 4 * math.pi * r**2), np.abs(got - ref).max()
     sr = e_off.sasa_areas(0, "shrake_rupley", 960)
     np.testing.assert_allclose(sr, oracle_sr(x, r, 960), rtol=0, atol=1e-9)
+
+
+def fibonacci_directions(n):
+    k = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * k / n
+    phi = math.pi * (1.0 + 5.0 ** 0.5) * k
+    s = np.sqrt(1.0 - z * z)
+    return np.stack([s * np.cos(phi), s * np.sin(phi), z], 1)
+
+
+def test_many_live_circles_match_oracle(origami):
+    """A sulfur under 69 evenly spread hydrogens (75 directions, those near
+    the +z pole left out) whose caps on it are all 20 degrees: no cap lies
+    inside another, so all 69 circles stay live -- more than the crossing
+    masks cover -- each crossing 5 to 9 neighbours, and the caps cover the
+    sphere but for one hole at the pole.  The arrangement takes the plain
+    pair scan."""
+    o = oracle()
+    ri, rj, c = o.orc_sasa_radius(5), o.orc_sasa_radius(0), math.cos(math.radians(20.0))
+    d = c * ri + math.sqrt((c * ri) ** 2 - (ri * ri - rj * rj))
+    dirs = fibonacci_directions(75)
+    dirs = dirs[dirs[:, 2] < 0.85]
+    assert len(dirs) == 69
+    x = np.vstack([np.zeros(3), dirs * d])
+    el = np.array([5] + [0] * len(dirs))
+    check_cluster(origami, x, el)
+
+
+def test_tangent_circles_areas_match_oracle(origami):
+    """Two caps on a carbon whose circles touch at one point (30-degree
+    caps, axes 60 degrees apart: one transition each, by the tangent
+    tolerance) and a third cap crossing one of them.  The atom leaves the
+    crossing masks for plain counts.  Areas only: the reference's gradient
+    divides by the root of c_sq, which vanishes at tangency, so its forces
+    there are of order 1e7 and carry no parity."""
+    rc = oracle().orc_sasa_radius(1)
+    d = rc * math.sqrt(3.0)  # cap cosine d / (2 rc) = cos 30 degrees
+    a3 = np.array([math.cos(-0.35), math.sin(-0.35), 0.3])
+    dirs = np.array([[1.0, 0.0, 0.0], [math.cos(math.pi / 3), math.sin(math.pi / 3), 0.0], a3 / np.linalg.norm(a3)])
+    x = np.vstack([np.zeros(3), dirs * d])
+    check_cluster(origami, x, np.array([1, 1, 1, 1]), forces=False)
 
 
 @pytest.mark.parametrize("scale", [1.0, 0.25])
