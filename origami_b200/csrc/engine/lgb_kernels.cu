@@ -13,17 +13,20 @@ constexpr float kMu0 = 1.5f, kShell = 0.7f;
 constexpr float kInv2Sigma2 = 1.0f / (2.0f * 0.7f * 0.7f);
 constexpr float kCut = 12.0f;
 constexpr float kPiF = 3.14159265358979f;
+constexpr float kPiOverCut = kPiF / kCut;
 
 // Hawkins-Cramer-Truhlar pairwise descreening integral of atom i (offset
-// radius rti) by a partner sphere of scaled radius sj at distance r (the
-// standard closed form of the 1/r^4 volume integral outside atom i).
-__device__ __forceinline__ float hct_term(float r, float rti, float sj) {
+// radius rti) by a partner sphere of scaled radius sj at distance r, 1/r = ir
+// (the standard closed form of the 1/r^4 volume integral outside atom i).
+// Reciprocals by the special-function unit's approximation (relative error
+// of order 1e-7, far inside the descriptors' tolerance).
+__device__ __forceinline__ float hct_term(float r, float ir, float rti, float sj) {
   if (!(rti < r + sj)) return 0.0f;
   const float l = fmaxf(rti, fabsf(r - sj)), u = r + sj;
-  const float il = __frcp_rn(l), iu = __frcp_rn(u), ir = __frcp_rn(r);
+  const float il = __fdividef(1.0f, l), iu = __fdividef(1.0f, u);
   float t = 0.5f * (il - iu + 0.25f * r * (iu * iu - il * il) + 0.5f * ir * __logf(l * iu) +
                     0.25f * sj * sj * ir * (il * il - iu * iu));
-  if (rti < sj - r) t += 2.0f * (1.0f / rti - il);
+  if (rti < sj - r) t += 2.0f * (__fdividef(1.0f, rti) - il);
   return t;
 }
 
@@ -31,36 +34,35 @@ __device__ __forceinline__ float hct_term(float r, float rti, float sj) {
 // (2 sigma^2), by recurrence: with d = r - mu_s, g_{s+1} = g_s exp(a (2 D d -
 // D^2)) and g_{s-1} = g_s exp(-a (2 D d + D^2)) (D = 0.7), and each of those
 // factors changes by exp(-2 a D^2) = exp(-1) per shell (sigma = D).  Seeds at
-// shells kMid run the recurrence over [kLo, kHi]: two seeds of four shells
-// each side keep the error within a few 1e-6 of the shell value (about five
-// times the direct evaluation's) at 6 exponentials per partner instead of 16,
-// which is what bounds this kernel (the special-function unit).
-template <int kMid, int kLo, int kHi>
-__device__ __forceinline__ void add_shell_run(float* acc, float r, float w) {
+// shells 4 and 12 run the recurrence over [0, 7] and [8, 15]: two seeds of
+// four shells each side keep the error within a few 1e-6 of the shell value
+// (about five times the direct evaluation's) at 6 exponentials per partner
+// instead of 16, which is what bounds this kernel (the special-function
+// unit).  The two runs take the same steps, so they advance together as the
+// halves of packed FP32x2 values: acc[k] holds shells (k, k + 8).
+__device__ __forceinline__ void add_shells(float2* acc, float r, float w) {
   constexpr float kStep = 0.36787944117144233f;  // exp(-2 a D^2) = exp(-1)
-  const float d = r - (kMu0 + kShell * kMid);
-  const float g = __expf(-d * d * kInv2Sigma2);
-  float up = __expf(kInv2Sigma2 * (2.0f * kShell * d - kShell * kShell));
-  float dn = __expf(-kInv2Sigma2 * (2.0f * kShell * d + kShell * kShell));
-  acc[kMid] += w * g;
-  float gu = g, gd = g;
+  const float da = r - (kMu0 + kShell * 4), db = r - (kMu0 + kShell * 12);
+  const float2 g = make_float2(__expf(-da * da * kInv2Sigma2), __expf(-db * db * kInv2Sigma2));
+  float2 up = make_float2(__expf(kInv2Sigma2 * (2.0f * kShell * da - kShell * kShell)),
+                          __expf(kInv2Sigma2 * (2.0f * kShell * db - kShell * kShell)));
+  float2 dn = make_float2(__expf(-kInv2Sigma2 * (2.0f * kShell * da + kShell * kShell)),
+                          __expf(-kInv2Sigma2 * (2.0f * kShell * db + kShell * kShell)));
+  const float2 w2 = make_float2(w, w), step = make_float2(kStep, kStep);
+  acc[4] = __ffma2_rn(w2, g, acc[4]);
+  float2 gu = g, gd = g;
 #pragma unroll
-  for (int s = kMid + 1; s <= kHi; ++s) {
-    gu *= up;
-    up *= kStep;
-    acc[s] += w * gu;
+  for (int s = 5; s <= 7; ++s) {
+    gu = __fmul2_rn(gu, up);
+    up = __fmul2_rn(up, step);
+    acc[s] = __ffma2_rn(w2, gu, acc[s]);
   }
 #pragma unroll
-  for (int s = kMid - 1; s >= kLo; --s) {
-    gd *= dn;
-    dn *= kStep;
-    acc[s] += w * gd;
+  for (int s = 3; s >= 0; --s) {
+    gd = __fmul2_rn(gd, dn);
+    dn = __fmul2_rn(dn, step);
+    acc[s] = __ffma2_rn(w2, gd, acc[s]);
   }
-}
-
-__device__ __forceinline__ void add_shells(float* acc, float r, float w) {
-  add_shell_run<4, 0, 7>(acc, r, w);
-  add_shell_run<12, 8, 15>(acc, r, w);
 }
 
 // One block of four warps per tile of 32 i-atoms (lane = atom).  The warps
@@ -94,9 +96,9 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_lgb_desc(LgbDescArgs a) {
   const int cls1 = warp == 3 ? 2 : -1;
   const int stride_mask = warp < 2 ? 1 : 0;
   const int residue = warp < 2 ? warp : 0;
-  float acc[32];
+  float2 acc[16];  // per class, shells (k, k + 8)
 #pragma unroll
-  for (int k = 0; k < 32; ++k) acc[k] = 0.0f;
+  for (int k = 0; k < 16; ++k) acc[k] = make_float2(0.0f, 0.0f);
   float cfa = 0.0f;
   if (sys >= 0) {
     const int2 st = a.sys_tiles[sys];
@@ -135,24 +137,33 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_lgb_desc(LgbDescArgs a) {
           const float r2 = dx * dx + dy * dy + dz * dz;
           const bool ok = live_i && r2 < kCut * kCut && !(tj == ti && b == lane);
           if (!__any_sync(kFull, ok)) continue;  // partner out of range of the whole tile
-          const float r = sqrtf(r2);
-          const float fc = ok ? 0.5f * (__cosf(kPiF * r / kCut) + 1.0f) : 0.0f;
+          // r and 1/r from one reciprocal square root (r = 0 exactly for
+          // the atom itself, which ok excludes)
+          const float ir = rsqrtf(fmaxf(r2, 1e-6f));
+          const float r = r2 * ir;
+          const float fc = ok ? 0.5f * (__cosf(kPiOverCut * r) + 1.0f) : 0.0f;
           const float w = wb * fc;
-          if (ok) cfa += fc * hct_term(r, rti, sb);
+          if (ok) cfa += fc * hct_term(r, ir, rti, sb);
           if (cb == cls0)
             add_shells(acc, r, w);
           else
-            add_shells(acc + 16, r, w);
+            add_shells(acc + 8, r, w);
         }
       }
     }
   }
   // partial sums -> shared memory
 #pragma unroll
-  for (int k = 0; k < 16; ++k) part[warp][k][lane] = acc[k];
+  for (int k = 0; k < 8; ++k) {
+    part[warp][k][lane] = acc[k].x;
+    part[warp][k + 8][lane] = acc[k].y;
+  }
   if (cls1 >= 0) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) part[4][k][lane] = acc[16 + k];
+    for (int k = 0; k < 8; ++k) {
+      part[4][k][lane] = acc[8 + k].x;
+      part[4][k + 8][lane] = acc[8 + k].y;
+    }
   }
   cfa_part[warp][lane] = cfa;
   __syncthreads();

@@ -624,6 +624,8 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       if (w.tother[sl] != kNoOther) {
         const double as = w.ta[sl];
         if (!isfinite(as)) nonfinite = true;
+        // one loop over the circle (two loops split at sl, one comparison
+        // each, measured slower: the split point differs between lanes)
         for (int t = sb; t < se; ++t) {
           const double at = w.ta[t];
           const bool before = (at < as) || (at == as && t < sl);
