@@ -14,19 +14,51 @@ constexpr float kInv2Sigma2 = 1.0f / (2.0f * 0.7f * 0.7f);
 constexpr float kCut = 12.0f;
 constexpr float kPiF = 3.14159265358979f;
 constexpr float kPiOverCut = kPiF / kCut;
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kLn2 = 0.6931471805599453f;
+constexpr float kA2 = kInv2Sigma2 * kLog2e;  // shell exponent in base 2
+
+// Special-function-unit approximations (PTX .approx.ftz: one instruction
+// each, relative error of order 1e-7, subnormals flushed), for the
+// descriptor loop only; the descriptors' tolerance is 2e-5 on log(1 + D).
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float cos_approx(float x) {
+  float y;
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 
 // Hawkins-Cramer-Truhlar pairwise descreening integral of atom i (offset
 // radius rti) by a partner sphere of scaled radius sj at distance r, 1/r = ir
 // (the standard closed form of the 1/r^4 volume integral outside atom i).
-// Reciprocals by the special-function unit's approximation (relative error
-// of order 1e-7, far inside the descriptors' tolerance).
+// 1/l and 1/u come from one reciprocal of l u.
 __device__ __forceinline__ float hct_term(float r, float ir, float rti, float sj) {
   if (!(rti < r + sj)) return 0.0f;
   const float l = fmaxf(rti, fabsf(r - sj)), u = r + sj;
-  const float il = __fdividef(1.0f, l), iu = __fdividef(1.0f, u);
-  float t = 0.5f * (il - iu + 0.25f * r * (iu * iu - il * il) + 0.5f * ir * __logf(l * iu) +
+  const float q = rcp_approx(l * u);
+  const float il = u * q, iu = l * q;
+  float t = 0.5f * (il - iu + 0.25f * r * (iu * iu - il * il) + (0.5f * kLn2) * ir * lg2_approx(l * iu) +
                     0.25f * sj * sj * ir * (il * il - iu * iu));
-  if (rti < sj - r) t += 2.0f * (__fdividef(1.0f, rti) - il);
+  if (rti < sj - r) t += 2.0f * (rcp_approx(rti) - il);
   return t;
 }
 
@@ -43,11 +75,11 @@ __device__ __forceinline__ float hct_term(float r, float ir, float rti, float sj
 __device__ __forceinline__ void add_shells(float2* acc, float r, float w) {
   constexpr float kStep = 0.36787944117144233f;  // exp(-2 a D^2) = exp(-1)
   const float da = r - (kMu0 + kShell * 4), db = r - (kMu0 + kShell * 12);
-  const float2 g = make_float2(__expf(-da * da * kInv2Sigma2), __expf(-db * db * kInv2Sigma2));
-  float2 up = make_float2(__expf(kInv2Sigma2 * (2.0f * kShell * da - kShell * kShell)),
-                          __expf(kInv2Sigma2 * (2.0f * kShell * db - kShell * kShell)));
-  float2 dn = make_float2(__expf(-kInv2Sigma2 * (2.0f * kShell * da + kShell * kShell)),
-                          __expf(-kInv2Sigma2 * (2.0f * kShell * db + kShell * kShell)));
+  const float2 g = make_float2(ex2_approx(-da * da * kA2), ex2_approx(-db * db * kA2));
+  float2 up = make_float2(ex2_approx(kA2 * (2.0f * kShell * da - kShell * kShell)),
+                          ex2_approx(kA2 * (2.0f * kShell * db - kShell * kShell)));
+  float2 dn = make_float2(ex2_approx(-kA2 * (2.0f * kShell * da + kShell * kShell)),
+                          ex2_approx(-kA2 * (2.0f * kShell * db + kShell * kShell)));
   const float2 w2 = make_float2(w, w), step = make_float2(kStep, kStep);
   acc[4] = __ffma2_rn(w2, g, acc[4]);
   float2 gu = g, gd = g;
@@ -139,9 +171,9 @@ __global__ void __launch_bounds__(kDescWarps * 32) k_lgb_desc(LgbDescArgs a) {
           if (!__any_sync(kFull, ok)) continue;  // partner out of range of the whole tile
           // r and 1/r from one reciprocal square root (r = 0 exactly for
           // the atom itself, which ok excludes)
-          const float ir = rsqrtf(fmaxf(r2, 1e-6f));
+          const float ir = rsqrt_approx(fmaxf(r2, 1e-6f));
           const float r = r2 * ir;
-          const float fc = ok ? 0.5f * (__cosf(kPiOverCut * r) + 1.0f) : 0.0f;
+          const float fc = ok ? 0.5f * (cos_approx(kPiOverCut * r) + 1.0f) : 0.0f;
           const float w = wb * fc;
           if (ok) cfa += fc * hct_term(r, ir, rti, sb);
           if (cb == cls0)
