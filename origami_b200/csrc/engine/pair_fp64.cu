@@ -11,8 +11,10 @@ namespace ogk {
 // One warp per unordered near-field tile pair (i-tile <= j-tile) -- the
 // tiles that carry exclusion / 1-4 masks, i.e. the bonded neighbourhood
 // where the large LJ and Coulomb pair forces cancel against the bonded terms.
-// FP64 throughout, term for term as forces_nonbonded.rs:196-232 +
-// forces_gb.rs:82-111.  Each pair is evaluated once (Newton's third law):
+// FP64 throughout, the terms of forces_nonbonded.rs:196-232 +
+// forces_gb.rs:82-111 with their square roots and divisions rewritten as
+// reciprocal square roots and products (equal up to rounding; see the pair
+// loop).  Each pair is evaluated once (Newton's third law):
 // the j-tile's atoms are staged in the warp's shared memory, lane l meets
 // partner (l + k) mod 32 at step k, so within a step every lane touches a
 // different partner and the j-side sums need no atomics.  On a diagonal tile
@@ -23,9 +25,11 @@ namespace {
 
 constexpr int kNearWarps = 4;
 
+// The j-tile staged per warp: eps as its square root (the LJ mixing rule
+// sqrt(eps_i eps_j) as a product) and the Born radius with its inverse.
 struct NearTile {
-  double x[kTile], y[kTile], z[kTile], q[kTile], r[kTile];
-  double rmin[kTile], eps[kTile], rmin14[kTile], eps14[kTile];
+  double x[kTile], y[kTile], z[kTile], q[kTile], r[kTile], ir[kTile];
+  double rmin[kTile], seps[kTile], rmin14[kTile], seps14[kTile];
   double fx[kTile], fy[kTile], fz[kTile];
   int32_t valid[kTile];
 };
@@ -44,17 +48,19 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(PairArgs a, const in
   t.z[lane] = a.z64[jl];
   t.q[lane] = a.q64[jl];
   t.r[lane] = a.born_r64[jl];
+  t.ir[lane] = 1.0 / a.born_r64[jl];
   t.rmin[lane] = a.rmin64[jl];
-  t.eps[lane] = a.eps64[jl];
+  t.seps[lane] = sqrt(a.eps64[jl]);
   t.rmin14[lane] = a.rmin14_64[jl];
-  t.eps14[lane] = a.eps14_64[jl];
+  t.seps14[lane] = sqrt(a.eps14_64[jl]);
   t.valid[lane] = a.atom_valid[jl];
   t.fx[lane] = t.fy[lane] = t.fz[lane] = 0.0;
   const uint32_t ex = a.mask_ex[w.z * kTile + lane];
   const uint32_t m14 = a.mask_14[w.z * kTile + lane];
   const bool valid_i = a.atom_valid[i] != 0;
   const double xi = a.x64[i], yi = a.y64[i], zi = a.z64[i], qi = a.q64[i], Ri = a.born_r64[i];
-  const double rmi = a.rmin64[i], epi = a.eps64[i], rm14i = a.rmin14_64[i], ep14i = a.eps14_64[i];
+  const double rmi = a.rmin64[i], sepi = sqrt(a.eps64[i]), rm14i = a.rmin14_64[i], sep14i = sqrt(a.eps14_64[i]);
+  const double iRi = 1.0 / Ri;
   const double coul_kj = kCoulomb * kKcalToKj;
   const double gb_pref = (1.0 - 1.0 / kEpsWater) * kCoulomb * kKcalToKj;
   const bool diag = w.x == w.y;
@@ -70,23 +76,25 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(PairArgs a, const in
       const double r2 = dx * dx + dy * dy + dz * dz;
       const double qq = qi * t.q[p];
       if (r2 >= 1e-18) {
+        // 1/r from one reciprocal square root; the GB factor
+        // (1/f^2) ((2r - r e / 2) / (2f)) / r of the reference is
+        // (1 - e/4) / f^3, and f^-1 another reciprocal square root
+        const double inv_r = rsqrt(r2);
+        const double inv_r2 = inv_r * inv_r;
         if (!((ex >> p) & 1u) && r2 <= a.nb_c2_64) {
           const bool is14 = (m14 >> p) & 1u;
           const double rmin = is14 ? rm14i + t.rmin14[p] : rmi + t.rmin[p];
-          const double eps = sqrt(is14 ? ep14i * t.eps14[p] : epi * t.eps[p]);
-          const double inv_r2 = 1.0 / r2;
+          const double eps = is14 ? sep14i * t.seps14[p] : sepi * t.seps[p];
           const double ratio2 = rmin * rmin * inv_r2;
           const double r6 = ratio2 * ratio2 * ratio2;
           coeff += 12.0 * eps * inv_r2 * (r6 - r6 * r6) * kKcalToKj;
-          if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 / sqrt(r2) - a.inv_rc3_64);
+          if (qq != 0.0) coeff += -coul_kj * qq * (inv_r2 * inv_r - a.inv_rc3_64);
         }
         if (qq != 0.0 && r2 <= a.gb_c2_64) {
-          const double r = sqrt(r2);
           const double rp = Ri * t.r[p];
-          const double e = exp(-r2 / (4.0 * rp));
-          const double f2 = r2 + rp * e;
-          const double f = sqrt(f2);
-          coeff += gb_pref * qq / f2 * ((2.0 * r - 0.5 * r * e) / (2.0 * f)) / r;
+          const double e = exp(-0.25 * r2 * (iRi * t.ir[p]));
+          const double inv_f = rsqrt(r2 + rp * e);
+          coeff += gb_pref * qq * (1.0 - 0.25 * e) * (inv_f * inv_f * inv_f);
         }
       }
     }
