@@ -280,6 +280,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
   const int sys = a.atom_sys[i];
   const D3 pi = pos(a, i);
   const double ri = a.radius[i];
+  const double half_inv_ri = 0.5 / ri;
   const int2 st = a.sys_tiles[sys];
 
   // ---- caps (build_caps), neighbours in ascending atom order
@@ -304,17 +305,21 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       if (j != i && a.atom_sys[j] >= 0) {
         const double dx = a.x[j] - pi.x, dy = a.y[j] - pi.y, dz = a.z[j] - pi.z;
         const double rj = a.radius[j];
-        const double d = sqrt(dx * dx + dy * dy + dz * dz);
+        // d and 1/d from one reciprocal square root (d = 0 exactly for
+        // coincident centres); the quotients by d as products
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double inv_d = rsqrt(d2);
+        const double d = d2 > 0.0 ? d2 * inv_d : 0.0;
         if (d <= ri + rj) {
           if (d + ri <= rj) {
             enclosed = true;
           } else if (!(d + rj <= ri || d >= ri + rj)) {
-            ca = (d * d + ri * ri - rj * rj) / (2.0 * d * ri);
+            ca = (d2 + ri * ri - rj * rj) * (inv_d * half_inv_ri);
             if (ca >= -1.0 && ca <= 1.0) {
               is_cap = true;
-              ax = dx / d;
-              ay = dy / d;
-              az = dz / d;
+              ax = dx * inv_d;
+              ay = dy * inv_d;
+              az = dz * inv_d;
             }
           }
         }
