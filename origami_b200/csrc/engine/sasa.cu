@@ -93,9 +93,13 @@ __device__ __forceinline__ PairClass classify(Cap c1, Cap c2) {
   return r;
 }
 
-// The transition points of a pair with count 1 or 2 (q only for 2).
+// The transition points of a pair with count 1 or 2 (q only for 2).  For
+// unit axes |a1 x a2|^2 = 1 - sigma^2 = denom, so one reciprocal square root
+// of denom gives both 1 / denom and the normalisation of a1 x a2 (equal to
+// the reference's division and norm up to rounding).
 __device__ __forceinline__ void transition_points(Cap c1, Cap c2, PairClass pc, D3* p, D3* q) {
-  const double inv = 1.0 / pc.denom;
+  const double rd = rsqrt(pc.denom);
+  const double inv = rd * rd;
   const double a = (c1.c - pc.sigma * c2.c) * inv;
   const double b = (c2.c - pc.sigma * c1.c) * inv;
   const D3 base = c1.axis * a + c2.axis * b;
@@ -105,7 +109,7 @@ __device__ __forceinline__ void transition_points(Cap c1, Cap c2, PairClass pc, 
   }
   const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * pc.sigma;
   const D3 nc = cross(c1.axis, c2.axis);
-  const D3 off = nc * (sqrt(fmax(c_sq, 0.0)) * rsqrt(norm2(nc)));
+  const D3 off = nc * (sqrt(fmax(c_sq, 0.0)) * rd);
   *p = base + off;
   *q = base - off;
 }
