@@ -15,6 +15,10 @@ two transitions on a circle coincide and the reference keeps whichever sorts
 first by an FP64 angle that ties to the last bit.  Rounding decides that tie
 (and so which neighbour the vertex is attributed to), and the area is not
 differentiable there; on such builds only areas and energies are compared.
+
+In the tangent band (0 < c_sq <= 1e-9) the engine departs from the reference
+on purpose (vertex roots, link_boundary in sasa.cu): its forces there are
+checked against central differences of the oracle's surface energy instead.
 """
 from __future__ import annotations
 
@@ -230,13 +234,68 @@ def test_tangent_circles_areas_match_oracle(origami):
     tolerance) and a third cap crossing one of them.  The atom leaves the
     crossing masks for plain counts.  Areas only: the reference's gradient
     divides by the root of c_sq, which vanishes at tangency, so its forces
-    there are of order 1e7 and carry no parity."""
+    there are of order 1e7, with a sign rounding decides (the engine's forces
+    in the tangent band are checked against differences of the area in
+    test_tangent_band_forces_match_area_differences)."""
     rc = oracle().orc_sasa_radius(1)
     d = rc * math.sqrt(3.0)  # cap cosine d / (2 rc) = cos 30 degrees
     a3 = np.array([math.cos(-0.35), math.sin(-0.35), 0.3])
     dirs = np.array([[1.0, 0.0, 0.0], [math.cos(math.pi / 3), math.sin(math.pi / 3), 0.0], a3 / np.linalg.norm(a3)])
     x = np.vstack([np.zeros(3), dirs * d])
     check_cluster(origami, x, np.array([1, 1, 1, 1]), forces=False)
+
+
+def ch2_tangent_cluster(c_sq=5e-10):
+    """A carbon with two hydrogens at 1.111 A (a CH2 group under SHAKE) whose
+    H-C-H angle puts the two H caps on the carbon sphere in the tangent band,
+    0 < c_sq <= 1e-9: for equal caps of cosine c with axes at cos sigma,
+    c_sq = 1 - 2 c^2 / (1 + sigma), solved for sigma.  The three spheres then
+    nearly share one point, so the circles on each H sphere are in the band
+    too.  An oxygen adds a generic cap."""
+    o = oracle()
+    rc, rh = o.orc_sasa_radius(1), o.orc_sasa_radius(0)
+    d = 1.111
+    c = (d * d + rc * rc - rh * rh) / (2.0 * d * rc)
+    th = math.acos(2.0 * c * c / (1.0 - c_sq) - 1.0)
+    x = np.array([[0.0, 0.0, 0.0], [d, 0.0, 0.0], [d * math.cos(th), d * math.sin(th), 0.0], [-1.3, -0.9, 2.1]])
+    return x, np.array([1, 0, 0, 3])
+
+
+def test_tangent_band_forces_match_area_differences(origami):
+    """In the tangent band a pair has one transition, halfway between its two
+    roots, and the reference picks each vertex's root by proximity -- a tie
+    that rounding breaks -- so its analytical forces here are of order 1e4
+    kJ/mol/A with either sign (MD of CH2 groups meets this whenever the
+    H-C-H angle passes twice the cap angle).  The engine gives both vertices
+    of the pair the same root, which cancels the 1/sqrt(c_sq) terms: its
+    forces match central differences of the oracle's surface energy."""
+    x, el = ch2_tangent_cluster()
+    o = oracle()
+    r = np.array([o.orc_sasa_radius(int(e)) for e in el])
+    g = np.array([o.orc_sasa_gamma(int(e), 1.0) for e in el])
+    t = cluster_topology(origami, el)
+    on, off = origami.Params(), origami.Params()
+    on.include_sasa = True
+    e_on, e_off = origami.Engine(on), origami.Engine(off)
+    e_on.add_system(t, x)
+    e_off.add_system(t, x)
+    e_on.finalize()
+    e_off.finalize()
+    df = e_on.total_force(0) - e_off.total_force(0)
+
+    def energy(xx):
+        return float((g * oracle_areas(xx, r)).sum())
+
+    h = 1e-6
+    fd = np.zeros_like(x)
+    for k in range(len(x)):
+        for ax in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[k, ax] += h
+            xm[k, ax] -= h
+            fd[k, ax] = -(energy(xp) - energy(xm)) / (2.0 * h)
+    assert np.abs(fd).max() < 1.0
+    assert np.abs(df - fd).max() < 1e-3, np.abs(df - fd).max()
 
 
 @pytest.mark.parametrize("scale", [1.0, 0.25])
