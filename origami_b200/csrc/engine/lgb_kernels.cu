@@ -110,7 +110,7 @@ __device__ __forceinline__ void add_shells(float2* acc, float r, float w) {
 constexpr int kDescWarps = 4;
 constexpr int kDescSlots = 5;  // one per warp, plus the second class of warp 3
 
-__global__ void __launch_bounds__(kDescWarps * 32) k_lgb_desc(LgbDescArgs a) {
+__global__ void __launch_bounds__(kDescWarps * 32, 8) k_lgb_desc(LgbDescArgs a) {
   __shared__ float part[kDescSlots][16][33];  // [slot][shell][atom], padded
   __shared__ float cfa_part[kDescWarps][32];
   const int ti = blockIdx.x;
