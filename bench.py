@@ -94,6 +94,12 @@ class Clocks:
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            # wait (at most 5 s) for the first sample, taken before the timed
+            # region and left out, so that sampling is running when the
+            # region starts even when the region is short
+            import select
+            if select.select([self.proc.stdout], [], [], 5.0)[0]:
+                self.proc.stdout.readline()
         except Exception:
             self.proc = None
         return self

@@ -38,7 +38,8 @@ namespace {
 // Tuning knobs (compile-time): CTAs per SM the register budget is sized for
 // and groups of four j atoms in flight per lane.  Defaults are the measured
 // best on B200 for 64 x 4.7k-atom systems (Born pass 1.29 ms at 4 CTAs/SM vs
-// 1.68 ms at 2; force pass 1.34 ms at 2 CTAs/SM vs 1.43 ms at 4).
+// 1.68 ms at 2; force pass 1.34 ms at 2 CTAs/SM vs 1.38 ms at 3, 80
+// registers, and 1.43 ms at 4).
 #ifndef OG_BORN_MIN_BLOCKS
 #define OG_BORN_MIN_BLOCKS 4
 #endif
