@@ -298,6 +298,33 @@ def test_tangent_band_forces_match_area_differences(origami):
     assert np.abs(df - fd).max() < 1e-3, np.abs(df - fd).max()
 
 
+@pytest.mark.parametrize("relaxed", [False, True])
+def test_sasa_on_the_bench_chain_match_oracle(origami, relaxed):
+    """The benchmark's seeded 300-residue chain (4 694 atoms), as built and
+    after the bench's relaxation, each coordinate jittered by 0.02 A: surface
+    forces at the bench's gamma scale 0.25 and analytical areas against the
+    oracle -- the crossing masks, the pair-scan fallback and the
+    large-capacity queue at the workload's own size."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    seq, chain = bench.build_workload(origami, 300, 0)
+    if relaxed:
+        bench.relax(origami, chain, all_pairs=True)
+    rng = np.random.default_rng(17)
+    x = chain.positions + rng.normal(scale=0.02, size=chain.positions.shape)
+    r, g = radii_gamma(chain, 0.25)
+    with_s = engine(origami, chain, x, True, 0.25)
+    without = engine(origami, chain, x, False)
+    df = with_s.total_force(0) - without.total_force(0)
+    f_ref = oracle_sasa_forces(x, r, g)
+    assert np.abs(df - f_ref).max() < 1e-6, np.abs(df - f_ref).max()
+    got = without.sasa_areas(0, "powersasa")
+    ref = oracle_areas(x, r)
+    assert np.all(np.abs(got - ref) <= 1e-9 * 4 * math.pi * r**2), np.abs(got - ref).max()
+
+
 @pytest.mark.parametrize("scale", [1.0, 0.25])
 def test_sasa_forces_match_oracle(origami, scale):
     for name, ch, x in generic_chains(origami):
