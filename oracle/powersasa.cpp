@@ -1,7 +1,10 @@
 // ORACLE -- test infrastructure only.
 //
 // CPU FP64 restatement of origami's PowerSasa analytical SASA (Klenin et al.
-// 2011 spherical Gauss-Bonnet) and its analytical gradient.  Paths are
+// 2011 spherical Gauss-Bonnet) and its analytical gradient.  One extra entry
+// point, orc_sasa_forces_tangent_one_root, applies the engine's deliberate
+// change for tangent pairs (see build_atom_cache); orc_sasa_forces is the
+// reference's rule.  Paths are
 // relative to the reference's crates/energy/src/powersasa/ directory:
 //   geometry.rs      SmallCircle, intersect_circles (:70-102), signed angles
 //   arrangement.rs   build_caps (:69-97), find_boundary (:100-227),
@@ -524,8 +527,12 @@ struct CVert {
 
 // analytical.rs:101-214 (without the loop / component counts, which the
 // gradient does not use).  Returns false when the atom has no boundary.
+// tangent_one_root = false is the reference (each vertex's root by
+// proximity); true gives both vertices of a tangent pair the root
+// s = +1 for the lower cap index and -1 for the higher, the engine's rule.
 bool build_atom_cache(int i, const double* xyz, const double* radii, const std::vector<int>& cand,
-                      std::vector<int>* owners, std::vector<CArc>* carcs, std::vector<CVert>* cverts) {
+                      std::vector<int>* owners, std::vector<CArc>* carcs, std::vector<CVert>* cverts,
+                      bool tangent_one_root = false) {
   const V3 pi = P(xyz, i);
   const double ri = radii[i];
   std::vector<int> nb;
@@ -538,8 +545,14 @@ bool build_atom_cache(int i, const double* xyz, const double* radii, const std::
   const Boundary b = find_boundary(caps, &arcs, &verts);
   if (b != kBounded) return false;
   cverts->clear();
-  for (const Vert& v : verts)
-    cverts->push_back({v.in_cap, v.out_cap, identify_root_sign(caps[v.in_cap], caps[v.out_cap], v.point)});
+  for (const Vert& v : verts) {
+    V3 tp, tq;
+    const bool tangent =
+        tangent_one_root && intersect(caps[v.in_cap], caps[v.out_cap], &tp, &tq) == kTangent;
+    cverts->push_back({v.in_cap, v.out_cap,
+                       tangent ? (v.in_cap < v.out_cap ? kPlus : kMinus)
+                               : identify_root_sign(caps[v.in_cap], caps[v.out_cap], v.point)});
+  }
   auto find_vertex = [&](V3 t) {
     for (size_t k = 0; k < verts.size(); ++k)
       if (norm2(verts[k].point - t) < 1e-10) return static_cast<int>(k);
@@ -701,9 +714,12 @@ void orc_shrake_rupley_areas(int n, const double* xyz, const double* radii, int 
   }
 }
 
+}  // extern "C"
+
 // SASA forces F_x -= gamma_i dA_i/dr_x (add_sasa_forces_analytical,
 // analytical.rs:583-649); f is ADDED to.
-void orc_sasa_forces(int n, const double* xyz, const double* radii, const double* gamma, double* f) {
+void sasa_forces(int n, const double* xyz, const double* radii, const double* gamma, double* f,
+                 bool tangent_one_root) {
   std::vector<double> acc(3 * static_cast<size_t>(n), 0.0);
 #pragma omp parallel
   {
@@ -718,7 +734,7 @@ void orc_sasa_forces(int n, const double* xyz, const double* radii, const double
       std::vector<int> owners;
       std::vector<CArc> arcs;
       std::vector<CVert> verts;
-      if (!build_atom_cache(i, xyz, radii, cand, &owners, &arcs, &verts)) continue;
+      if (!build_atom_cache(i, xyz, radii, cand, &owners, &arcs, &verts, tangent_one_root)) continue;
       std::vector<int> affected{i};
       for (int o : owners)
         if (std::find(affected.begin(), affected.end(), o) == affected.end()) affected.push_back(o);
@@ -736,6 +752,21 @@ void orc_sasa_forces(int n, const double* xyz, const double* radii, const double
     for (size_t k = 0; k < acc.size(); ++k) acc[k] += local[k];
   }
   for (size_t k = 0; k < acc.size(); ++k) f[k] += acc[k];
+}
+
+extern "C" {
+
+// The reference's forces.
+void orc_sasa_forces(int n, const double* xyz, const double* radii, const double* gamma, double* f) {
+  sasa_forces(n, xyz, radii, gamma, f, false);
+}
+
+// The same with the engine's rule for tangent pairs (both vertices on one
+// root, which cancels the pair's 1/sqrt(c_sq) terms); equal to
+// orc_sasa_forces wherever no pair is in the tangent band.
+void orc_sasa_forces_tangent_one_root(int n, const double* xyz, const double* radii, const double* gamma,
+                                      double* f) {
+  sasa_forces(n, xyz, radii, gamma, f, true);
 }
 
 }  // extern "C"

@@ -84,6 +84,8 @@ def oracle() -> C.CDLL:
         o.orc_sasa_areas.restype = None
         o.orc_sasa_forces.argtypes = [C.c_int, dp, dp, dp, dp]
         o.orc_sasa_forces.restype = None
+        o.orc_sasa_forces_tangent_one_root.argtypes = [C.c_int, dp, dp, dp, dp]
+        o.orc_sasa_forces_tangent_one_root.restype = None
         o.orc_shrake_rupley_areas.argtypes = [C.c_int, dp, dp, C.c_int, dp]
         o.orc_shrake_rupley_areas.restype = None
         _oracle = o
@@ -167,3 +169,20 @@ def known(key: str):
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "known_answers.json")) as f:
             _KNOWN = json.load(f)
     return _KNOWN[key]["value"]
+
+
+def ch2_tangent_cluster(c_sq=5e-10):
+    """A carbon with two hydrogens at 1.111 A (a CH2 group under SHAKE) whose
+    H-C-H angle puts the two H caps on the carbon sphere in the PowerSasa
+    tangent band, 0 < c_sq <= 1e-9: for equal caps of cosine c with axes at
+    cos sigma, c_sq = 1 - 2 c^2 / (1 + sigma), solved for sigma.  The three
+    spheres then nearly share one point, so the circles on each H sphere are
+    in the band too.  An oxygen adds a generic cap.  Returns (xyz, elements)."""
+    import math
+    o = oracle()
+    rc, rh = o.orc_sasa_radius(1), o.orc_sasa_radius(0)
+    d = 1.111
+    c = (d * d + rc * rc - rh * rh) / (2.0 * d * rc)
+    th = math.acos(2.0 * c * c / (1.0 - c_sq) - 1.0)
+    x = np.array([[0.0, 0.0, 0.0], [d, 0.0, 0.0], [d * math.cos(th), d * math.sin(th), 0.0], [-1.3, -0.9, 2.1]])
+    return x, np.array([1, 0, 0, 3])

@@ -27,7 +27,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import Orc, dp, oracle
+from conftest import Orc, ch2_tangent_cluster, dp, oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -245,22 +245,6 @@ def test_tangent_circles_areas_match_oracle(origami):
     check_cluster(origami, x, np.array([1, 1, 1, 1]), forces=False)
 
 
-def ch2_tangent_cluster(c_sq=5e-10):
-    """A carbon with two hydrogens at 1.111 A (a CH2 group under SHAKE) whose
-    H-C-H angle puts the two H caps on the carbon sphere in the tangent band,
-    0 < c_sq <= 1e-9: for equal caps of cosine c with axes at cos sigma,
-    c_sq = 1 - 2 c^2 / (1 + sigma), solved for sigma.  The three spheres then
-    nearly share one point, so the circles on each H sphere are in the band
-    too.  An oxygen adds a generic cap."""
-    o = oracle()
-    rc, rh = o.orc_sasa_radius(1), o.orc_sasa_radius(0)
-    d = 1.111
-    c = (d * d + rc * rc - rh * rh) / (2.0 * d * rc)
-    th = math.acos(2.0 * c * c / (1.0 - c_sq) - 1.0)
-    x = np.array([[0.0, 0.0, 0.0], [d, 0.0, 0.0], [d * math.cos(th), d * math.sin(th), 0.0], [-1.3, -0.9, 2.1]])
-    return x, np.array([1, 0, 0, 3])
-
-
 def test_tangent_band_forces_match_area_differences(origami):
     """In the tangent band a pair has one transition, halfway between its two
     roots, and the reference picks each vertex's root by proximity -- a tie
@@ -268,7 +252,8 @@ def test_tangent_band_forces_match_area_differences(origami):
     kJ/mol/A with either sign (MD of CH2 groups meets this whenever the
     H-C-H angle passes twice the cap angle).  The engine gives both vertices
     of the pair the same root, which cancels the 1/sqrt(c_sq) terms: its
-    forces match central differences of the oracle's surface energy."""
+    forces match the oracle with the same rule, and central differences of
+    the oracle's surface energy."""
     x, el = ch2_tangent_cluster()
     o = oracle()
     r = np.array([o.orc_sasa_radius(int(e)) for e in el])
@@ -296,6 +281,10 @@ def test_tangent_band_forces_match_area_differences(origami):
             fd[k, ax] = -(energy(xp) - energy(xm)) / (2.0 * h)
     assert np.abs(fd).max() < 1.0
     assert np.abs(df - fd).max() < 1e-3, np.abs(df - fd).max()
+    xc = np.ascontiguousarray(x)
+    f_rule = np.zeros_like(xc)
+    o.orc_sasa_forces_tangent_one_root(len(xc), dp(xc), dp(r), dp(g), dp(f_rule))
+    assert np.abs(df - f_rule).max() < 1e-6, np.abs(df - f_rule).max()
 
 
 @pytest.mark.parametrize("relaxed", [False, True])

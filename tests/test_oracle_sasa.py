@@ -10,6 +10,9 @@ reference's own test cases, all on the CPU:
   extended Trp-cage (powersasa/mod.rs:161-172, 459-474)
 * Shrake-Rupley: isolated atom, far-apart atoms, extended 20-mer range
   (crates/energy/src/sasa.rs:205-277)
+* the engine's rule for tangent pairs (orc_sasa_forces_tangent_one_root):
+  the reference's forces wherever no pair is tangent, and the area's
+  central differences where one is
 """
 from __future__ import annotations
 
@@ -18,7 +21,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import dp, oracle, known
+from conftest import ch2_tangent_cluster, dp, known, oracle
 
 TRP = "NLYIQWLKDGGPSSGRPPPS"
 
@@ -176,3 +179,44 @@ def test_gamma_is_carbon_and_sulfur_only():
     assert o.orc_sasa_gamma(5, 0.25) == pytest.approx(0.25 * 0.005 * 4.184)
     for e in (0, 2, 3, 4):
         assert o.orc_sasa_gamma(e, 1.0) == 0.0
+
+
+def sasa_forces_one_root(x, r, g):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    f = np.zeros_like(x)
+    oracle().orc_sasa_forces_tangent_one_root(x.shape[0], dp(x), dp(np.ascontiguousarray(r)),
+                                              dp(np.ascontiguousarray(g)), dp(f))
+    return f
+
+
+def test_tangent_rule_changes_nothing_off_the_band(origami):
+    """On a jittered Trp-cage no pair is tangent: the two rules agree (to the
+    oracle's own run-to-run spread, ~1e-17: its OpenMP partial sums meet in
+    completion order)."""
+    ch = origami.Chain.build(TRP)
+    x = ch.positions + np.random.default_rng(8).normal(scale=0.02, size=ch.positions.shape)
+    r, g = radii_gamma(ch)
+    assert np.abs(sasa_forces(x, r, g) - sasa_forces_one_root(x, r, g)).max() < 1e-12
+
+
+def test_tangent_rule_matches_area_differences():
+    """A CH2 group in the tangent band: with both vertices of each tangent
+    pair on one root, the analytical force equals the central differences
+    of the oracle's own area.  (The reference's rule picks the roots by a
+    rounding-decided proximity test here; its value is not asserted.)"""
+    x, el = ch2_tangent_cluster()
+    o = oracle()
+    r = np.array([o.orc_sasa_radius(int(e)) for e in el])
+    g = np.array([o.orc_sasa_gamma(int(e), 1.0) for e in el])
+    f = sasa_forces_one_root(x, r, g)
+    h = 1e-6
+    fd = np.zeros_like(x)
+    for k in range(len(x)):
+        for ax in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[k, ax] += h
+            xm[k, ax] -= h
+            fd[k, ax] = -((g * areas(xp, r)).sum() - (g * areas(xm, r)).sum()) / (2.0 * h)
+    assert np.abs(fd).max() < 1.0
+    assert np.abs(f - fd).max() < 1e-3, np.abs(f - fd).max()
+
