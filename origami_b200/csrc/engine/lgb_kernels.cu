@@ -19,8 +19,8 @@ constexpr float kLn2 = 0.6931471805599453f;
 constexpr float kA2 = kInv2Sigma2 * kLog2e;  // shell exponent in base 2
 
 // Special-function-unit approximations (PTX .approx.ftz: one instruction
-// each, relative error of order 1e-7, subnormals flushed), for the
-// descriptor loop only; the descriptors' tolerance is 2e-5 on log(1 + D).
+// each, errors of 1e-7 to 1e-6, subnormals flushed), for the descriptor
+// loop only; the descriptors' tolerance is 2e-5 on log(1 + D).
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
