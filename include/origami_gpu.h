@@ -129,6 +129,22 @@ og_status og_set_data_dir(const char* path);
 og_status og_chain_build(const char* sequence, double phi, double psi, double omega, og_chain** out);
 /* Appends one residue at the C terminus (cotranslate.rs:204 append_residue). */
 og_status og_chain_append(og_chain* chain, char residue, double phi, double psi, double omega);
+/* A chain from a structure the caller already holds: origami's
+ * geom::Structure (geom/src/structure.rs), residues in order, each with its
+ * chain id and its atoms' names, elements and positions -- what read_pdb
+ * (io/src/pdb_read.rs:167) returns and what the CLI's energy / minimize /
+ * dynamics commands score.  residues: n_residues one-letter codes; chains:
+ * one chain id per residue (NULL = all 'A'; the peptide bond C(i-1)-N(i) is
+ * made only inside a chain, topology_graph.rs:199-209); atoms_per_residue:
+ * n_residues counts; names: 8 bytes per atom, NUL-padded wwPDB v3.3 names
+ * as the residue templates use them; elements: 0 H, 1 C, 2 N, 3 O, 4 P, 5 S
+ * per atom (NULL = from the name's first letter, pdb_read.rs:452-462); xyz:
+ * 3 doubles per atom.  Atom order is kept as given.  An atom the force field
+ * cannot type is OG_E_DATA (ForceScratch::rebuild_params panics there,
+ * scratch.rs:202-205). */
+og_status og_chain_from_structure(int32_t n_residues, const char* residues, const char* chains,
+                                  const int32_t* atoms_per_residue, const char* names, const int32_t* elements,
+                                  const double* xyz, og_chain** out);
 og_status og_chain_n_atoms(const og_chain* chain, int32_t* n_atoms);
 og_status og_chain_n_residues(const og_chain* chain, int32_t* n_residues);
 /* Topology arrays stay valid until the chain is modified or freed. */
@@ -340,18 +356,27 @@ og_status og_profile_read(og_engine* e, og_kernel_time* out, int32_t cap, int32_
  * when they need the energy: a host whose GPU memory is reserved up front by
  * another framework's caching allocator, or a latency-critical loop that
  * forbids allocation (and the device synchronisation it implies) after
- * start-up.  Computes what gb_energy returns (Born radii with descreening
- * pairs within born_cutoff, self term, pair sum over ALL pairs; FP64) into
- * energy_out[0..2] = {gb, self, pair} in kJ/mol.  Every pointer is a device
- * pointer the caller owns: xyz (3 * n_atoms, interleaved), charge, gb_rho,
- * gb_scale (n_atoms each), energy_out (3); work is queued on `stream`
- * (cudaStream_t, NULL = legacy default stream) and the call does not wait.
- * Scratch is a fixed device array inside the library, sized for at most
- * OG_NOALLOC_MAX_ATOMS atoms (~129 KiB held on every GPU that loads the
- * library until exit); larger systems are rejected with OG_E_BADARG.  The
- * first call on a device looks up that array's address (do it before any
- * stream capture).  All calls share the array, so calls that overlap on the
- * GPU race: order them. */
+ * start-up.  Computes, in FP64, OBC-II effective Born radii (HCT
+ * descreening over the pairs within born_cutoff, <= 0 or >= 1e30 = all
+ * pairs; tanh map; radius floor) and then the generalized-Born energy: the
+ * per-atom self terms plus the pair terms over ALL pairs, written as
+ * energy_out[0..2] = {total, self, pair} in kJ/mol.  Every pointer is a
+ * device pointer the caller owns: xyz (3 * n_atoms, interleaved), charge,
+ * gb_rho, gb_scale (n_atoms each), energy_out (3); work is queued on
+ * `stream` (cudaStream_t, NULL = legacy default stream) and the call does
+ * not wait.  Scratch is a fixed device array inside the library, sized for
+ * at most OG_NOALLOC_MAX_ATOMS atoms (~129 KiB held on every GPU that uses
+ * it until exit); larger systems are rejected with OG_E_BADARG.
+ * Set-up: the driver places that array and the kernels in device memory the
+ * first time they are used on a device (CUDA's lazy module loading), which
+ * can fail once another allocator holds all the memory.  A call with
+ * n_atoms = 0 and every pointer NULL does that set-up for the current device
+ * and nothing else; make it (or a first real call) before other frameworks
+ * reserve their memory, and before any stream capture.  Each call outside
+ * capture looks the array's address up again, so a cudaDeviceReset between
+ * calls is harmless; calls made during capture reuse the last address found.
+ * All calls share the array, so calls that overlap on the GPU race: order
+ * them. */
 #define OG_NOALLOC_MAX_ATOMS 16384
 og_status og_gb_energy_noalloc(const double* xyz, const double* charge, const double* gb_rho,
                                const double* gb_scale, int32_t n_atoms, double born_cutoff,

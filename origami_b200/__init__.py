@@ -87,6 +87,28 @@ class Chain:
         _check(lib().og_chain_build(sequence.encode(), phi, psi, omega, C.byref(h)))
         return cls(h)
 
+    @classmethod
+    def from_structure(cls, residues: str, atoms_per_residue, names, xyz, elements=None,
+                       chains: str | None = None) -> "Chain":
+        """A chain from a structure held by the caller (og_chain_from_structure):
+        one-letter residue codes, atom counts per residue, atom names in
+        wwPDB v3.3 form, positions (n x 3) and optionally element codes
+        (0 H .. 5 S) and one chain id per residue."""
+        counts = np.ascontiguousarray(atoms_per_residue, dtype=np.int32)
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        if len(residues) != counts.shape[0] or int(counts.sum()) != x.shape[0] or len(names) != x.shape[0]:
+            raise ValueError("residue, count, name and position arrays disagree")
+        name_buf = b"".join(n.encode()[:8].ljust(8, b"\0") for n in names)
+        el = None
+        if elements is not None:
+            el = np.ascontiguousarray(elements, dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().og_chain_from_structure(
+            len(residues), residues.encode(), None if chains is None else chains.encode(),
+            counts.ctypes.data_as(F.c_int32_p), name_buf,
+            None if el is None else el.ctypes.data_as(F.c_int32_p), _dptr(x), C.byref(h)))
+        return cls(h)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h and _lib is not None:

@@ -90,6 +90,8 @@ SIGNATURES = [
     ("og_set_data_dir", C.c_int, [C.c_char_p]),
     ("og_chain_build", C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_void_p)]),
     ("og_chain_append", C.c_int, [C.c_void_p, C.c_char, C.c_double, C.c_double, C.c_double]),
+    ("og_chain_from_structure", C.c_int, [C.c_int32, C.c_char_p, C.c_char_p, c_int32_p, C.c_char_p, c_int32_p,
+                                          c_double_p, C.POINTER(C.c_void_p)]),
     ("og_chain_n_atoms", C.c_int, [C.c_void_p, c_int32_p]),
     ("og_chain_n_residues", C.c_int, [C.c_void_p, c_int32_p]),
     ("og_chain_topology", C.c_int, [C.c_void_p, C.POINTER(C.POINTER(og_topology))]),

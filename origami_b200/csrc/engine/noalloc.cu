@@ -14,10 +14,20 @@
 //                      (16 384 + 128 doubles, ~129 KiB on every GPU that
 //                      loads the library, held until the process exits).
 //
-// Host code cannot use the array's name as a device address, so the first
-// call on each device looks the address up with cudaGetSymbolAddress (with
-// that device current) and caches it; that first call should come before any
-// stream capture.  Every call shares the one array: calls whose kernels
+// The driver places that array (and the three kernels' code) in device
+// memory when it loads this file's module, which with CUDA's default lazy
+// loading happens at the first use, not at library load.  A call with
+// n_atoms = 0 and every pointer NULL does only that set-up -- loads the
+// module and resolves the array's address on the current device -- so a
+// caller whose memory another allocator will reserve makes that call first.
+//
+// Host code cannot use the array's name as a device address, so each call
+// looks the address up with cudaGetSymbolAddress with the target device
+// current (the lookup allocates nothing once the module is loaded), which
+// also keeps the address right after a cudaDeviceReset has replaced the
+// context.  A call issued while its stream is being captured does not look
+// anything up: it uses the address the last call outside capture on that
+// device found.  Every call shares the one array: calls whose kernels
 // overlap on the GPU (two streams, or two host threads) race and must be
 // ordered by the caller.  Nothing in the scratch needs to start at zero --
 // every element a call reads is written earlier in the same call.
@@ -132,21 +142,41 @@ __global__ void k_noalloc_total(const double* __restrict__ partial, int n_blocks
   out[2] = pair_e * ogk::kKcalToKj;
 }
 
-// Device address of the scratch array for the current device (looked up once
-// per device, with that device current).
-og_status scratch_address(double** out) {
+// Loads this module on the current device (under lazy loading the driver
+// places the scratch array and the kernels' code at this point) and returns
+// the scratch array's device address there.  Outside stream capture the
+// address is looked up afresh and cached per device; inside capture the
+// cached address is used, since a lookup could have to load the module.
+og_status scratch_address(cudaStream_t stream, double** out) {
   int dev = 0;
   cudaError_t err = cudaGetDevice(&dev);
   if (err != cudaSuccess) return og_fail(OG_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(err));
   if (dev < 0 || dev >= kMaxDevices) return og_fail(OG_E_UNSUPPORTED, "device index beyond the supported range");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  err = cudaStreamIsCapturing(stream, &cap);
+  if (err != cudaSuccess) return og_fail(OG_E_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(err));
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (err != cudaSuccess || !p)
-      return og_fail(OG_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(err));
-    g_scratch_ptr[dev] = static_cast<double*>(p);
+  if (cap != cudaStreamCaptureStatusNone) {
+    if (!g_scratch_ptr[dev])
+      return og_fail(OG_E_STATE, "og_gb_energy_noalloc: first call on this device made during stream capture; "
+                                 "make a set-up call (n_atoms = 0, NULL pointers) before capturing");
+    *out = g_scratch_ptr[dev];
+    return OG_OK;
   }
+  cudaFuncAttributes attr;
+  const void* kernels[] = {reinterpret_cast<const void*>(&k_noalloc_radii),
+                           reinterpret_cast<const void*>(&k_noalloc_energy),
+                           reinterpret_cast<const void*>(&k_noalloc_total)};
+  for (const void* k : kernels) {
+    err = cudaFuncGetAttributes(&attr, k);
+    if (err != cudaSuccess)
+      return og_fail(OG_E_CUDA, std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(err));
+  }
+  void* p = nullptr;
+  err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (err != cudaSuccess || !p)
+    return og_fail(OG_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(err));
+  g_scratch_ptr[dev] = static_cast<double*>(p);
   *out = g_scratch_ptr[dev];
   return OG_OK;
 }
@@ -156,18 +186,19 @@ og_status scratch_address(double** out) {
 extern "C" og_status og_gb_energy_noalloc(const double* xyz, const double* charge, const double* gb_rho,
                                           const double* gb_scale, int32_t n_atoms, double born_cutoff,
                                           double* energy_out, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* scratch = nullptr;
+  if (n_atoms == 0 && !xyz && !charge && !gb_rho && !gb_scale && !energy_out) return scratch_address(s, &scratch);
   if (!xyz || !charge || !gb_rho || !gb_scale || !energy_out) return og_fail(OG_E_BADARG, "null argument");
   if (n_atoms < 1 || n_atoms > kNoAllocMaxAtoms)
     return og_fail(OG_E_BADARG, "og_gb_energy_noalloc: n_atoms must be in [1, " +
                                     std::to_string(kNoAllocMaxAtoms) + "], got " + std::to_string(n_atoms));
-  double* scratch = nullptr;
-  og_status st = scratch_address(&scratch);
+  og_status st = scratch_address(s, &scratch);
   if (st != OG_OK) return st;
   double* radii = scratch;
   double* partial = scratch + kNoAllocMaxAtoms;
   const double c2 = (!(born_cutoff > 0.0) || born_cutoff >= 1e30) ? static_cast<double>(INFINITY)
                                                                    : born_cutoff * born_cutoff;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int blocks = (n_atoms + kThreads - 1) / kThreads;
   k_noalloc_radii<<<blocks, kThreads, 0, s>>>(xyz, gb_rho, gb_scale, n_atoms, c2, radii);
   k_noalloc_energy<<<blocks, kThreads, 0, s>>>(xyz, charge, radii, n_atoms, partial);

@@ -239,6 +239,42 @@ og_status og_chain_append(og_chain* c, char residue, double phi, double psi, dou
   return rebuild(c);
 }
 
+og_status og_chain_from_structure(int32_t n_residues, const char* residues, const char* chains,
+                                  const int32_t* atoms_per_residue, const char* names, const int32_t* elements,
+                                  const double* xyz, og_chain** out) {
+  if (!out) return og_fail(OG_E_BADARG, "null argument");
+  *out = nullptr;
+  if (n_residues < 1 || !residues || !atoms_per_residue || !names || !xyz)
+    return og_fail(OG_E_BADARG, "og_chain_from_structure: null array or no residues");
+  auto c = std::make_unique<og_chain>();
+  int64_t k = 0;
+  for (int32_t r = 0; r < n_residues; ++r) {
+    const int aa = og::aa_from_one_letter(residues[r]);
+    if (aa < 0) return og_fail(OG_E_BADARG, std::string("not an amino-acid code: ") + residues[r]);
+    if (atoms_per_residue[r] < 0) return og_fail(OG_E_BADARG, "negative atom count");
+    og::PlacedResidue res;
+    res.aa = aa;
+    res.chain = chains ? chains[r] : 'A';
+    for (int32_t a = 0; a < atoms_per_residue[r]; ++a, ++k) {
+      og::PlacedAtom at;
+      at.name.assign(names + 8 * k, strnlen(names + 8 * k, 8));
+      if (elements) {
+        if (elements[k] < 0 || elements[k] > 5) return og_fail(OG_E_BADARG, "element code out of range");
+        at.element = static_cast<og::Element>(elements[k]);
+      } else if (!og::element_from_symbol(at.name.substr(0, 1), &at.element)) {
+        return og_fail(OG_E_DATA, "cannot determine the element of atom " + at.name);
+      }
+      at.pos = og::Vec3{xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]};
+      res.atoms.push_back(at);
+    }
+    c->s.residues.push_back(std::move(res));
+  }
+  og_status st = rebuild(c.get());
+  if (st != OG_OK) return st;
+  *out = c.release();
+  return OG_OK;
+}
+
 og_status og_chain_n_atoms(const og_chain* c, int32_t* n) {
   if (!c || !n) return og_fail(OG_E_BADARG, "null argument");
   *n = c->s.atom_count();

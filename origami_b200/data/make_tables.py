@@ -22,9 +22,9 @@ tokens unchanged, so the C++ loader (origami_b200/csrc/host/forcefield.cpp)
 applies the reference's first-wins / append semantics to exactly the same
 inputs.
 
-Usage:  python origami_b200/data/make_tables.py [REFERENCE_ROOT]
-(default reference root: /root/reference).  Run it only where the reference
-source is present; the outputs are committed.
+Usage:  python origami_b200/data/make_tables.py REFERENCE_ROOT
+(or with ORIGAMI_REFERENCE_DIR set).  Run it only where the reference source
+is present; the outputs are committed.
 """
 from __future__ import annotations
 
@@ -349,7 +349,9 @@ def parse_rtf(text: str, tpl: dict) -> dict[tuple[str, str], str]:
 
 
 def main(argv: list[str]) -> int:
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.environ.get("ORIGAMI_REFERENCE_DIR", "")
+    if not ref:
+        raise SystemExit(__doc__)
     with open(os.path.join(ref, "crates/chem/src/topology_data.rs")) as fh:
         tpl = parse_templates(fh.read())
     assert sorted(tpl) == sorted(AA3), sorted(tpl)

@@ -171,6 +171,66 @@ def known(key: str):
     return _KNOWN[key]["value"]
 
 
+_HOST_GOLDEN = None
+
+
+def host_golden() -> dict:
+    """tests/golden/host_model.npz by case: {case: {array: value}} (the
+    independent host-model oracle's output, tests/golden/make_host_golden.py)."""
+    global _HOST_GOLDEN
+    if _HOST_GOLDEN is None:
+        z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "host_model.npz"))
+        out = {}
+        for key in z.files:
+            case, name = key.split("/", 1)
+            out.setdefault(case, {})[name] = z[key]
+        _HOST_GOLDEN = out
+    return _HOST_GOLDEN
+
+
+class GoldenSystem:
+    """An og_topology over the golden (oracle-built) arrays of one case, with
+    the case's coordinates: what Orc needs, without the product's host model."""
+
+    TOPO_FIELDS = ("charge", "rmin_half", "epsilon", "rmin_half_14", "epsilon_14", "gb_rho", "gb_scale", "mass")
+
+    def __init__(self, case: dict, positions=None):
+        self.case = case
+        self._keep = {}
+
+        def arr(name, dt):
+            a = np.ascontiguousarray(case["topo_" + name], dtype=dt)
+            self._keep[name] = a
+            return a
+
+        t = F.og_topology()
+        t.n_atoms = int(case["counts"].sum())
+        for f in self.TOPO_FIELDS:
+            setattr(t, f, arr(f, np.float64).ctypes.data_as(F.c_double_p))
+        t.element = arr("element", np.int32).ctypes.data_as(F.c_int32_p)
+        i32 = lambda n: arr(n, np.int32).ctypes.data_as(F.c_int32_p)  # noqa: E731
+        f64 = lambda n: arr(n, np.float64).ctypes.data_as(F.c_double_p)  # noqa: E731
+        t.n_bonds, t.bond_atoms, t.bond_k, t.bond_r0 = len(case["topo_bond_k"]), i32("bonds"), f64("bond_k"), f64("bond_r0")
+        t.n_angles, t.angle_atoms = len(case["topo_angle_k"]), i32("angles")
+        t.angle_k, t.angle_theta0 = f64("angle_k"), f64("angle_theta0")
+        t.n_dihedrals = len(case["topo_dihedral_term_start"]) - 1
+        t.dihedral_atoms, t.dihedral_term_start = i32("dihedrals"), i32("dihedral_term_start")
+        t.n_dihedral_terms = len(case["topo_term_k"])
+        t.term_k, t.term_n, t.term_delta = f64("term_k"), i32("term_n"), f64("term_delta")
+        t.n_impropers, t.improper_atoms = len(case["topo_improper_k"]), i32("impropers")
+        t.improper_k, t.improper_psi0 = f64("improper_k"), f64("improper_psi0")
+        t.n_exclusions, t.exclusion_atoms = len(case["topo_exclusion_kind"]), i32("exclusions")
+        t.exclusion_kind = arr("exclusion_kind", np.int8).ctypes.data_as(F.c_int8_p)
+        t.n_constraints, t.constraint_atoms = len(case["topo_constraint_length"]), i32("constraints")
+        t.constraint_length = f64("constraint_length")
+        self.topo = t
+        self.positions = np.array(case["xyz"] if positions is None else positions, dtype=np.float64).reshape(-1, 3)
+        self.n_atoms = t.n_atoms
+
+    def topology_ptr(self):
+        return C.pointer(self.topo)
+
+
 def ch2_tangent_cluster(c_sq=5e-10):
     """A carbon with two hydrogens at 1.111 A (a CH2 group under SHAKE) whose
     H-C-H angle puts the two H caps on the carbon sphere in the PowerSasa

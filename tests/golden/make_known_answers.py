@@ -73,6 +73,19 @@ def extract(root: str) -> dict:
     put("sasa_isolated_carbon_vdw_a", num(v), src, "isolated carbon: area 4 pi (vdW + probe)^2")
     v, src = find(root, "crates/dynamics/tests/cotranslate_acceptance.rs", r"assert_eq!\(final_s\.atom_count\(\), (\d+)\)")
     put("cotranslate_agaga_atoms", int(v), src, "Ala-Gly-Ala-Gly-Ala grown by cotranslate")
+    v, src = find(root, "README.md", r"native 1L2Y an energy ([\d,]+) kJ/mol below")
+    put("readme_native_1l2y_gap_kj", num(v), src, "extended minus native 1L2Y total (no SASA)")
+    for key, name, pat in (
+            ("m7_chignolin_min_gap_kj", "GYDPETGTWG", r"\"GYDPETGTWG\",\s*([\d.]+),"),
+            ("m7_trp_cage_min_gap_kj", "NLYIQWLKDGGPSSGRPPPS", r"\"NLYIQWLKDGGPSSGRPPPS\",\s*([\d.]+),"),
+            ("m7_villin_min_gap_kj", "villin", r"gap > ([\d_.]+),\s*\n\s*\"villin")):
+        v, src = find(root, "crates/io/tests/m7_native_vs_extended.rs", pat)
+        put(key, num(v), src, f"native {name} scores at least this far below the extended build")
+    v, src = find(root, "crates/io/tests/m7_native_vs_extended.rs", r"max_steps: (\d+),\s*\n\s*gradient_tol: ([\d.]+)")
+    put("m7_villin_lbfgs_steps", int(v), src, "L-BFGS steps on the villin fixture before scoring (gtol 50, "
+        "energy tol 1, max step 0.1 A)")
+    v, src = find(root, "crates/energy/src/nonbonded.rs", r"pub const DEFAULT_CUTOFF_A: f64 = ([\d.]+);")
+    put("nonbonded_default_cutoff_a", num(v), src, "LJ / Coulomb cutoff of the energy the pins use")
     return out
 
 

@@ -1,8 +1,9 @@
 """Pins the CPU oracle (the checker of every GPU parity test) to origami's
 known answers and its own invariants: the Coulomb constant, finite-difference
 gradients of every term (the reference's main correctness tool, ε = 1e-5),
-Newton's third law, the extended Trp-cage energy terms, the xoshiro256++
-stream.  CPU only."""
+Newton's third law, the xoshiro256++ stream.  The whole-structure energy
+pins (extended and native Trp-cage, chignolin, villin) are in
+tests/test_host_oracle.py.  CPU only."""
 from __future__ import annotations
 
 import math
@@ -18,18 +19,6 @@ TRP_CAGE = "NLYIQWLKDGGPSSGRPPPS"
 def test_coulomb_known_value():
     # energy/src/nonbonded.rs known_coulomb_value: +1e and -1e at 5 A
     assert abs(-332.0637 / 5.0 * 4.184 - known("coulomb_unit_pair_5A_kj")) < 0.01
-
-
-def test_extended_trp_cage_pins(origami):
-    # dynamics/tests/trp_cage_minimise.rs:1-5 records the extended Trp-cage's
-    # bond term as +23494 kJ/mol and README.md:35 its total as +47506 (both
-    # recorded for earlier revisions of the force field, so the pins are loose).
-    orc = Orc(origami.Chain.build(TRP_CAGE))
-    e = orc.energy_terms()
-    bond, total = known("trp_cage_extended_bond_kj"), known("trp_cage_extended_total_kj")
-    assert total == known("readme_extended_total_kj")
-    assert abs(e["bond"] - bond) / bond < 1e-3, e["bond"]
-    assert abs(e["total"] - total) / total < 1e-2, e["total"]
 
 
 def test_born_radii_floor(origami):

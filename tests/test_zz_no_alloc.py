@@ -3,12 +3,15 @@ allocate device memory when they need it (their GPU memory is reserved up
 front by another allocator, or their loop forbids allocation after start-up).
 
 The entry point keeps its scratch in a fixed array inside the library, so
-this test hands it only device buffers the test owns (torch tensors) and
-checks two calls in a row -- on two different conformations, so a second
-call cannot pass on what the first left in the shared scratch -- against the
-engine's own FP64 energy path (og_compute_energies), within the 1e-6
-relative tolerance of the other energy tests.  Collected last so that a run
-stopping at its first failure has already run every other test.
+this test hands it only device buffers the test owns (torch tensors).  It
+makes the set-up call first (n_atoms = 0, every pointer NULL: loads the
+kernels and the array on the device), then checks two calls in a row -- on
+two different conformations, so a second call cannot pass on what the first
+left in the shared scratch -- against the engine's own FP64 energy path
+(og_compute_energies) and against the FP64 CPU oracle, within the 1e-6
+relative tolerance of the other energy tests, and checks that the device's
+free memory is the same before and after a call.  Collected last so that a
+run stopping at its first failure has already run every other test.
 """
 from __future__ import annotations
 
@@ -16,6 +19,8 @@ import math
 
 import numpy as np
 import pytest
+
+from conftest import Orc
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +46,7 @@ def test_gb_energy_noalloc_matches_engine(origami):
     out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream().cuda_stream
     n = chain.n_atoms
+    assert lib.og_gb_energy_noalloc(None, None, None, None, 0, 20.0, None, stream) == 0, lib.og_last_error()
 
     for x in (x1, x2):
         eng = origami.Engine(origami.Params())
@@ -49,13 +55,20 @@ def test_gb_energy_noalloc_matches_engine(origami):
         ref = eng.energies(0)
         eng.close()
 
+        orc = Orc(chain).energy_terms(x, nb=10.0, born=20.0)
+
         xyz = torch.tensor(x.reshape(-1), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         st = lib.og_gb_energy_noalloc(_dev(xyz), _dev(q), _dev(rho), _dev(scale), n, 20.0, _dev(out), stream)
         assert st == 0, lib.og_last_error()
         torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info(dev)[0] == free_before  # the call took no device memory
         gb, self_e, pair = out.tolist()
-        for got, want in ((gb, ref["gb"]), (self_e, ref["gb_self"]), (pair, ref["gb_pair"])):
+        for got, want, oracle_want in ((gb, ref["gb"], orc["gb"]), (self_e, ref["gb_self"], orc["gb_self"]),
+                                       (pair, ref["gb_pair"], orc["gb_pair"])):
             assert abs(got - want) <= 1e-6 * max(abs(want), 1.0), (got, want)
+            assert abs(got - oracle_want) <= 1e-6 * max(abs(oracle_want), 1.0), (got, oracle_want)
 
 
 def test_gb_energy_noalloc_rejects_oversized_systems(origami):
