@@ -10,6 +10,11 @@ Metric: aggregate ns/day over all replicas (and GPUs).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
 
+The system (sequence, topology arrays, relaxed coordinates) is read from
+tests/golden/bench_chain_300.npz, written once by
+tests/golden/make_bench_chain.py, so every arm times the same input; other
+sizes or seeds are built and relaxed on the GPU at start-up.
+
 Timing: CUDA events on the engine's stream (torch's current stream), one
 event pair per step with a 256 MiB L2 flush before each; under torchrun the
 max over ranks.  `e2e` is the same metric through the C ABI with the whole
@@ -39,12 +44,26 @@ METRIC = "aggregate ns/day (64 replicas, 5k atoms, GB+SASA): learned-GB vs plain
 # replica's packed arrays stay in L2 across its tile sweep, so the traffic
 # grows with replicas, not with pairs.
 FORCE_PASS_DRAM_BYTES_PER_REPLICA = 1.514496e6 / 4
+FIXTURE = os.path.join(ROOT, "tests", "golden", "bench_chain_300.npz")
+TOPO_FIELDS = ("charge", "rmin_half", "epsilon", "rmin_half_14", "epsilon_14", "gb_rho", "gb_scale", "mass",
+               "element", "bonds", "bond_k", "bond_r0", "angles", "angle_k", "angle_theta0", "dihedrals",
+               "dihedral_term_start", "term_k", "term_n", "term_delta", "impropers", "improper_k", "improper_psi0",
+               "exclusions", "exclusion_kind", "constraints", "constraint_length")
 
 
 def seeded_sequence(n_res: int, seed: int) -> str:
     from origami_b200 import Xoshiro256pp
     rng = Xoshiro256pp(seed)
     return "".join(AA_ORDER[min(int(rng.next_f64() * 20), 19)] for _ in range(n_res))
+
+
+def fixture_arrays(args) -> dict | None:
+    """The benchmark system from the committed fixture when the workload is
+    the fixture's (300 residues, seed 0), else None."""
+    if args.residues != 300 or args.seed != 0 or args.no_fixture or not os.path.exists(FIXTURE):
+        return None
+    z = np.load(FIXTURE)
+    return {k: z[k] for k in z.files}
 
 
 def dist_env():
@@ -147,97 +166,118 @@ def relax(og, chain, all_pairs: bool, max_steps: int = 300):
     return res
 
 
-def cpu_sample(chain, dt_fs: float, replicas: int, budget_s: float = 15.0, all_pairs: bool = True,
-               sasa_scale: float | None = 0.25) -> dict:
-    """Oracle port (FP64, OpenMP over all host threads): BAOAB+SHAKE steps of
-    one replica, plus (when sasa_scale is set) one analytical PowerSasa force
-    evaluation per step timed beside it; returns aggregate ns/day for
-    `replicas` replicas run on the CPU."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from conftest import INF, Orc, dp, oracle
-    orc = Orc(chain)
-    x = np.ascontiguousarray(chain.positions)
+def cpu_sample(arrays: dict, xyz: np.ndarray, dt_fs: float, budget_s: float = 15.0, all_pairs: bool = True,
+               sasa_scale: float | None = 0.25, max_steps: int = 50, warmup: int = 0) -> dict:
+    """The CPU oracle (FP64, OpenMP over all host threads) stepping one
+    replica: each step is one BAOAB+SHAKE step (its force evaluation
+    included) plus, with sasa_scale set, one analytical PowerSasa force
+    evaluation.  `warmup` steps run first, untimed.  Returns the seconds of
+    each timed step and the SASA share.  Only the oracle's library is loaded
+    (oracle/orc.py)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    s_ = orc.System(arrays)
+    o = orc.lib()
+    x = np.ascontiguousarray(xyz, dtype=np.float64).copy()
     v = np.zeros_like(x)
-    cut = (INF, INF, INF) if all_pairs else (10.0, 20.0, 10.0)
-    f = orc.total_force(x, *cut)
-    el_sasa = 0.0
+    cut = (orc.INF, orc.INF, orc.INF) if all_pairs else (10.0, 20.0, 10.0)
+    f = s_.total_force(x, *cut)
     if sasa_scale is not None:
-        el_ = np.array(chain.topology().element)
-        rad = np.array([oracle().orc_sasa_radius(int(e)) for e in el_])
-        gam = np.array([oracle().orc_sasa_gamma(int(e), sasa_scale) for e in el_])
+        rad, gam = s_.sasa_params(sasa_scale)
         fs = np.zeros_like(x)
-    steps, t0 = 0, time.perf_counter()
+    times, el_sasa, step = [], 0.0, 0
+    t_all = time.perf_counter()
     while True:
-        oracle().orc_baoab(orc.tp, dp(x), dp(v), dp(f), 1, dt_fs, 2.0, 310.0, 1, 0, 0, steps, *cut)
+        t0 = time.perf_counter()
+        o.orc_baoab(s_.tp, orc.dp(x), orc.dp(v), orc.dp(f), 1, dt_fs, 2.0, 310.0, 1, 0, 0, step, *cut)
         if sasa_scale is not None:
             ts = time.perf_counter()
             fs[:] = 0.0
-            oracle().orc_sasa_forces(x.shape[0], dp(x), dp(rad), dp(gam), dp(fs))
-            el_sasa += time.perf_counter() - ts
-        steps += 1
-        el = time.perf_counter() - t0
-        if el > budget_s or steps >= 50:
+            o.orc_sasa_forces(x.shape[0], orc.dp(x), orc.dp(rad), orc.dp(gam), orc.dp(fs))
+            if step >= warmup:
+                el_sasa += time.perf_counter() - ts
+        if step >= warmup:
+            times.append(time.perf_counter() - t0)
+        step += 1
+        if len(times) >= max_steps or (times and time.perf_counter() - t_all > budget_s):
             break
-    per_step = el / steps  # one replica
-    agg = dt_fs * 1e-6 / (per_step * replicas) * 86400.0
-    what = "BAOAB+SHAKE step(s)" + (" + PowerSasa force evaluation(s)" if sasa_scale is not None else "")
+    return {"step_s": times, "sasa_share": el_sasa / sum(times), "atoms": x.shape[0]}
+
+
+def cpu_line(sample: dict, args, replicas: int) -> dict:
+    """CPU throughput as the aggregate ns/day of `replicas` replicas run back
+    to back on the same cores (each step of the whole set takes replicas x
+    one replica's step, so the aggregate equals one replica's rate)."""
+    per = statistics.median(sample["step_s"])
+    agg = replicas * args.dt * 1e-6 / (replicas * per) * 86400.0
+    what = "BAOAB+SHAKE step" + ("" if args.no_sasa else " + PowerSasa force evaluation")
     return {"value": agg, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{steps} {what} of 1 replica ({chain.n_atoms} atoms, all pairs, FP64 oracle, "
-                      f"OpenMP {os.cpu_count()} threads; SASA share {el_sasa / el:.0%}), scaled to {replicas} "
-                      "replicas run back to back"}
+            "sample": f"{len(sample['step_s'])} timed {what}(s) of one replica ({sample['atoms']} atoms, "
+                      f"{'cutoff' if args.cutoff else 'all pairs'}, FP64 oracle, OpenMP {os.cpu_count()} threads; "
+                      f"SASA share {sample['sasa_share']:.0%}); {replicas} replicas run back to back give the "
+                      "same aggregate rate",
+            "seconds_per_replica_step": per}
 
 
 def run_reference(args):
+    """The CPU arm: origami's force-and-integrate path as restated by the
+    oracle (the reference itself is Rust and cannot be built here), on the
+    fixture system.  A step is one replica's BAOAB+SHAKE step with one
+    PowerSasa force evaluation; the 64 replicas would run back to back on
+    these cores, so the aggregate ns/day is one replica's rate.  Loads no
+    product code.  Rank 0 only."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    import origami_b200 as og
-    seq, chain = build_workload(og, args.residues, args.seed)
-    samples = []
-    for _ in range(args.warmup):
-        pass  # the oracle has no warm-up state; warm-up steps are skipped on the CPU arm
-    t_all = time.perf_counter()
-    for _ in range(max(args.steps, 1)):
-        samples.append(cpu_sample(chain, args.dt, args.replicas, budget_s=5.0, all_pairs=not args.cutoff,
-                                  sasa_scale=None if args.no_sasa else args.sasa_gamma_scale)["value"])
-        if time.perf_counter() - t_all > 120:
-            break
-    val = statistics.median(samples)
-    per_step_ms = args.dt * 1e-6 / val * 86400.0 * 1e3
+    arrays = fixture_arrays(args)
+    if arrays is None:
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU arm reads its system from "
+                          "tests/golden/bench_chain_300.npz (300 residues, seed 0); this workload has none"}))
+        return
+    t0 = time.perf_counter()
+    sample = cpu_sample(arrays, arrays["xyz"], args.dt, budget_s=args.reference_budget, all_pairs=not args.cutoff,
+                        sasa_scale=None if args.no_sasa else args.sasa_gamma_scale, max_steps=max(args.steps, 1),
+                        warmup=args.warmup)
+    wall = time.perf_counter() - t0
+    cpu = cpu_line(sample, args, args.replicas)
+    per_ms = 1e3 * statistics.mean(sample["step_s"])
     line = {
-        "impl": "reference", "metric": METRIC, "value": val, "unit": "ns/day", "n_gpus": args.gpus,
-        "steps": len(samples), "warmup": args.warmup, "ms_per_step": per_step_ms, "higher_is_better": True,
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "ns/day", "n_gpus": args.gpus,
+        "steps": len(sample["step_s"]), "warmup": args.warmup, "ms_per_step": per_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, chain),
-        "cpu_baseline": {"value": val, "unit": "ns/day", "cores": os.cpu_count(), "kind": "port",
-                         "sample": "BAOAB+SHAKE steps (+ one PowerSasa force evaluation each) of one replica "
-                                   "for about 5 s per timed step, FP64 oracle (CPU restatement of origami's "
-                                   "force/integrator path), OpenMP over all host threads, scaled to "
-                                   f"{args.replicas} replicas"},
-        "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": workload_config(args, int(arrays["xyz"].shape[0]), "plain OBC-II pass"),
+        "step": "one replica's BAOAB+SHAKE step (force evaluation included) plus one PowerSasa force evaluation; "
+                f"the {args.replicas} replicas run back to back, so the aggregate ns/day is one replica's rate",
+        "replicas_timed_per_step": 1,
+        "ms_per_step_all_replicas": per_ms * args.replicas,
+        "same_config": True,
+        "system": "tests/golden/bench_chain_300.npz (the GPU arm's input)",
+        "wall_s": wall,
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cpu["value"], "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-def workload_config(args, chain):
+def workload_config(args, atoms: int, born: str):
     surface = "no SASA" if args.no_sasa else f"PowerSasa gamma scale {args.sasa_gamma_scale}"
     return {"workload": f"{args.replicas} replicas x {args.residues}-residue seeded chain, "
                         f"{'reference cutoffs 10/20/10 A' if args.cutoff else 'all pairs (no cutoff)'}, "
-                        f"dt {args.dt} fs + SHAKE, 310 K, plain GB + {surface}",
-            "replicas": args.replicas, "residues": args.residues, "atoms_per_replica": chain.n_atoms,
+                        f"dt {args.dt} fs + SHAKE, 310 K, GB ({born}) + {surface}",
+            "replicas": args.replicas, "residues": args.residues, "atoms_per_replica": atoms,
             "mode": "cutoff" if args.cutoff else "all_pairs", "dt_fs": args.dt, "shake": True,
             "sasa": None if args.no_sasa else {"method": "analytical PowerSasa", "gamma_scale": args.sasa_gamma_scale},
-            "born": "plain OBC-II pass", "l2": "flushed (256 MiB write) before every timed step",
+            "born": born, "l2": "flushed (256 MiB write) before every timed step",
             "seed": args.seed}
 
 
-def make_engine(og, args, chain, rank: int, born_mode: int, stream):
+def make_engine(og, args, topo, xyz, rank: int, born_mode: int, stream):
     mk = og.Params if args.cutoff else og.Params.all_pairs
     params = mk(dt_fs=args.dt, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1000 * rank,
                 include_sasa=not args.no_sasa, sasa_gamma_scale=args.sasa_gamma_scale, born_mode=born_mode)
     eng = og.Engine(params)
     for _ in range(args.replicas):
-        eng.add_system(chain, chain.positions, 310.0)
+        eng.add_system(topo, xyz, 310.0)
     eng.finalize()
     eng.set_stream(stream.cuda_stream)
     for r in range(args.replicas):
@@ -316,14 +356,30 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
-    seq, chain = build_workload(og, args.residues, args.seed)
-    if not args.no_relax:
-        relax(og, chain, all_pairs=not args.cutoff)
-    atoms = chain.n_atoms
+    arrays = fixture_arrays(args)
+    if arrays is not None:
+        # the committed system; the product's own build of its sequence must
+        # give the same topology (the fixture is the product's output)
+        seq, xyz = str(arrays["seq"]), arrays["xyz"]
+        topo = og.Topology(**{f: arrays["topo_" + f] for f in TOPO_FIELDS})
+        own = og.Chain.build(seq).topology()
+        for f in TOPO_FIELDS:
+            if not np.array_equal(np.asarray(getattr(own, f)), arrays["topo_" + f]):
+                raise SystemExit(f"bench fixture topology differs from this build's ({f})")
+        system = "tests/golden/bench_chain_300.npz (relaxed coordinates and topology)"
+    else:
+        seq, chain = build_workload(og, args.residues, args.seed)
+        if not args.no_relax:
+            relax(og, chain, all_pairs=not args.cutoff)
+        t = chain.topology()
+        arrays = {"topo_" + f: np.asarray(getattr(t, f)) for f in TOPO_FIELDS}
+        topo, xyz = chain, chain.positions
+        system = "built and relaxed at start-up" if not args.no_relax else "extended build"
+    atoms = int(xyz.shape[0])
     pairs = args.replicas * atoms * (atoms - 1) / 2
 
     # ---- plain GB arm
-    plain = make_engine(og, args, chain, rank, 0, stream)
+    plain = make_engine(og, args, topo, xyz, rank, 0, stream)
     plain_ms, plain_clk = timed_steps(plain, args, stream, flush, local, ws)
     plain.profile(True)
     plain.step(5)
@@ -336,7 +392,7 @@ def run_b200(args):
     learned_info = None
     if not args.plain_only:
         params, train_info = train_network(og, args, stream)
-        eng = make_engine(og, args, chain, rank, 1, stream)
+        eng = make_engine(og, args, topo, xyz, rank, 1, stream)
         lgb.set_params(eng, params)
         lgb.set_judge(eng, args.judge_interval, 1e-3)
         torch.cuda.synchronize()
@@ -358,7 +414,7 @@ def run_b200(args):
                         "kernels_ms_per_step": {k: v[0] / v[1] for k, v in lprof.items()}}
         ms_per_step = eff_ms
     else:
-        eng = make_engine(og, args, chain, rank, 0, stream)
+        eng = make_engine(og, args, topo, xyz, rank, 0, stream)
         ms_per_step, clk = plain_ms, plain_clk
     value = aggregate_ns_per_day(ws, args.replicas, args.dt, ms_per_step)
 
@@ -402,8 +458,9 @@ def run_b200(args):
     sasa_k = 0 if args.no_sasa else 3
     cut_k = 0 if not args.cutoff else (2 if args.plain_only else 1)
     launches = 6 + 2 + 3 + sasa_k + cut_k
-    cfg = workload_config(args, chain)
-    cfg["born"] = "plain OBC-II pass" if args.plain_only else "learned radii (network on tcgen05 GEMMs), plain-GB judge"
+    cfg = workload_config(args, atoms, "plain OBC-II pass" if args.plain_only
+                          else "learned radii (network on tcgen05 GEMMs), plain-GB judge")
+    cfg["system"] = system
     line = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -440,9 +497,9 @@ def run_b200(args):
         "clocks": clk,
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(chain, args.dt, args.replicas, budget_s=args.cpu_budget,
-                                          all_pairs=not args.cutoff,
-                                          sasa_scale=None if args.no_sasa else args.sasa_gamma_scale)
+        smp = cpu_sample(arrays, xyz, args.dt, budget_s=args.cpu_budget, all_pairs=not args.cutoff,
+                         sasa_scale=None if args.no_sasa else args.sasa_gamma_scale)
+        line["cpu_baseline"] = cpu_line(smp, args, args.replicas)
     if rank == 0:
         print(json.dumps(line))
     eng.close()
@@ -470,6 +527,10 @@ def main():
     ap.add_argument("--train-stride", type=int, default=50)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--sasa-gamma-scale", type=float, default=0.25)
+    ap.add_argument("--no-fixture", action="store_true",
+                    help="build and relax the system at start-up instead of reading the committed fixture")
+    ap.add_argument("--reference-budget", type=float, default=150.0,
+                    help="seconds of timed CPU steps after which the reference arm stops early")
     ap.add_argument("--no-relax", action="store_true",
                     help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")
     args = ap.parse_args()
