@@ -55,6 +55,49 @@ constexpr int kMaskCircles = 63;
 constexpr uint64_t kMaskContained = 1ull << 63;
 constexpr double kPi = 3.14159265358979323846;
 
+// Optional per-phase cycle counters of the boundary kernels (measurement
+// builds only: -DOG_SASA_PHASE_CLOCKS=1).  Lane 0 of each warp accumulates
+// clock64() differences per phase in registers and adds them to
+// g_sasa_phase when its atom is done; og_sasa_phase_clocks reads them.
+// Phases: 0 caps, 1 nested-cap cull, 2 pair counts, 3 batch set-up,
+// 4 transitions, 5 sort, 6 de-duplication, 7 exposure and arcs, 8 vertex
+// signs and links, 9 term records; sums of 10 caps, 11 live circles,
+// 12 transitions, 13 atoms.
+constexpr int kPhases = 14;
+#ifdef OG_SASA_PHASE_CLOCKS
+__device__ unsigned long long g_sasa_phase[kPhases];
+__device__ __forceinline__ long long cycles() {
+  long long v = 0;
+#ifdef __CUDA_ARCH__
+  asm volatile("mov.u64 %0, %%clock64;" : "=l"(v));
+#endif
+  return v;
+}
+struct PhaseClock {
+  unsigned long long acc[kPhases];
+  long long t;
+  __device__ PhaseClock() : t(cycles()) {
+    for (int k = 0; k < kPhases; ++k) acc[k] = 0;
+  }
+  __device__ __forceinline__ void mark(int id) {
+    const long long n = cycles();
+    acc[id] += static_cast<unsigned long long>(n - t);
+    t = n;
+  }
+  __device__ __forceinline__ void count(int id, int v) { acc[id] += static_cast<unsigned long long>(v); }
+  __device__ __forceinline__ void flush(int lane) {
+    if (lane == 0)
+      for (int k = 0; k < kPhases; ++k) atomicAdd(&g_sasa_phase[k], acc[k]);
+  }
+};
+#else
+struct PhaseClock {
+  __device__ __forceinline__ void mark(int) {}
+  __device__ __forceinline__ void count(int, int) {}
+  __device__ __forceinline__ void flush(int) {}
+};
+#endif
+
 __device__ __forceinline__ D3 normalize(D3 a) { return a / norm(a); }
 
 struct Cap {
@@ -280,7 +323,7 @@ __device__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D
 // for kBounded, *n_arcs / *n_verts are the boundary sizes (possibly zero).
 template <class W>
 __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_arcs_out, int* n_verts_out,
-                              int* n_live_out) {
+                              int* n_live_out, PhaseClock& ph) {
   const int sys = a.atom_sys[i];
   const D3 pi = pos(a, i);
   const double ri = a.radius[i];
@@ -342,6 +385,8 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       n_caps += __popc(caps);
     }
   }
+  ph.mark(0);
+  ph.count(10, n_caps);
   if (__any_sync(kFull, enclosed)) return kBuried;
   if (n_caps > W::kCaps) return kInvalid;
   if (n_caps == 0) return kExposed;
@@ -382,6 +427,8 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     n_live += __popc(lvb);
   }
   __syncwarp();
+  ph.mark(1);
+  ph.count(11, n_live);
 
   // ---- boundary arcs (find_boundary), a batch of circles at a time: the
   // transitions of every circle are counted first (each ordered pair once,
@@ -441,6 +488,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     if (!masks || !__any_sync(kFull, tangent)) break;
     masks = false;
   }
+  ph.mark(2);
 
   int n_arcs = 0, n_verts = 0;
   bool bad = false;
@@ -478,6 +526,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       w.bbase[j] = 0;
     }
     __syncwarp();
+    ph.mark(3);
 
     // transitions: pairs (batch circle j, live circle m), j-major, m ascending
     // (the reference's push order), kept as unit radial directions u
@@ -622,6 +671,8 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     }
     __syncwarp();
     const int n_tr = w.sbeg[nb];
+    ph.mark(4);
+    ph.count(12, n_tr);
 
     // stable sort of each circle's transitions by angle (ties: push order),
     // summing the toggles met on the way
@@ -668,6 +719,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       break;
     }
     __syncwarp();
+    ph.mark(5);
 
     // consecutive de-duplication within each circle (|dp|^2 < 1e-12 against
     // the last kept; |dp| = sin(alpha) |du|)
@@ -708,6 +760,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       for (int j = lane; j < nb; j += 32) w.skept[j] = static_cast<uint8_t>(w.sbeg[j + 1] - w.sbeg[j]);
     }
     __syncwarp();
+    ph.mark(6);
 
     // exposure of every segment (and of every transition-free circle)
     for (int r0 = 0; r0 < n_tr; r0 += 32) {
@@ -800,6 +853,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       n_verts += __popc(exv);
     }
     __syncwarp();
+    ph.mark(7);
     b0 = b1;
   }
   if (bad) return kInvalid;
@@ -881,13 +935,20 @@ __device__ void boundary_task(const SasaArgs& a, W& w, int i, int lane, bool big
   const int sys = a.atom_sys[i];
   if (a.sys[sys].status & kStatusDiverged) return;
   int n_arcs = 0, n_verts = 0, n_live = 0;
-  const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live);
+  PhaseClock ph;
+  ph.count(13, 1);
+  const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live, ph);
   if (outcome == kInvalid) {
     overflow_atom(a, i, sys, lane, big);
+    ph.flush(lane);
     return;
   }
-  if (outcome != kBounded || n_arcs == 0) return;
+  if (outcome != kBounded || n_arcs == 0) {
+    ph.flush(lane);
+    return;
+  }
   link_boundary(w, n_arcs, n_verts, lane);
+  ph.mark(8);
   int arc_base = 0, vert_base = 0;
   if (lane == 0) {
     arc_base = atomicAdd(&a.counts[0], n_arcs);
@@ -921,6 +982,8 @@ __device__ void boundary_task(const SasaArgs& a, W& w, int i, int lane, bool big
   }
   for (int v = lane; v < n_verts; v += 32)
     a.vertex_terms[vert_base + v] = SasaVertexTerm{i, w.owner[w.v_in[v]], w.owner[w.v_out[v]], w.v_sign[v]};
+  ph.mark(9);
+  ph.flush(lane);
 }
 
 __global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
@@ -1092,7 +1155,8 @@ __device__ void areas_task(const SasaArgs& a, W& w, int i, int lane, bool big) {
   const double ri = a.radius[i];
   const double four_pi_r2 = 4.0 * kPi * ri * ri;
   int n_arcs = 0, n_verts = 0, n_live = 0;
-  const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live);
+  PhaseClock ph;  // not flushed: the counters describe the force path
+  const int outcome = build_boundary(a, w, i, lane, &n_arcs, &n_verts, &n_live, ph);
   double area = 0.0;
   if (outcome == kInvalid) {
     if (overflow_atom(a, i, sys, lane, big)) return;  // the large-capacity kernel writes its area
@@ -1254,3 +1318,17 @@ void launch_shrake_rupley(const SasaArgs& a, const double* dots, int n_dots, cud
 }
 
 }  // namespace ogk
+
+#ifdef OG_SASA_PHASE_CLOCKS
+// Reads (and with reset != 0 clears) the phase counters of a measurement
+// build; out receives kPhases values.
+extern "C" int og_sasa_phase_clocks(unsigned long long* out, int reset) {
+  if (cudaMemcpyFromSymbol(out, ogk::g_sasa_phase, sizeof(unsigned long long) * ogk::kPhases) != cudaSuccess)
+    return 5;
+  if (reset) {
+    unsigned long long zero[ogk::kPhases] = {};
+    if (cudaMemcpyToSymbol(ogk::g_sasa_phase, zero, sizeof(zero)) != cudaSuccess) return 5;
+  }
+  return 0;
+}
+#endif

@@ -78,18 +78,23 @@ def test_total_force_matches_oracle(origami, mode, build):
     assert np.isfinite(f_gpu).all()
 
 
+def bench_chain(origami):
+    """The benchmark's system: the seeded 300-residue chain (4 694 atoms, 147
+    tiles) relaxed, from tests/golden/bench_chain_300.npz, as a product chain
+    (its topology equals the fixture's, which bench.py also checks)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "bench_chain_300.npz"))
+    ch = origami.Chain.build(str(z["seq"]))
+    ch.positions = z["xyz"]
+    return ch
+
+
 @pytest.mark.parametrize("mode", ["cutoff", "all_pairs"])
 def test_total_force_on_the_bench_chain_matches_oracle(origami, mode):
-    """The benchmark's seeded 300-residue chain (4 694 atoms, 147 tiles) after
-    the bench's relaxation, jittered: every force term against the oracle at
-    the workload's own size (culled tile lists in cutoff mode, the full
-    Newton-3 sweep in all-pairs mode)."""
-    import os
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-    import bench
-    seq, ch = bench.build_workload(origami, 300, 0)
-    bench.relax(origami, ch, all_pairs=mode == "all_pairs")
+    """The bench's relaxed chain, jittered: every force term against the
+    oracle at the workload's own size (culled tile lists in cutoff mode, the
+    full Newton-3 sweep in all-pairs mode)."""
+    ch = bench_chain(origami)
     x = jitter(ch.positions, 0.02, 3)
     params = origami.Params() if mode == "cutoff" else origami.Params.all_pairs()
     f_gpu = make_engine(origami, ch, x, params).total_force(0)
@@ -98,6 +103,21 @@ def test_total_force_on_the_bench_chain_matches_oracle(origami, mode):
     err = rms_rel(f_gpu, f_ref)
     assert err < 1e-5, err
     assert np.isfinite(f_gpu).all()
+
+
+@pytest.mark.parametrize("mode", ["cutoff", "all_pairs"])
+def test_energies_on_the_bench_chain_match_oracle(origami, mode):
+    """Per-term FP64 energies of the bench's relaxed chain (4 694 atoms: 11 M
+    pair terms in the all-pairs GB and Coulomb sums) against the oracle at
+    1e-6 relative, the tolerance of the smaller systems."""
+    ch = bench_chain(origami)
+    x = jitter(ch.positions, 0.02, 4)
+    params = origami.Params() if mode == "cutoff" else origami.Params.all_pairs()
+    e = make_engine(origami, ch, x, params).energies(0)
+    nb, born = (10.0, 20.0) if mode == "cutoff" else (INF, INF)
+    ref = Orc(ch).energy_terms(x, nb, born)
+    for k in ("bond", "angle", "dihedral", "improper", "lj", "coulomb", "gb", "gb_self", "gb_pair", "total"):
+        assert abs(e[k] - ref[k]) / max(abs(ref[k]), 1.0) < 1e-6, (k, e[k], ref[k])
 
 
 def test_born_radii_match_oracle(origami):
