@@ -57,6 +57,19 @@ def seeded_sequence(n_res: int, seed: int) -> str:
     return "".join(AA_ORDER[min(int(rng.next_f64() * 20), 19)] for _ in range(n_res))
 
 
+def c3b_sequences(seed: int, n_chains: int = 256) -> list[str]:
+    """The 256-chain workload's sequences: from one xoshiro256++ stream
+    (seed), per chain a residue count uniform in [10, 80] and then its
+    residues uniform over AminoAcid::ALL."""
+    from origami_b200 import Xoshiro256pp
+    rng = Xoshiro256pp(seed)
+    out = []
+    for _ in range(n_chains):
+        n = 10 + min(int(rng.next_f64() * 71), 70)
+        out.append("".join(AA_ORDER[min(int(rng.next_f64() * 20), 19)] for _ in range(n)))
+    return out
+
+
 def fixture_arrays(args) -> dict | None:
     """The benchmark system from the committed fixture when the workload is
     the fixture's (300 residues, seed 0), else None."""
@@ -282,6 +295,8 @@ def make_engine(og, args, topo, xyz, rank: int, born_mode: int, stream):
     eng.set_stream(stream.cuda_stream)
     for r in range(args.replicas):
         eng.init_velocities(r, replica_seed(args.seed, rank, args.replicas, r), remove_com=False)
+    if not args.no_autotune:  # untimed set-up: pick the pair passes' launch variants
+        eng.tune = eng.autotune(args.tune_cache)
     return eng
 
 
@@ -381,6 +396,7 @@ def run_b200(args):
     # ---- plain GB arm
     plain = make_engine(og, args, topo, xyz, rank, 0, stream)
     plain_ms, plain_clk = timed_steps(plain, args, stream, flush, local, ws)
+    plain_tune = getattr(plain, "tune", None)
     plain.profile(True)
     plain.step(5)
     prof = plain.profile_read()
@@ -495,6 +511,7 @@ def run_b200(args):
                 "path": "og_set_state (page-locked host state in) + og_step(1) + og_get_state (state out) per step"},
         "gpu_launches": args.steps * launches,
         "clocks": clk,
+        "autotune": {"plain": plain_tune, "headline": getattr(eng, "tune", None)},
     }
     if rank == 0 and ws == 1 and not args.no_cpu:
         smp = cpu_sample(arrays, xyz, args.dt, budget_s=args.cpu_budget, all_pairs=not args.cutoff,
@@ -505,6 +522,108 @@ def run_b200(args):
     eng.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def _timed_region(stream, fn):
+    """Device time (CUDA events on `stream`) of fn(), with clocks sampled."""
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+    return a.elapsed_time(b), clk.summary, out
+
+
+def run_c3b(args):
+    """256 independent chains, residue counts U[10, 80] (seeded), 310 K, GB
+    only, all pairs, dt 2 fs + SHAKE: aggregate ns/day of the batch in one
+    engine (one launch per pass over every chain) after autotuning."""
+    import torch
+    import origami_b200 as og
+    stream = torch.cuda.current_stream()
+    seqs = c3b_sequences(args.seed)
+    chains = [og.Chain.build(q) for q in seqs]
+    # untimed set-up: every extended build relaxed at once (L-BFGS over the
+    # batch), then a short overdamped settle
+    from origami_b200.minimize import MinimizeOptions, minimize_all
+    pre = og.Engine(og.Params.all_pairs(dt_fs=0.5, friction_ps_inv=50.0, seed=9))
+    for c in chains:
+        pre.add_system(c, c.positions, 100.0)
+    pre.finalize()
+    minimize_all(pre, MinimizeOptions(max_steps=400, gradient_tol=5.0))
+    pre.step(200)
+    xs = [pre.positions(k) for k in range(len(chains))]
+    pre.close()
+    eng = og.Engine(og.Params.all_pairs(dt_fs=2.0, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 1))
+    for c, x in zip(chains, xs):
+        eng.add_system(c, x, 310.0)
+    eng.finalize()
+    eng.set_stream(stream.cuda_stream)
+    for k in range(len(chains)):
+        eng.init_velocities(k, replica_seed(args.seed, 0, len(chains), k), remove_com=False)
+    tune = eng.autotune(args.tune_cache)
+    eng.step(args.warmup)
+    ms, clk, _ = _timed_region(stream, lambda: eng.step(args.steps))
+    per = ms / args.steps
+    atoms = [c.n_atoms for c in chains]
+    pairs = sum(n * (n - 1) / 2 for n in atoms)
+    line = {"metric": "aggregate ns/day (256 chains, residues U[10,80], GB, SHAKE)",
+            "value": len(chains) * args.dt * 1e-6 / (per * 1e-3) * 86400.0, "unit": "ns/day", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "256 chains, residue counts U[10,80] (xoshiro256++ seed 0), 310 K, GB only, "
+                                   "all pairs, dt 2 fs + SHAKE, one engine", "chains": len(chains),
+                       "atoms_total": sum(atoms), "atoms_min": min(atoms), "atoms_max": max(atoms),
+                       "l2": "inputs resident; timed as one region of K steps"},
+            "pair_interactions_per_s": pairs / (per * 1e-3), "autotune": tune, "clocks": clk,
+            "gpu_launches": args.steps * 11}
+    eng.close()
+    print(json.dumps(line))
+
+
+def run_c3a(args):
+    """Replica exchange: 64 replicas of a seeded 40-residue chain on a
+    geometric 280-420 K ladder, dt 2 fs + SHAKE, GB, all pairs, swap
+    attempts every 1 ps for 100 ps, the swaps decided on the device."""
+    import torch
+    import origami_b200 as og
+    from origami_b200.minimize import MinimizeOptions, minimize_chain
+    stream = torch.cuda.current_stream()
+    seq = seeded_sequence(40, args.seed)
+    ch = og.Chain.build(seq)
+    minimize_chain(ch, og.Params.all_pairs(), MinimizeOptions(max_steps=500, gradient_tol=5.0))
+    n = 64
+    temps = [280.0 * (420.0 / 280.0) ** (k / (n - 1)) for k in range(n)]
+    eng = og.Engine(og.Params.all_pairs(dt_fs=2.0, friction_ps_inv=2.0, constrain_h_bonds=True, seed=args.seed + 2))
+    for t in temps:
+        eng.add_system(ch, ch.positions, t)
+    eng.finalize()
+    eng.set_stream(stream.cuda_stream)
+    for k in range(n):
+        eng.init_velocities(k, (args.seed + k * 0xC0FFEE) & og.Xoshiro256pp.M, remove_com=False)
+    tune = eng.autotune(args.tune_cache)
+    eng.step(args.warmup)
+    steps_per_swap = int(round(1000.0 / 2.0))
+    rounds = int(round(args.c3a_ps / 1.0))
+    ms, clk, r = _timed_region(stream, lambda: eng.remd_run(rounds, steps_per_swap,
+                                                            (args.seed + 0xDEADBEEF) & og.Xoshiro256pp.M))
+    steps = rounds * steps_per_swap
+    acc = [a / t if t else 0.0 for a, t in zip(r["accepts"], r["attempts"])]
+    line = {"metric": "aggregate ns/day (REMD, 64 replicas x 40 residues, 280-420 K)",
+            "value": n * steps * 2.0 * 1e-6 / (ms * 1e-3) * 86400.0, "unit": "ns/day", "n_gpus": 1,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 replicas of a seeded 40-residue chain, geometric ladder 280-420 K, dt 2 fs + "
+                                   f"SHAKE, GB, all pairs, swap attempts every 1 ps for {rounds} ps, device swaps",
+                       "atoms": ch.n_atoms, "swap_interval_steps": steps_per_swap, "rounds": rounds},
+            "acceptance_per_pair": acc, "acceptance_mean": float(np.mean(acc)),
+            "swap_attempts": int(np.sum(r["attempts"])), "swap_accepts": int(np.sum(r["accepts"])),
+            "autotune": tune, "clocks": clk}
+    eng.close()
+    print(json.dumps(line))
 
 
 def main():
@@ -531,12 +650,21 @@ def main():
                     help="build and relax the system at start-up instead of reading the committed fixture")
     ap.add_argument("--reference-budget", type=float, default=150.0,
                     help="seconds of timed CPU steps after which the reference arm stops early")
+    ap.add_argument("--config", default="metric", choices=["metric", "c3a", "c3b"],
+                    help="metric: the headline workload; c3a: 64-replica REMD; c3b: 256 uneven chains")
+    ap.add_argument("--c3a-ps", type=float, default=100.0, help="simulated time of the c3a run per replica (ps)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default pair-pass launches")
+    ap.add_argument("--tune-cache", default=None, help="JSON file caching the autotuner's choices")
     ap.add_argument("--no-relax", action="store_true",
                     help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "c3b":
+        run_c3b(args)
+    elif args.config == "c3a":
+        run_c3a(args)
     else:
         run_b200(args)
 

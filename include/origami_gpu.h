@@ -337,6 +337,26 @@ og_status og_trajectory_close(og_trajectory* t);
  * unscaled tension, as remd.rs:529-537 potential_energy uses. */
 og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int32_t* accepted);
 
+/* Parallel tempering run on the device (remd.rs:136 run_remd's loop,
+ * :425-474 attempt_swaps): n_rounds rounds of steps_per_swap og_step steps,
+ * each followed by one swap round between neighbouring temperatures (pairs
+ * (0,1), (2,3), ... on even rounds, (1,2), ... on odd ones, counting rounds
+ * across calls).  The potential energies (bonded + LJ/RF + GB, FP64, as
+ * og_compute_energies) stay on the device; the Metropolis decision uses
+ * delta = (beta_i - beta_j)(E_i - E_j) with a uniform from a counter-based
+ * generator keyed by (seed, round, pair); an accepted exchange swaps the two
+ * systems' temperatures and rescales each one's velocities by
+ * sqrt(T_new / T_old) -- the reference's exchange of coordinates between
+ * temperatures, without moving coordinates.  The ladder is the systems'
+ * temperatures at the first call, sorted.  attempts / accepts (optional,
+ * n_systems - 1 entries) receive the cumulative counts per temperature pair,
+ * sys_of_slot (optional, n_systems) the system now at each temperature,
+ * ascending.  Systems must have equal atom counts; with include_sasa the
+ * swap energy is the Shrake-Rupley one of og_remd_swap (OG_E_UNSUPPORTED
+ * here).  A diverged system is skipped, as run_remd does. */
+og_status og_remd_run(og_engine* e, int32_t n_rounds, int32_t steps_per_swap, uint64_t seed, int64_t* attempts,
+                      int64_t* accepts, int32_t* sys_of_slot);
+
 /* Per-atom solvent-accessible area (A^2, radius vdW + 1.4 A) of system `sys`
  * at its current positions; area_out receives n_atoms doubles.
  * method 0: analytical PowerSasa (powersasa/mod.rs:55 powersasa_energy's
@@ -344,6 +364,37 @@ og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int
  * (sasa.rs:65 sasa_per_atom_with_dots; n_dots <= 0 means the reference's
  * 960).  FP64 on the device; works whether or not include_sasa is set. */
 og_status og_compute_sasa(og_engine* e, int32_t sys, int32_t method, int32_t n_dots, double* area_out);
+
+/* Launch configuration of the two O(N^2) pair passes (Born descreening,
+ * far-field force) for this engine's systems.  No counterpart in the
+ * reference: origami's replica loop (dynamics/src/remd.rs:286,
+ * replicas.par_iter_mut()) and its per-call rayon pool take this role on
+ * the CPU.  Every variant computes the same sums; shapes differ in the
+ * fixed-point rounding of partial sums only (well inside the force
+ * tolerance), and for a fixed configuration runs are bit-reproducible.
+ *   shape       0: 8 i-tiles (256 atoms) per CTA at the default occupancy
+ *               target (Born 4 CTAs/SM, force 2); 1: 4 i-tiles (128 atoms)
+ *               per CTA at twice the CTAs per SM; 2: 8 i-tiles at 3 CTAs/SM
+ *   persistent  0: one CTA per work item; 1: resident CTAs taking items from
+ *               an atomic work queue
+ *   chunk       j-tiles per work item (default 16)
+ * og_engine_autotune times every combination (3 shapes x 2 x chunks 8, 16,
+ * 32) of each pass on the engine's systems at their current positions and
+ * keeps the fastest; the choice is cached in the JSON file cache_path (NULL
+ * = no cache) under the workload's bucket (mode, total 32-atom tiles and
+ * the largest system's tiles rounded up to powers of two), so a later
+ * engine in the same bucket is configured without timing.  The next step
+ * re-evaluates the forces. */
+typedef struct og_autotune_result {
+  int32_t born_shape, born_persistent, born_chunk;
+  int32_t force_shape, force_persistent, force_chunk;
+  double born_ms, force_ms;                 /* the chosen variants' times (ms per launch) */
+  double born_ms_default, force_ms_default; /* shape 0, one CTA per item, chunk 16; -1 from cache */
+  int32_t from_cache;
+} og_autotune_result;
+og_status og_engine_autotune(og_engine* e, const char* cache_path, og_autotune_result* out);
+/* Sets one pass's launch by hand: pass 0 = Born, 1 = force. */
+og_status og_engine_set_pair_launch(og_engine* e, int32_t pass, int32_t shape, int32_t persistent, int32_t chunk);
 
 /* CUDA-event timing of the kernels the last og_step launched: fills up to
  * `cap` entries of (kernel id, milliseconds) summed over the call. */

@@ -513,8 +513,35 @@ class Engine:
         _check(lib().og_remd_swap(self._h, parity, _dptr(u), acc.ctypes.data_as(F.c_int32_p)))
         return acc[: self.n_systems - 1]
 
+    def remd_run(self, n_rounds: int, steps_per_swap: int, seed: int) -> dict:
+        """Device-side parallel tempering rounds (og_remd_run): cumulative
+        attempts / accepts per temperature pair and the system at each
+        temperature slot."""
+        n = self.n_systems
+        att = np.zeros(max(n - 1, 1), dtype=np.int64)
+        acc = np.zeros(max(n - 1, 1), dtype=np.int64)
+        slots = np.zeros(n, dtype=np.int32)
+        _check(lib().og_remd_run(self._h, n_rounds, steps_per_swap, seed & 0xFFFFFFFFFFFFFFFF,
+                                 att.ctypes.data_as(C.POINTER(C.c_int64)), acc.ctypes.data_as(C.POINTER(C.c_int64)),
+                                 slots.ctypes.data_as(F.c_int32_p)))
+        return {"attempts": att[: n - 1], "accepts": acc[: n - 1], "sys_of_slot": slots}
+
     def profile(self, on: bool = True) -> None:
         _check(lib().og_profile_enable(self._h, int(on)))
+
+    def autotune(self, cache_path: str | None = None) -> dict:
+        """Times the pair passes' launch variants on this engine's systems and
+        keeps the fastest (og_engine_autotune); the choice is cached in the
+        JSON file cache_path when given."""
+        r = F.og_autotune_result()
+        _check(lib().og_engine_autotune(self._h, None if cache_path is None else os.fsencode(cache_path),
+                                        C.byref(r)))
+        return {k: getattr(r, k) for k, _ in F.og_autotune_result._fields_}
+
+    def set_pair_launch(self, pass_: str, shape: int, persistent: bool, chunk: int = 16) -> None:
+        """Sets one pair pass's launch variant ("born" or "force") by hand."""
+        _check(lib().og_engine_set_pair_launch(self._h, {"born": 0, "force": 1}[pass_], shape, int(persistent),
+                                               chunk))
 
     def profile_read(self) -> dict:
         buf = (F.og_kernel_time * 64)()
@@ -686,12 +713,17 @@ class RemdOptions:
     seed: int = 0
     include_sasa: bool = False
     constrain_h_bonds: bool = False
+    # swap decisions on the device (og_remd_run: temperature labels exchanged,
+    # counter-based uniforms) instead of host Metropolis with origami's swap
+    # RNG stream; not with include_sasa
+    device_swaps: bool = False
 
 
 def run_remd(chain: Chain, opts: RemdOptions, callback=None, params: Params | None = None) -> dict:
     """Parallel tempering on one GPU (dynamics/src/remd.rs:136): every replica
     is a system of one engine; swaps follow origami's odd/even schedule,
-    Metropolis rule and swap-RNG seed (seed + 0xDEADBEEF)."""
+    Metropolis rule and swap-RNG seed (seed + 0xDEADBEEF), or with
+    opts.device_swaps run as device rounds (og_remd_run)."""
     temps = sorted(opts.temperatures_k)
     p = params or Params()
     p.dt_fs, p.friction_ps_inv = opts.dt_fs, opts.friction_ps_inv
@@ -706,6 +738,26 @@ def run_remd(chain: Chain, opts: RemdOptions, callback=None, params: Params | No
     steps_per_swap = max(1, round(opts.swap_interval_fs / opts.dt_fs))
     total_steps = round(opts.total_time_fs / opts.dt_fs)
     n_rounds = -(-total_steps // steps_per_swap)
+    if opts.device_swaps:
+        if callback is not None or total_steps % steps_per_swap:
+            raise ValueError("device swaps run whole rounds without a frame callback")
+        r = eng.remd_run(n_rounds, steps_per_swap, (opts.seed + 0xDEADBEEF) & Xoshiro256pp.M)
+        energies = eng.all_energies()
+        slot_of = {int(sy): k for k, sy in enumerate(r["sys_of_slot"])}
+        order = [int(sy) for sy in r["sys_of_slot"]]
+        att, acc = r["attempts"], r["accepts"]
+        return {
+            "n_replicas": len(temps), "atoms_count": chain.n_atoms,
+            "swap_attempts": att.tolist(), "swap_accepts": acc.tolist(),
+            "acceptance_ratios": [a / t if t else 0.0 for a, t in zip(acc, att)],
+            "sys_of_slot": order,
+            "per_replica": [
+                {"temperature_k": temps[k], "system": order[k],
+                 "final_kinetic_energy_kj_mol": eng.kinetic(order[k])[0],
+                 "final_potential_energy_kj_mol": energies[order[k]]["total"], **eng.stats(order[k])}
+                for k in range(len(temps))],
+            "slot_of_system": slot_of,
+        }
     swap_rng = Xoshiro256pp((opts.seed + 0xDEADBEEF) & Xoshiro256pp.M)
     n_pairs = max(len(temps) - 1, 0)
     attempts = np.zeros(n_pairs, dtype=np.int64)

@@ -59,6 +59,16 @@ class og_energies(C.Structure):
     ]
 
 
+class og_autotune_result(C.Structure):
+    _fields_ = [
+        ("born_shape", C.c_int32), ("born_persistent", C.c_int32), ("born_chunk", C.c_int32),
+        ("force_shape", C.c_int32), ("force_persistent", C.c_int32), ("force_chunk", C.c_int32),
+        ("born_ms", C.c_double), ("force_ms", C.c_double),
+        ("born_ms_default", C.c_double), ("force_ms_default", C.c_double),
+        ("from_cache", C.c_int32),
+    ]
+
+
 class og_kernel_time(C.Structure):
     _fields_ = [("name", C.c_char_p), ("ms", C.c_double), ("launches", C.c_int64)]
 
@@ -124,6 +134,10 @@ SIGNATURES = [
     ("og_remd_swap", C.c_int, [C.c_void_p, C.c_int32, c_double_p, c_int32_p]),
     ("og_compute_sasa", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, c_double_p]),
     ("og_profile_enable", C.c_int, [C.c_void_p, C.c_int32]),
+    ("og_remd_run", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_int64),
+                              C.POINTER(C.c_int64), c_int32_p]),
+    ("og_engine_autotune", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(og_autotune_result)]),
+    ("og_engine_set_pair_launch", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     ("og_profile_read", C.c_int, [C.c_void_p, C.POINTER(og_kernel_time), C.c_int32, c_int32_p]),
     ("og_measure_fp32_peak", C.c_int, [c_double_p]),
     ("og_gb_energy_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_double,

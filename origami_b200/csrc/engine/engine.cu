@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -30,7 +31,6 @@
 #include "step_kernels.cuh"
 
 namespace ogk {
-int force_warps_per_cta();
 }
 
 namespace {
@@ -195,6 +195,17 @@ struct og_engine {
   DVec<int32_t> jlist_cut_b, jlist_cut_f, seg_end_b, seg_end_f;
   int n_cut_b = 0, n_cut_f = 0;
   int n_work = 0, n_near = 0, n_work_f = 0;
+  // how the two pair passes are launched and chunked (og_engine_autotune),
+  // and the persistent launches' queue heads (Born, force)
+  ogk::PairLaunch born_launch, force_launch;
+  int chunk_b = 16, chunk_f = 16;
+  DVec<int32_t> pair_queue;
+  // device-side replica exchange (og_remd_run): temperature slots, counters
+  bool remd_ready = false;
+  uint32_t remd_round = 0;
+  DVec<int32_t> remd_slot, remd_begin, remd_count;
+  DVec<double> remd_temps, remd_total, remd_vscale;
+  DVec<long long> remd_attempts, remd_accepts;
   // bonded
   DVec<int2> bond_atoms, dih_terms;
   DVec<int4> angle_atoms, dih_atoms, imp_atoms;
@@ -324,6 +335,7 @@ struct og_engine {
     a.lj_kj12 = static_cast<float>(12.0 * ogk::kKcalToKj);
     a.gb_pref_kj = static_cast<float>((1.0 - 1.0 / ogk::kEpsWater) * ogk::kCoulomb * ogk::kKcalToKj);
     a.error_flag = error_flag.p;
+    a.queue = pair_queue.p;
     a.atom_sys = atom_sys.p;
     a.sys_nonfinite = sys_nonfinite.p;
     a.x64 = x.p; a.y64 = y.p; a.z64 = z.p; a.q64 = q.p;
@@ -513,7 +525,7 @@ struct og_engine {
           pb.jlist = jlist_cut_b.p;
           pb.seg_end = seg_end_b.p;
         }
-        ogk::launch_born_pass(pb, stream);
+        ogk::launch_born_pass(pb, born_launch, stream);
       }
       {
         Timer t(this, "born_finalize");
@@ -526,13 +538,14 @@ struct og_engine {
       pf.work = work_f.p;
       pf.n_work = n_work_f;
       pf.jlist = jlist_f.p;
+      pf.queue = pair_queue.p + 1;
       if (!no_cutoff(p.nb_cutoff) && !no_cutoff(p.gb_force_cutoff)) {
         ogk::launch_cut_lists(cut_f.p, n_cut_f, jlist_f.p, origin.p, std::max(p.nb_cutoff, p.gb_force_cutoff),
                               jlist_cut_f.p, seg_end_f.p, stream);
         pf.jlist = jlist_cut_f.p;
         pf.seg_end = seg_end_f.p;
       }
-      ogk::launch_force_pass(pf, stream);
+      ogk::launch_force_pass(pf, force_launch, stream);
     }
     {
       Timer t(this, "near_force64");
@@ -736,6 +749,48 @@ og_status set_xyz(og_engine* e, int s, DVec<double>& a, DVec<double>& b, DVec<do
   OG_CUDA(cudaMemcpyAsync(c.p + sh.atom_begin, hz.data(), sizeof(double) * n, cudaMemcpyHostToDevice, e->stream));
   OG_CUDA(cudaStreamSynchronize(e->stream));
   return OG_OK;
+}
+
+// Pair work (Newton-3 layout): i-blocks of W consecutive tiles (W from the
+// pass's launch shape) against the tiles from the block's first tile on
+// (Born pass: the block's own diagonal included) or after it (far-field
+// force pass), cut into chunks of at most `chunk` j-tiles and ordered
+// longest first; plus the i-blocks of cutoff mode's culled lists.
+og_status build_pass_list(og_engine* e, int first_offset, int W, int chunk, DVec<ogk::PairWork>* work,
+                          int* n_work, DVec<int32_t>* jlist, DVec<ogk::CutBlock>* cut, int* n_cut,
+                          DVec<int32_t>* jlist_cut, DVec<int32_t>* seg_end, cudaStream_t st) {
+  std::vector<int32_t> hj;
+  std::vector<ogk::PairWork> hw;
+  std::vector<ogk::CutBlock> hc;
+  for (const auto& s : e->sys) {
+    for (int t0 = 0; t0 < s.n_tiles; t0 += W) {
+      const int jb = static_cast<int>(hj.size());
+      for (int t = t0 + first_offset; t < s.n_tiles; ++t) hj.push_back(s.tile_begin + t);
+      const int je = static_cast<int>(hj.size());
+      hc.push_back(ogk::CutBlock{s.tile_begin + t0, std::min(W, s.n_tiles - t0), jb, je});
+      for (int j0 = jb; j0 < je; j0 += chunk)
+        hw.push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
+    }
+  }
+  std::stable_sort(hw.begin(), hw.end(), [](const ogk::PairWork& a, const ogk::PairWork& b) {
+    return (a.j_end - a.j_begin) > (b.j_end - b.j_begin);
+  });
+  *n_cut = static_cast<int>(hc.size());
+  OG_CUDA(cut->upload(hc, st));
+  OG_CUDA(jlist_cut->alloc(std::max<size_t>(hj.size(), 1)));
+  OG_CUDA(seg_end->alloc(std::max(e->n_tiles, 1)));
+  *n_work = static_cast<int>(hw.size());
+  OG_CUDA(work->upload(hw, st));
+  OG_CUDA(jlist->upload(hj, st));
+  return OG_OK;
+}
+
+og_status build_pair_lists(og_engine* e, cudaStream_t st) {
+  og_status s = build_pass_list(e, 0, ogk::pair_shape_warps(e->born_launch.shape), e->chunk_b, &e->work, &e->n_work,
+                                &e->jlist, &e->cut_b, &e->n_cut_b, &e->jlist_cut_b, &e->seg_end_b, st);
+  if (s != OG_OK) return s;
+  return build_pass_list(e, 1, ogk::pair_shape_warps(e->force_launch.shape), e->chunk_f, &e->work_f, &e->n_work_f,
+                         &e->jlist_f, &e->cut_f, &e->n_cut_f, &e->jlist_cut_f, &e->seg_end_f, st);
 }
 
 og_status finalize_impl(og_engine* e) {
@@ -943,48 +998,11 @@ og_status finalize_impl(og_engine* e) {
   }
   OG_CUDA(e->sys_state.upload(hs, st));
 
-  // ---- pair work (Newton-3 layout): i-blocks of W consecutive tiles against
-  // the tiles from the block's first tile on (Born pass: the block's own
-  // diagonal included) or after it (far-field force pass), cut into chunks of
-  // at most 16 j-tiles and ordered longest first.
+  // ---- pair work lists (build_pair_lists) and the persistent-launch queues
+  OG_CUDA(e->pair_queue.alloc(2));
   {
-    const int W = ogk::force_warps_per_cta();
-    const int chunk = 16;
-    auto build_list = [&](int first_offset, std::vector<ogk::PairWork>* hw, std::vector<int32_t>* hj,
-                          std::vector<ogk::CutBlock>* hc) {
-      for (const auto& s : e->sys) {
-        for (int t0 = 0; t0 < s.n_tiles; t0 += W) {
-          const int jb = static_cast<int>(hj->size());
-          for (int t = t0 + first_offset; t < s.n_tiles; ++t) hj->push_back(s.tile_begin + t);
-          const int je = static_cast<int>(hj->size());
-          hc->push_back(ogk::CutBlock{s.tile_begin + t0, std::min(W, s.n_tiles - t0), jb, je});
-          for (int j0 = jb; j0 < je; j0 += chunk)
-            hw->push_back(ogk::PairWork{s.tile_begin + t0, std::min(W, s.n_tiles - t0), j0, std::min(je, j0 + chunk)});
-        }
-      }
-      std::stable_sort(hw->begin(), hw->end(), [](const ogk::PairWork& a, const ogk::PairWork& b) {
-        return (a.j_end - a.j_begin) > (b.j_end - b.j_begin);
-      });
-    };
-    std::vector<int32_t> hj, hjf;
-    std::vector<ogk::PairWork> hw, hwf;
-    std::vector<ogk::CutBlock> hcb, hcf;
-    build_list(0, &hw, &hj, &hcb);
-    build_list(1, &hwf, &hjf, &hcf);
-    e->n_cut_b = static_cast<int>(hcb.size());
-    e->n_cut_f = static_cast<int>(hcf.size());
-    OG_CUDA(e->cut_b.upload(hcb, st));
-    OG_CUDA(e->cut_f.upload(hcf, st));
-    OG_CUDA(e->jlist_cut_b.alloc(hj.size()));
-    OG_CUDA(e->jlist_cut_f.alloc(hjf.size()));
-    OG_CUDA(e->seg_end_b.alloc(e->n_tiles));
-    OG_CUDA(e->seg_end_f.alloc(e->n_tiles));
-    e->n_work = static_cast<int>(hw.size());
-    OG_CUDA(e->work.upload(hw, st));
-    OG_CUDA(e->jlist.upload(hj, st));
-    e->n_work_f = static_cast<int>(hwf.size());
-    OG_CUDA(e->work_f.upload(hwf, st));
-    OG_CUDA(e->jlist_f.upload(hjf, st));
+    og_status ls = build_pair_lists(e, st);
+    if (ls != OG_OK) return ls;
   }
 
   // ---- exclusion masks (per ordered tile pair) and the FP64 CSR
@@ -1933,6 +1951,111 @@ og_status og_remd_swap(og_engine* e, int32_t parity, const double* uniforms, int
   return OG_OK;
 }
 
+namespace {
+
+// The FP64 energy kernels of og_compute_energies without its host reductions
+// (their per-atom and per-term outputs stay on the device).
+void enqueue_energy_kernels(og_engine* e, cudaStream_t stream) {
+  ogk::EnergyArgs a{};
+  a.x = e->x.p; a.y = e->y.p; a.z = e->z.p; a.q = e->q.p;
+  a.rmin = e->rmin.p; a.eps = e->eps.p; a.rmin14 = e->rmin14.p; a.eps14 = e->eps14.p;
+  a.rho_tilde = e->rho_tilde.p; a.srho = e->srho.p; a.born_r = e->born_r64.p;
+  a.atom_sys = e->atom_sys.p;
+  a.sys_begin = e->remd_begin.p;
+  a.sys_count = e->remd_count.p;
+  a.excl_row = e->excl_row.p; a.excl_col = e->excl_col.p; a.excl_kind = e->excl_kind.p;
+  a.n_atoms_padded = e->n_padded;
+  a.nb_c2 = no_cutoff(e->p.nb_cutoff) ? INFINITY : e->p.nb_cutoff * e->p.nb_cutoff;
+  a.born_c2 = no_cutoff(e->p.born_cutoff) ? INFINITY : e->p.born_cutoff * e->p.born_cutoff;
+  const double rc = e->p.nb_cutoff;
+  a.kappa = no_cutoff(rc) ? 0.0 : 1.0 / (2.0 * rc * rc * rc);
+  a.crf = no_cutoff(rc) ? 0.0 : 3.0 / (2.0 * rc);
+  a.integral = e->integral64.p;
+  a.e_lj = e->e_lj.p; a.e_coul = e->e_coul.p; a.e_gb = e->e_gb.p; a.e_self = e->e_self.p;
+  a.n_pairs = e->n_pairs.p;
+  ogk::launch_born64(a, stream);
+  ogk::launch_born_finalize(e->atoms(), e->integral64.p, e->born_r64.p, false, e->clamp_count.p, stream);
+  ogk::launch_energy64(a, stream);
+  ogk::launch_bonded_energies(e->bonded_args(), stream);
+}
+
+}  // namespace
+
+og_status og_remd_run(og_engine* e, int32_t n_rounds, int32_t steps_per_swap, uint64_t seed, int64_t* attempts,
+                      int64_t* accepts, int32_t* sys_of_slot) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  const int n = static_cast<int>(e->sys.size());
+  if (n_rounds < 0 || steps_per_swap < 1) return og_fail(OG_E_BADARG, "og_remd_run: n_rounds >= 0, steps_per_swap >= 1");
+  if (e->p.include_sasa)
+    return og_fail(OG_E_UNSUPPORTED, "og_remd_run: the surface term's swap energy (Shrake-Rupley) is og_remd_swap's");
+  for (const auto& sh : e->sys)
+    if (sh.topo.n != e->sys[0].topo.n) return og_fail(OG_E_BADARG, "replica exchange between unequal systems");
+  cudaStream_t stream = e->stream;
+  if (!e->remd_ready) {
+    std::vector<int32_t> order(n), hb(n), hc(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return e->sys[a].temperature < e->sys[b].temperature; });
+    std::vector<double> temps(n);
+    for (int k = 0; k < n; ++k) {
+      temps[k] = e->sys[order[k]].temperature;
+      hb[k] = e->sys[k].atom_begin;
+      hc[k] = e->sys[k].topo.n;
+    }
+    OG_CUDA(e->remd_slot.upload(order, stream));
+    OG_CUDA(e->remd_temps.upload(temps, stream));
+    OG_CUDA(e->remd_begin.upload(hb, stream));
+    OG_CUDA(e->remd_count.upload(hc, stream));
+    OG_CUDA(e->remd_total.alloc(n));
+    OG_CUDA(e->remd_vscale.alloc(n));
+    OG_CUDA(e->remd_attempts.alloc(std::max(n - 1, 1)));
+    OG_CUDA(e->remd_accepts.alloc(std::max(n - 1, 1)));
+    OG_CUDA(cudaMemsetAsync(e->remd_attempts.p, 0, sizeof(long long) * std::max(n - 1, 1), stream));
+    OG_CUDA(cudaMemsetAsync(e->remd_accepts.p, 0, sizeof(long long) * std::max(n - 1, 1), stream));
+    e->remd_ready = true;
+    e->remd_round = 0;
+  }
+  ogk::RemdArgs r{};
+  r.sys = e->sys_state.p;
+  r.sys_of_slot = e->remd_slot.p;
+  r.temps = e->remd_temps.p;
+  r.total = e->remd_total.p;
+  r.vscale = e->remd_vscale.p;
+  r.attempts = e->remd_attempts.p;
+  r.accepts = e->remd_accepts.p;
+  r.e_lj = e->e_lj.p; r.e_coul = e->e_coul.p; r.e_gb = e->e_gb.p; r.e_self = e->e_self.p;
+  r.bonded_e = e->bonded_e.p;
+  r.seg_begin = e->seg_begin.p;
+  r.seg_end = e->seg_end.p;
+  r.n_slots = n;
+  r.seed = seed;
+  for (int round = 0; round < n_rounds; ++round) {
+    if ((st = og_step(e, steps_per_swap)) != OG_OK && st != OG_E_NONFINITE) return st;
+    enqueue_energy_kernels(e, stream);
+    ogk::launch_remd_round(e->atoms(), r, static_cast<int>(e->remd_round & 1u), e->remd_round, stream);
+    e->remd_round += 1;
+    if ((st = launch_check("replica exchange")) != OG_OK) return st;
+  }
+  std::vector<long long> ha(std::max(n - 1, 1)), hac(std::max(n - 1, 1));
+  OG_CUDA(cudaMemcpyAsync(ha.data(), e->remd_attempts.p, sizeof(long long) * ha.size(), cudaMemcpyDeviceToHost,
+                          stream));
+  OG_CUDA(cudaMemcpyAsync(hac.data(), e->remd_accepts.p, sizeof(long long) * hac.size(), cudaMemcpyDeviceToHost,
+                          stream));
+  std::vector<int32_t> slots(n);
+  OG_CUDA(cudaMemcpyAsync(slots.data(), e->remd_slot.p, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream));
+  std::vector<ogk::SysState> hs;
+  if ((st = read_status(e, &hs)) != OG_OK) return st;  // synchronises
+  for (int k = 0; k < n; ++k) e->sys[k].temperature = hs[k].temperature;
+  for (int k = 0; k + 1 < n; ++k) {
+    if (attempts) attempts[k] = ha[k];
+    if (accepts) accepts[k] = hac[k];
+  }
+  if (sys_of_slot)
+    for (int k = 0; k < n; ++k) sys_of_slot[k] = slots[k];
+  return OG_OK;
+}
+
 og_status og_compute_sasa(og_engine* e, int32_t s, int32_t method, int32_t n_dots, double* area_out) {
   og_status st = check_sys(e, s);
   if (st != OG_OK) return st;
@@ -2029,6 +2152,233 @@ og_status og_lgb_samples(og_engine* e, int32_t s, float* x_out, float* target_ou
     for (int a = 0; a < sh.topo.n; ++a)
       target_out[row + a] = static_cast<float>(std::log(rp[sh.atom_begin + a] / rc[sh.atom_begin + a]));
     row += sh.topo.n;
+  }
+  return OG_OK;
+}
+
+// ------------------------------------------------------------ autotuner
+// Launch variants of the two pair passes, timed on the engine's own systems:
+// CTA shape (i-tiles per CTA and the occupancy target), one CTA per work item
+// or a persistent grid on a work queue, and the j-tile chunk of a work item.
+// The best of each pass is kept in a JSON cache keyed by the workload's
+// bucket (mode, total tiles and largest system's tiles rounded up to a power
+// of two), so an engine with a cached bucket is configured without timing.
+
+namespace {
+
+int pow2_bucket(int x) {
+  int b = 1;
+  while (b < x) b <<= 1;
+  return b;
+}
+
+std::string tune_key(const og_engine* e) {
+  int max_tiles = 0;
+  for (const auto& s : e->sys) max_tiles = std::max(max_tiles, s.n_tiles);
+  const bool all_pairs = no_cutoff(e->p.nb_cutoff) && no_cutoff(e->p.gb_force_cutoff) && no_cutoff(e->p.born_cutoff);
+  return std::string(all_pairs ? "all_pairs" : "cutoff") + "|tiles<=" + std::to_string(pow2_bucket(e->n_tiles)) +
+         "|system_tiles<=" + std::to_string(pow2_bucket(max_tiles));
+}
+
+struct TuneEntry {
+  int b[3], f[3];
+  double born_ms, force_ms;
+};
+
+std::map<std::string, TuneEntry> read_tune_cache(const char* path) {
+  std::map<std::string, TuneEntry> out;
+  if (!path || !*path) return out;
+  FILE* fh = std::fopen(path, "r");
+  if (!fh) return out;
+  char line[512], key[256];
+  while (std::fgets(line, sizeof(line), fh)) {
+    TuneEntry t{};
+    if (std::sscanf(line, " \"%255[^\"]\": {\"born\": [%d, %d, %d], \"force\": [%d, %d, %d], \"born_ms\": %lf, "
+                          "\"force_ms\": %lf}",
+                    key, &t.b[0], &t.b[1], &t.b[2], &t.f[0], &t.f[1], &t.f[2], &t.born_ms, &t.force_ms) == 9)
+      out[key] = t;
+  }
+  std::fclose(fh);
+  return out;
+}
+
+bool write_tune_cache(const char* path, const std::map<std::string, TuneEntry>& m) {
+  if (!path || !*path) return true;
+  const std::string tmp = std::string(path) + ".tmp";
+  FILE* fh = std::fopen(tmp.c_str(), "w");
+  if (!fh) return false;
+  std::fprintf(fh, "{\n");
+  size_t k = 0;
+  for (const auto& kv : m) {
+    const TuneEntry& t = kv.second;
+    std::fprintf(fh, " \"%s\": {\"born\": [%d, %d, %d], \"force\": [%d, %d, %d], \"born_ms\": %.6f, \"force_ms\": %.6f}%s\n",
+                 kv.first.c_str(), t.b[0], t.b[1], t.b[2], t.f[0], t.f[1], t.f[2], t.born_ms, t.force_ms,
+                 ++k < m.size() ? "," : "");
+  }
+  std::fprintf(fh, "}\n");
+  const bool ok = std::fclose(fh) == 0;
+  return ok && std::rename(tmp.c_str(), path) == 0;
+}
+
+// Median-free best of `reps` timed launches (after one untimed) of one pass
+// variant, with the culled lists rebuilt in each launch in cutoff mode.
+og_status time_pass(og_engine* e, bool born, const ogk::PairLaunch& lc, int chunk, int reps, double* best_ms) {
+  cudaStream_t st = e->stream;
+  DVec<ogk::PairWork> work;
+  DVec<int32_t> jl, jl_cut, seg;
+  DVec<ogk::CutBlock> cut;
+  int n_work = 0, n_cut = 0;
+  og_status s = build_pass_list(e, born ? 0 : 1, ogk::pair_shape_warps(lc.shape), chunk, &work, &n_work, &jl, &cut,
+                                &n_cut, &jl_cut, &seg, st);
+  if (s != OG_OK) return s;
+  ogk::PairArgs a = e->pair_args();
+  a.work = work.p;
+  a.n_work = n_work;
+  a.jlist = jl.p;
+  a.queue = e->pair_queue.p + (born ? 0 : 1);
+  const double cutoff = born ? e->p.born_cutoff : std::max(e->p.nb_cutoff, e->p.gb_force_cutoff);
+  const bool culled = born ? !no_cutoff(e->p.born_cutoff) : (!no_cutoff(e->p.nb_cutoff) && !no_cutoff(e->p.gb_force_cutoff));
+  if (culled) {
+    a.jlist = jl_cut.p;
+    a.seg_end = seg.p;
+  }
+  cudaEvent_t t0, t1;
+  OG_CUDA(cudaEventCreate(&t0));
+  OG_CUDA(cudaEventCreate(&t1));
+  double best = 1e30;
+  for (int r = 0; r <= reps; ++r) {
+    cudaEventRecord(t0, st);
+    if (culled) ogk::launch_cut_lists(cut.p, n_cut, jl.p, e->origin.p, cutoff, jl_cut.p, seg.p, st);
+    if (born)
+      ogk::launch_born_pass(a, lc, st);
+    else
+      ogk::launch_force_pass(a, lc, st);
+    cudaEventRecord(t1, st);
+    cudaError_t err = cudaEventSynchronize(t1);
+    if (err != cudaSuccess) {
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      return cuda_fail(err, "autotune");
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    if (r > 0) best = std::min(best, static_cast<double>(ms));
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  og_status ls = launch_check("autotune");
+  if (ls != OG_OK) return ls;
+  *best_ms = best;
+  return OG_OK;
+}
+
+og_status apply_launch(og_engine* e, const TuneEntry& t) {
+  e->born_launch.shape = t.b[0];
+  e->born_launch.persistent = t.b[1] != 0;
+  e->chunk_b = t.b[2];
+  e->force_launch.shape = t.f[0];
+  e->force_launch.persistent = t.f[1] != 0;
+  e->chunk_f = t.f[2];
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  og_status s = build_pair_lists(e, e->stream);
+  if (s != OG_OK) return s;
+  reset_graph(e);
+  e->forces_valid = false;
+  OG_CUDA(cudaStreamSynchronize(e->stream));
+  return OG_OK;
+}
+
+bool valid_launch(int shape, int persistent, int chunk) {
+  return shape >= 0 && shape <= 2 && (persistent == 0 || persistent == 1) && chunk >= 1 && chunk <= 4096;
+}
+
+}  // namespace
+
+og_status og_engine_set_pair_launch(og_engine* e, int32_t pass, int32_t shape, int32_t persistent, int32_t chunk) {
+  og_status s = check_ready(e);
+  if (s != OG_OK) return s;
+  if ((pass != 0 && pass != 1) || !valid_launch(shape, persistent, chunk))
+    return og_fail(OG_E_BADARG, "og_engine_set_pair_launch: pass 0/1, shape 0..2, persistent 0/1, chunk >= 1");
+  TuneEntry t{{e->born_launch.shape, e->born_launch.persistent ? 1 : 0, e->chunk_b},
+              {e->force_launch.shape, e->force_launch.persistent ? 1 : 0, e->chunk_f}, 0.0, 0.0};
+  int* dst = pass == 0 ? t.b : t.f;
+  dst[0] = shape;
+  dst[1] = persistent;
+  dst[2] = chunk;
+  return apply_launch(e, t);
+}
+
+og_status og_engine_autotune(og_engine* e, const char* cache_path, og_autotune_result* out) {
+  og_status s = check_ready(e);
+  if (s != OG_OK) return s;
+  const std::string key = tune_key(e);
+  std::map<std::string, TuneEntry> cache = read_tune_cache(cache_path);
+  TuneEntry best{};
+  bool from_cache = false;
+  double b_def = -1.0, f_def = -1.0;
+  auto it = cache.find(key);
+  if (it != cache.end() && valid_launch(it->second.b[0], it->second.b[1], it->second.b[2]) &&
+      valid_launch(it->second.f[0], it->second.f[1], it->second.f[2])) {
+    best = it->second;
+    from_cache = true;
+  } else {
+    // Born radii at the current positions, so the force pass runs on real
+    // data (the timed launches only add into accumulators that the next
+    // force evaluation zeroes)
+    ogk::launch_pack(e->atoms(), true, e->stream);
+    ogk::PairArgs pb = e->pair_args();
+    if (!no_cutoff(e->p.born_cutoff)) {
+      ogk::launch_cut_lists(e->cut_b.p, e->n_cut_b, e->jlist.p, e->origin.p, e->p.born_cutoff, e->jlist_cut_b.p,
+                            e->seg_end_b.p, e->stream);
+      pb.jlist = e->jlist_cut_b.p;
+      pb.seg_end = e->seg_end_b.p;
+    }
+    ogk::launch_born_pass(pb, e->born_launch, e->stream);
+    ogk::launch_born_finalize(e->atoms(), nullptr, e->born_r.p, true, nullptr, e->stream);
+    OG_CUDA(cudaStreamSynchronize(e->stream));
+    const int chunks[3] = {8, 16, 32};
+    for (int pass = 0; pass < 2; ++pass) {
+      double bt = 1e30;
+      int bc[3] = {0, 0, 16};
+      for (int shape = 0; shape <= 2; ++shape)
+        for (int pers = 0; pers <= 1; ++pers)
+          for (int chunk : chunks) {
+            double ms = 0.0;
+            ogk::PairLaunch lc;
+            lc.shape = shape;
+            lc.persistent = pers != 0;
+            s = time_pass(e, pass == 0, lc, chunk, 3, &ms);
+            if (s != OG_OK) return s;
+            if (shape == 0 && pers == 0 && chunk == 16) (pass == 0 ? b_def : f_def) = ms;
+            if (ms < bt) {
+              bt = ms;
+              bc[0] = shape;
+              bc[1] = pers;
+              bc[2] = chunk;
+            }
+          }
+      int* dst = pass == 0 ? best.b : best.f;
+      std::memcpy(dst, bc, sizeof(bc));
+      (pass == 0 ? best.born_ms : best.force_ms) = bt;
+    }
+    cache[key] = best;
+    if (!write_tune_cache(cache_path, cache)) return og_fail(OG_E_IO, std::string("cannot write ") + cache_path);
+  }
+  OG_CUDA(cudaMemsetAsync(e->sys_nonfinite.p, 0, sizeof(int32_t) * e->sys.size(), e->stream));
+  s = apply_launch(e, best);
+  if (s != OG_OK) return s;
+  if (out) {
+    out->born_shape = best.b[0];
+    out->born_persistent = best.b[1];
+    out->born_chunk = best.b[2];
+    out->force_shape = best.f[0];
+    out->force_persistent = best.f[1];
+    out->force_chunk = best.f[2];
+    out->born_ms = best.born_ms;
+    out->force_ms = best.force_ms;
+    out->born_ms_default = b_def;
+    out->force_ms_default = f_def;
+    out->from_cache = from_cache ? 1 : 0;
   }
   return OG_OK;
 }

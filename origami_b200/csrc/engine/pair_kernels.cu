@@ -9,8 +9,9 @@
 //                  near-field tiles (exclusions, 1-4 pairs) go to the FP64
 //                  kernel in pair_fp64.cu.
 //
-// Layout.  One warp owns one 32-atom i-tile and a CTA of kWarps warps owns
-// kWarps consecutive tiles.  The CTA walks a list of j-tiles (the tiles from
+// Layout.  One warp owns one 32-atom i-tile and a CTA of W warps owns W
+// consecutive tiles (W = 8 or 4, a launch variant).  The CTA walks a list of
+// j-tiles (the tiles from
 // its first tile on -- each unordered tile pair once); thread 0 streams them
 // into shared memory with 1-D TMA bulk copies (two stages in flight, mbarrier
 // completion, bounded waits).  The per-atom FP32 arrays are tile-SoA (four
@@ -23,9 +24,16 @@
 // accumulators; the i side accumulates FP32 per tile and FP64 across tiles.
 // Every sum therefore has a fixed order and results are bit-reproducible.
 //
+// Launch variants (PairConfig): W, the CTAs per SM the register budget is
+// sized for, and either one CTA per work item (the hardware assigns CTAs to
+// SMs as they free up) or a persistent grid of resident CTAs that take items
+// from an atomic queue.  The engine's autotuner times them on the actual
+// systems; every variant computes the same sums in the same order.
+//
 // Positions are FP32 offsets from a per-tile FP64 origin; the origin
 // difference of a tile pair is formed in FP64 once per tile, so |dx| keeps
 // ~1e-7 relative accuracy in chains 1000 A long.
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -35,19 +43,10 @@ namespace ogk {
 
 namespace {
 
-// Tuning knobs (compile-time): CTAs per SM the register budget is sized for
-// and groups of four j atoms in flight per lane.  Defaults are the measured
-// best on B200 for 64 x 4.7k-atom systems (Born pass 1.29 ms at 4 CTAs/SM vs
-// 1.68 ms at 2; force pass 1.34 ms at 2 CTAs/SM vs 1.38 ms at 3, 80
-// registers, and 1.43 ms at 4).
-#ifndef OG_BORN_MIN_BLOCKS
-#define OG_BORN_MIN_BLOCKS 4
-#endif
+// Groups of four j atoms in flight per lane (measured best on B200 for
+// 64 x 4.7k-atom systems).
 #ifndef OG_BORN_UNROLL
 #define OG_BORN_UNROLL 1
-#endif
-#ifndef OG_FORCE_MIN_BLOCKS
-#define OG_FORCE_MIN_BLOCKS 2
 #endif
 #ifndef OG_FORCE_UNROLL
 #define OG_FORCE_UNROLL 2
@@ -55,7 +54,6 @@ namespace {
 #define OG_PRAGMA(x) _Pragma(#x)
 #define OG_UNROLL(n) OG_PRAGMA(unroll n)
 
-constexpr int kWarps = 8;         // i-tiles per CTA
 constexpr int kStageTiles = 4;    // j-tiles per pipeline stage
 constexpr int kStageFloats = kStageTiles * 128;
 constexpr uint32_t kTileBytes = 128 * sizeof(float);
@@ -87,13 +85,17 @@ __device__ __forceinline__ float reduce_scatter4(float v0, float v1, float v2, f
 }
 
 // ------------------------------------------------------------- staging
+// Stage s of a work item is the CTA's stage g0 + s overall: buffer and
+// mbarrier (g0 + s) & 1, wait parity ((g0 + s) >> 1) & 1, so a persistent
+// CTA keeps alternating its two barriers across items.
 struct Stager {
   const int32_t* jlist;
   int j_begin, j_end, n_stages;
   uint64_t* bar;
+  uint32_t g0;
   template <int kArrays>
   __device__ __forceinline__ void issue(int s, float (*buf)[kArrays][kStageFloats], const float* const* src) const {
-    const int b = s & 1;
+    const int b = (g0 + s) & 1;
     const int t0 = j_begin + s * kStageTiles;
     const int cnt = min(kStageTiles, j_end - t0);
     mbar_arrive_expect_tx(&bar[b], static_cast<uint32_t>(cnt) * kTileBytes * kArrays);
@@ -107,7 +109,7 @@ struct Stager {
 
 // Adds the stage's j partials (s_part[w][c][q], summed over warps in a fixed
 // order) to the fixed-point accumulators.
-template <int kComps>
+template <int W, int kComps>
 __device__ __forceinline__ void flush_j(const PairArgs& a, const int32_t* jlist, int t0, int cnt,
                                         float (*s_part)[kComps][kStageTiles * kTile], unsigned long long* const* dst,
                                         double scale) {
@@ -120,7 +122,7 @@ __device__ __forceinline__ void flush_j(const PairArgs& a, const int32_t* jlist,
     for (int c = 0; c < kComps; ++c) {
       float sum = 0.0f;
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) sum += s_part[w][c][q];
+      for (int w = 0; w < W; ++w) sum += s_part[w][c][q];
       v[c] = sum;
       any = any || sum != 0.0f;
       finite = finite && isfinite(sum);
@@ -192,23 +194,38 @@ __device__ __forceinline__ float2 born_pair(float dx, float dy, float dz, float 
   return on ? h : make_float2(0.0f, 0.0f);
 }
 
-__global__ void __launch_bounds__(kWarps * 32, OG_BORN_MIN_BLOCKS) k_born(PairArgs a) {
+// The next work item of a CTA: its own (one CTA per item) or the queue's.
+template <bool kPersistent>
+__device__ __forceinline__ int next_item(const PairArgs& a, int* s_item, int prev) {
+  if (!kPersistent) return prev < 0 ? static_cast<int>(blockIdx.x) : a.n_work;
+  __syncthreads();  // every thread has read the previous item
+  if (threadIdx.x == 0) *s_item = atomicAdd(a.queue, 1);
+  __syncthreads();
+  return *s_item;
+}
+
+template <int W, int kMinBlocks, bool kPersistent>
+__global__ void __launch_bounds__(W * 32, kMinBlocks) k_born(PairArgs a) {
   __shared__ __align__(128) float s_buf[2][2][kStageFloats];          // columns of pq, gb
-  __shared__ float s_part[kWarps][1][kStageTiles * kTile];
+  __shared__ float s_part[W][1][kStageTiles * kTile];
   __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_item;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  PairWork w = a.work[blockIdx.x];
-  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
-  if (w.j_begin >= w.j_end) return;  // chunk culled by the cutoff (block-uniform)
-  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar};
-  const float* src[2] = {a.pq, a.gb};
   if (threadIdx.x == 0) {
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  uint32_t g = 0;  // stages this CTA has consumed
+  for (int item = next_item<kPersistent>(a, &s_item, -1); item < a.n_work;
+       item = next_item<kPersistent>(a, &s_item, item)) {
+  PairWork w = a.work[item];
+  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
+  if (w.j_begin >= w.j_end) continue;  // chunk culled by the cutoff (block-uniform)
+  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar, g};
+  const float* src[2] = {a.pq, a.gb};
   if (threadIdx.x == 0) {
     if (st.n_stages > 0) st.issue<2>(0, s_buf, src);
     if (st.n_stages > 1) st.issue<2>(1, s_buf, src);
@@ -223,8 +240,9 @@ __global__ void __launch_bounds__(kWarps * 32, OG_BORN_MIN_BLOCKS) k_born(PairAr
   const float c2 = a.born_c2;
   double acc = 0.0;
   for (int s = 0; s < st.n_stages; ++s) {
-    const int b = s & 1;
-    const bool ok = mbar_wait_bounded(&s_bar[b], static_cast<uint32_t>((s >> 1) & 1));
+    const uint32_t gs = g + s;
+    const int b = gs & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[b], (gs >> 1) & 1u);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
       return;
@@ -276,11 +294,13 @@ OG_UNROLL(OG_BORN_UNROLL)
     __syncthreads();  // every warp is done with buffer b and has written its j partials
     if (threadIdx.x == 0 && s + 2 < st.n_stages) st.issue<2>(s + 2, s_buf, src);
     unsigned long long* dst[1] = {a.born_sum};
-    flush_j<1>(a, a.jlist, t0, cnt, s_part, dst, kBornScale);
+    flush_j<W, 1>(a, a.jlist, t0, cnt, s_part, dst, kBornScale);
   }
+  g += st.n_stages;
   if (active && a.atom_valid[i]) {
     if (!isfinite(acc)) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
     add_fixed(a.born_sum + i, acc, kBornScale);
+  }
   }
 }
 
@@ -333,24 +353,28 @@ __device__ __forceinline__ float2 coeff2(float2 xj, float2 yj, float2 zj, float2
   return c;
 }
 
-template <bool kAllPairs>
-__global__ void __launch_bounds__(kWarps * 32, OG_FORCE_MIN_BLOCKS) k_force(PairArgs a) {
+template <bool kAllPairs, int W, int kMinBlocks, bool kPersistent>
+__global__ void __launch_bounds__(W * 32, kMinBlocks) k_force(PairArgs a) {
   __shared__ __align__(128) float s_buf[2][3][kStageFloats];          // columns of pq, lj, gb
-  __shared__ float s_part[kWarps][3][kStageTiles * kTile];
+  __shared__ float s_part[W][3][kStageTiles * kTile];
   __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_item;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  PairWork w = a.work[blockIdx.x];
-  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
-  if (w.j_begin >= w.j_end) return;  // chunk culled by the cutoff (block-uniform)
-  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar};
-  const float* src[3] = {a.pq, a.lj, a.gb};
   if (threadIdx.x == 0) {
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  uint32_t g = 0;  // stages this CTA has consumed
+  for (int item = next_item<kPersistent>(a, &s_item, -1); item < a.n_work;
+       item = next_item<kPersistent>(a, &s_item, item)) {
+  PairWork w = a.work[item];
+  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
+  if (w.j_begin >= w.j_end) continue;  // chunk culled by the cutoff (block-uniform)
+  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar, g};
+  const float* src[3] = {a.pq, a.lj, a.gb};
   if (threadIdx.x == 0) {
     if (st.n_stages > 0) st.issue<3>(0, s_buf, src);
     if (st.n_stages > 1) st.issue<3>(1, s_buf, src);
@@ -378,8 +402,9 @@ __global__ void __launch_bounds__(kWarps * 32, OG_FORCE_MIN_BLOCKS) k_force(Pair
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
 
   for (int s = 0; s < st.n_stages; ++s) {
-    const int b = s & 1;
-    const bool ok = mbar_wait_bounded(&s_bar[b], static_cast<uint32_t>((s >> 1) & 1));
+    const uint32_t gs = g + s;
+    const int b = gs & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[b], (gs >> 1) & 1u);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
       return;
@@ -445,19 +470,20 @@ OG_UNROLL(OG_FORCE_UNROLL)
     __syncthreads();  // every warp is done with buffer b and has written its j partials
     if (threadIdx.x == 0 && s + 2 < st.n_stages) st.issue<3>(s + 2, s_buf, src);
     unsigned long long* dst[3] = {a.fx, a.fy, a.fz};
-    flush_j<3>(a, a.jlist, t0, cnt, s_part, dst, kForceScale);
+    flush_j<W, 3>(a, a.jlist, t0, cnt, s_part, dst, kForceScale);
   }
+  g += st.n_stages;
   if (active && a.atom_valid[i]) {
     if (!(isfinite(acc0) && isfinite(acc1) && isfinite(acc2))) atomicOr(a.sys_nonfinite + a.atom_sys[i], 1);
     add_fixed(a.fx + i, acc0, kForceScale);
     add_fixed(a.fy + i, acc1, kForceScale);
     add_fixed(a.fz + i, acc2, kForceScale);
   }
+  }
 }
 
 }  // namespace
 
-int force_warps_per_cta() { return kWarps; }
 
 namespace {
 
@@ -499,16 +525,81 @@ void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* j
     k_cut_lists<<<(n_blocks + 3) / 4, 128, 0, s>>>(blocks, n_blocks, jlist_all, origin, cutoff, jlist_out, seg_end);
 }
 
-void launch_born_pass(const PairArgs& a, cudaStream_t s) {
-  if (a.n_work > 0) k_born<<<a.n_work, kWarps * 32, 0, s>>>(a);
+namespace {
+
+// A persistent launch fills the SMs with resident CTAs (at most one per item).
+template <class K>
+int persistent_grid(K kernel, int threads, int n_work) {
+  static int n_sm = 0;
+  if (n_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  return std::max(1, std::min(n_work, std::max(per_sm, 1) * std::max(n_sm, 1)));
 }
 
-void launch_force_pass(const PairArgs& a, cudaStream_t s) {
+template <int W, int MB, bool P>
+void born_variant(const PairArgs& a, cudaStream_t s) {
+  auto k = k_born<W, MB, P>;
+  if (P) {
+    cudaMemsetAsync(a.queue, 0, sizeof(int32_t), s);
+    k<<<persistent_grid(k, W * 32, a.n_work), W * 32, 0, s>>>(a);
+  } else {
+    k<<<a.n_work, W * 32, 0, s>>>(a);
+  }
+}
+
+template <bool AP, int W, int MB, bool P>
+void force_variant(const PairArgs& a, cudaStream_t s) {
+  auto k = k_force<AP, W, MB, P>;
+  if (P) {
+    cudaMemsetAsync(a.queue, 0, sizeof(int32_t), s);
+    k<<<persistent_grid(k, W * 32, a.n_work), W * 32, 0, s>>>(a);
+  } else {
+    k<<<a.n_work, W * 32, 0, s>>>(a);
+  }
+}
+
+template <bool AP, bool P>
+void force_shape(const PairArgs& a, int shape, cudaStream_t s) {
+  switch (shape) {
+    case 1: force_variant<AP, 4, 4, P>(a, s); break;
+    case 2: force_variant<AP, 8, 3, P>(a, s); break;
+    default: force_variant<AP, 8, 2, P>(a, s); break;
+  }
+}
+
+}  // namespace
+
+int pair_shape_warps(int shape) { return shape == 1 ? 4 : 8; }
+
+void launch_born_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s) {
   if (a.n_work <= 0) return;
-  if (a.nb_c2 == INFINITY && a.gb_c2 == INFINITY)
-    k_force<true><<<a.n_work, kWarps * 32, 0, s>>>(a);
-  else
-    k_force<false><<<a.n_work, kWarps * 32, 0, s>>>(a);
+  if (c.persistent && !a.queue) return;
+  switch (c.shape * 2 + (c.persistent ? 1 : 0)) {
+    case 2: born_variant<4, 8, false>(a, s); break;
+    case 3: born_variant<4, 8, true>(a, s); break;
+    case 4: born_variant<8, 3, false>(a, s); break;
+    case 5: born_variant<8, 3, true>(a, s); break;
+    case 1: born_variant<8, 4, true>(a, s); break;
+    default: born_variant<8, 4, false>(a, s); break;
+  }
+}
+
+void launch_force_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s) {
+  if (a.n_work <= 0) return;
+  if (c.persistent && !a.queue) return;
+  const bool all_pairs = a.nb_c2 == INFINITY && a.gb_c2 == INFINITY;
+  if (all_pairs) {
+    if (c.persistent) force_shape<true, true>(a, c.shape, s);
+    else force_shape<true, false>(a, c.shape, s);
+  } else {
+    if (c.persistent) force_shape<false, true>(a, c.shape, s);
+    else force_shape<false, false>(a, c.shape, s);
+  }
 }
 
 }  // namespace ogk

@@ -55,6 +55,8 @@ struct PairArgs {
   float lj_kj12;     // 12 * 4.184
   float gb_pref_kj;  // (1 - 1/78.5) * 332.0637 * 4.184
   int32_t* error_flag;
+  // persistent launches: the work-queue head (zeroed before each launch)
+  int32_t* queue;
   // per-system "a force or Born sum was NaN/Inf" flags (fixed point cannot
   // carry a NaN, so it is recorded here and turned into divergence)
   const int32_t* atom_sys;
@@ -84,9 +86,21 @@ struct CutBlock {
 void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* jlist_all, const double4* origin,
                       double cutoff, int32_t* jlist_out, int32_t* seg_end, cudaStream_t s);
 
-void launch_born_pass(const PairArgs& a, cudaStream_t s);
+// How a pair pass is launched.  shape: 0 = 8 i-tiles per CTA (256 atoms)
+// at the default occupancy target (Born 4 CTAs/SM, force 2), 1 = 4 i-tiles
+// per CTA (128 atoms) at twice the CTAs, 2 = 8 i-tiles at 3 CTAs/SM;
+// persistent: resident CTAs taking items from PairArgs::queue instead of
+// one CTA per item.  The work list must be built for
+// pair_shape_warps(shape) i-tiles per item.
+struct PairLaunch {
+  int shape = 0;
+  bool persistent = false;
+};
+int pair_shape_warps(int shape);
+
+void launch_born_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s);
 // Far field (tiles without exclusion masks), FP32.
-void launch_force_pass(const PairArgs& a, cudaStream_t s);
+void launch_force_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s);
 // Near field: near[k] = (i_tile, j_tile, mask block of (i_tile, j_tile), 0)
 // for every unordered tile pair (i_tile <= j_tile) that carries masks, FP64;
 // each pair once, both atoms' forces.

@@ -428,6 +428,80 @@ __global__ void k_kinetic(AtomArrays a, const int32_t* begin, const int32_t* end
   if (threadIdx.x == 0) out[s] = 0.5 * tot / kAccel;
 }
 
+// ------------------------------------------------------ replica exchange
+// Per system the potential energy og_compute_energies reports (bonded +
+// LJ/RF + GB, kJ/mol), from the per-atom and per-term FP64 energies: each
+// term summed exactly as k_segment_sum does, then combined in the same
+// order as the host, so the total is bit-identical to og_compute_energies'.
+__global__ void k_remd_totals(const double* e_lj, const double* e_coul, const double* e_gb, const double* e_self,
+                              const double* bonded_e, const int32_t* begin, const int32_t* end, int n_sys,
+                              double* total) {
+  const int s = blockIdx.x;
+  double part[8];
+  const double* per_atom[4] = {e_lj, e_coul, e_gb, e_self};
+  for (int t = 0; t < 8; ++t) {
+    const int seg = t < 4 ? s : (t - 3) * n_sys + s;
+    const double* v = t < 4 ? per_atom[t] : bonded_e;
+    double acc = 0.0;
+    for (int k = begin[seg] + threadIdx.x; k < end[seg]; k += kRedThreads) acc += v[k];
+    part[t] = block_sum_fixed_order(acc);
+    __syncthreads();  // the next sum reuses the shared buffer
+  }
+  if (threadIdx.x == 0) {
+    const double lj = 0.5 * part[0] * kKcalToKj, coul = 0.5 * part[1] * kKcalToKj;
+    const double gb_pair = 0.5 * part[2] * kKcalToKj, gb_self = part[3] * kKcalToKj;
+    const double gb = gb_self + gb_pair;
+    total[s] = part[4] + part[5] + part[6] + part[7] + lj + coul + gb;
+  }
+}
+
+// One swap round: neighbouring temperature slots (pi, pi + 1), pi = parity,
+// parity + 2, ... (remd.rs:425-474).  Slot pi holds system sys_of_slot[pi]
+// at temperature temps[pi]; an accepted exchange swaps the two systems'
+// slots (their temperatures) and marks their velocities for rescaling by
+// sqrt(T_new / T_old).  The uniform of pair pi in round r is Philox keyed by
+// (seed, r, pi).  One thread: the pairs are few and the decisions ordered.
+__global__ void k_remd_swap(SysState* sys, int32_t* sys_of_slot, const double* temps, const double* total,
+                            int n_slots, int parity, uint64_t seed, uint32_t round, long long* attempts,
+                            long long* accepts, double* vscale) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int k = 0; k < n_slots; ++k) vscale[k] = 1.0;
+  for (int pi = parity; pi + 1 < n_slots; pi += 2) {
+    const int a = sys_of_slot[pi], b = sys_of_slot[pi + 1];
+    if ((sys[a].status | sys[b].status) & kStatusDiverged) continue;
+    attempts[pi] += 1;
+    const U4 r = philox4x32_10(U4{static_cast<uint32_t>(pi), round, 0x52454D44u, 0u}, static_cast<uint32_t>(seed),
+                               static_cast<uint32_t>(seed >> 32));
+    const double u = u32_to_open01(r.x);
+    const double ta = temps[pi], tb = temps[pi + 1];
+    const double delta = (1.0 / (kBoltzmann * ta) - 1.0 / (kBoltzmann * tb)) * (total[a] - total[b]);
+    const double p_acc = delta >= 0.0 ? 1.0 : exp(delta);
+    if (u < p_acc) {
+      accepts[pi] += 1;
+      sys_of_slot[pi] = b;
+      sys_of_slot[pi + 1] = a;
+      sys[a].temperature = tb;
+      sys[a].kbt = kBoltzmann * tb;
+      sys[b].temperature = ta;
+      sys[b].kbt = kBoltzmann * ta;
+      vscale[a] = sqrt(tb / ta);
+      vscale[b] = sqrt(ta / tb);
+    }
+  }
+}
+
+__global__ void k_remd_rescale(AtomArrays a, const double* vscale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_padded) return;
+  const int s = a.atom_sys[i];
+  if (s < 0) return;
+  const double f = vscale[s];
+  if (f == 1.0) return;
+  a.vx[i] *= f;
+  a.vy[i] *= f;
+  a.vz[i] *= f;
+}
+
 inline int blocks_for(int n, int bs) { return (n + bs - 1) / bs; }
 
 }  // namespace
@@ -499,6 +573,15 @@ void launch_segment_sum(const double* v, const int32_t* begin, const int32_t* en
 void launch_kinetic(const AtomArrays& a, const int32_t* begin, const int32_t* end, int32_t n_sys, double* out,
                     cudaStream_t s) {
   if (n_sys > 0) k_kinetic<<<n_sys, kRedThreads, 0, s>>>(a, begin, end, out);
+}
+
+void launch_remd_round(const AtomArrays& a, const RemdArgs& r, int parity, uint32_t round, cudaStream_t s) {
+  if (r.n_slots < 2) return;
+  k_remd_totals<<<r.n_slots, kRedThreads, 0, s>>>(r.e_lj, r.e_coul, r.e_gb, r.e_self, r.bonded_e, r.seg_begin,
+                                                  r.seg_end, r.n_slots, r.total);
+  k_remd_swap<<<1, 32, 0, s>>>(r.sys, r.sys_of_slot, r.temps, r.total, r.n_slots, parity, r.seed, round, r.attempts,
+                               r.accepts, r.vscale);
+  k_remd_rescale<<<blocks_for(a.n_padded, 256), 256, 0, s>>>(a, r.vscale);
 }
 
 namespace {

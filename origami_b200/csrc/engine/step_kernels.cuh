@@ -128,6 +128,25 @@ struct TunnelParams {
 void launch_tunnel(const AtomArrays& a, const TunnelParams& t, cudaStream_t s);
 
 // Kinetic energy per system: sum m v^2 / 2 / ACCEL (langevin.rs:469-475).
+// Device-side replica exchange round (og_remd_run): per-system energies
+// from the FP64 energy kernels' outputs, Metropolis on neighbouring
+// temperature slots, temperature labels exchanged, velocities rescaled.
+struct RemdArgs {
+  SysState* sys;
+  int32_t* sys_of_slot;   // n_slots: the system at each temperature slot
+  const double* temps;    // n_slots ascending temperatures
+  double* total;          // n_slots scratch: potential energy per system
+  double* vscale;         // n_slots scratch: velocity factor per system
+  long long* attempts;    // n_slots - 1 counters per slot pair
+  long long* accepts;
+  const double* e_lj; const double* e_coul; const double* e_gb; const double* e_self; const double* bonded_e;
+  const int32_t* seg_begin;  // the engine's [atoms | bonds | angles | dihedrals | impropers] segments
+  const int32_t* seg_end;
+  int32_t n_slots;
+  uint64_t seed;
+};
+void launch_remd_round(const AtomArrays& a, const RemdArgs& r, int parity, uint32_t round, cudaStream_t s);
+
 void launch_kinetic(const AtomArrays& a, const int32_t* begin, const int32_t* end, int32_t n_sys, double* out,
                     cudaStream_t s);
 

@@ -162,3 +162,35 @@ def minimize_chain(chain, params=None, opts: MinimizeOptions | None = None) -> M
     chain.positions = eng.positions(0)
     eng.close()
     return res
+
+
+class _AllSystems:
+    """Every system of an engine as one minimisation problem: the sum of the
+    systems' energies over their concatenated coordinates (the systems do
+    not interact, so its minimum is each system's minimum).  Positions and
+    forces move through the whole-engine state (og_get_state /
+    og_set_state), energies through og_compute_energies(sys = -1)."""
+
+    FIXED_SCALE = 2.0 ** 32  # fixed-point force units per kJ/mol/A
+
+    def __init__(self, engine):
+        self.e = engine
+
+    def positions(self, _):
+        return self.e.get_state(parts=("positions",))["positions"]
+
+    def set_positions(self, _, x):
+        self.e.set_state({"positions": np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)})
+
+    def energies(self, _):
+        return {"total": float(sum(e["total"] for e in self.e.all_energies()))}
+
+    def total_force(self, _):
+        self.e.total_force(0)  # evaluates every system
+        return self.e.get_state(parts=("forces_fixed",))["forces_fixed"] / self.FIXED_SCALE
+
+
+def minimize_all(engine, opts: MinimizeOptions | None = None) -> MinimizeResult:
+    """L-BFGS over every system of a finalised Engine at once, in place:
+    one force evaluation per iteration serves the whole batch."""
+    return lbfgs(_AllSystems(engine), 0, opts)
