@@ -626,6 +626,89 @@ def run_c3a(args):
     print(json.dumps(line))
 
 
+def run_c5(args):
+    """Co-translational growth: a seeded sequence (the same xoshiro256++
+    stream as the headline chain, --c5-residues long, 1000 by default: about
+    16 000 atoms) emitted one residue per 0.5 ps into a cylindrical exit
+    tunnel (radius 10 A, length 80 A, 10 kJ/mol/A^2 = 1000 kJ/mol/nm^2), each
+    slice BAOAB at 310 K, dt 2 fs + SHAKE, GB + PowerSasa (gamma scale 0.25),
+    all pairs; every append relaxed by L-BFGS as run_cotranslate does.  Plain
+    and learned Born radii on the same seed.  ns/day = simulated time over
+    the whole run's wall time (growth, minimisation and engine builds
+    included); the pair passes' FP32 rate is measured on the full-length
+    chain afterwards."""
+    import ctypes as C
+    import torch
+    import origami_b200 as og
+    from origami_b200 import lgb
+    from origami_b200.cotranslate import CotranslateTimings, CylindricalTunnel, UniformRibosome, run_cotranslate
+    seq = seeded_sequence(args.c5_residues, args.seed)
+    tunnel = CylindricalTunnel(axis_origin=(-5.0, 0.0, 0.0), axis_direction=(1.0, 0.0, 0.0), radius_a=10.0,
+                               length_a=80.0, k_confine=10.0)
+    opts = og.LangevinOptions(dt_fs=2.0, temperature_k=310.0, friction_ps_inv=2.0, save_every=0, seed=args.seed,
+                              include_sasa=True, constrain_h_bonds=True)
+    arms = {}
+    lgb_params = None
+    if not args.plain_only:
+        stream = torch.cuda.current_stream()
+        lgb_params, train_info = train_network(og, args, stream)
+    for born in ("plain", "learned"):
+        if born == "learned" and lgb_params is None:
+            continue
+        p = og.Params.all_pairs(sasa_gamma_scale=0.25, born_mode=1 if born == "learned" else 0)
+        t = CotranslateTimings()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        chain = run_cotranslate(UniformRibosome(seq, 500.0), opts, 0, tunnel, params=p, lgb_params=lgb_params,
+                                judge_interval=250 if born == "learned" else 0, timings=t)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        sim_ns = t.steps * opts.dt_fs * 1e-6
+        arms[born] = {"ns_per_day": sim_ns / wall * 86400.0, "wall_s": wall, "simulated_ns": sim_ns,
+                      "steps": t.steps, "slices": t.slices, "final_atoms": chain.n_atoms,
+                      "ns_per_day_dynamics_only": sim_ns / max(t.steps_s, 1e-9) * 86400.0,
+                      "seconds": {"dynamics": t.steps_s, "minimisation": t.minimize_s, "engine_builds": t.build_s}}
+    # the pair passes on the full-length chain
+    n = chain.n_atoms
+    eng = og.Engine(og.Params.all_pairs(dt_fs=2.0, constrain_h_bonds=True, include_sasa=True,
+                                        sasa_gamma_scale=0.25))
+    eng.add_system(chain, chain.positions, 310.0)
+    eng.finalize()
+    tune = eng.autotune(args.tune_cache)
+    eng.init_velocities(0, 1, remove_com=False)
+    eng.step(5)
+    eng.profile(True)
+    eng.step(10)
+    prof = eng.profile_read()
+    eng.close()
+    tf = C.c_double()
+    og._check(og.lib().og_measure_fp32_peak(C.byref(tf)))
+    pairs = n * (n - 1) / 2
+    force_ms = prof["force_pass"][0] / prof["force_pass"][1]
+    born_ms = prof["born_pass"][0] / prof["born_pass"][1]
+    head = arms.get("learned", arms["plain"])
+    line = {"metric": "ns/day (cotranslation, 1000 residues into an exit tunnel, GB+SASA)",
+            "value": head["ns_per_day"], "unit": "ns/day", "n_gpus": 1, "steps": head["steps"], "warmup": 0,
+            "ms_per_step": head["wall_s"] / max(head["steps"], 1) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.c5_residues}-residue seeded chain emitted one residue per 0.5 ps into a "
+                                   "tunnel (R 10 A, L 80 A, k 10 kJ/mol/A^2), BAOAB 310 K, dt 2 fs + SHAKE, GB + "
+                                   "PowerSasa 0.25, all pairs, L-BFGS after every append",
+                       "residues": args.c5_residues, "final_atoms": n},
+            "arms": arms,
+            "learned_vs_plain": (arms["learned"]["ns_per_day"] / arms["plain"]["ns_per_day"]) if "learned" in arms
+            else None,
+            "full_length_pair_passes": {"atoms": n, "pairs": pairs, "force_ms": force_ms, "born_ms": born_ms,
+                                        "force_tflops": 55 * pairs / (force_ms * 1e-3) / 1e12,
+                                        "born_tflops": 60 * pairs / (born_ms * 1e-3) / 1e12,
+                                        "fp32_peak_tflops": tf.value,
+                                        "force_frac": 55 * pairs / (force_ms * 1e-3) / 1e12 / tf.value,
+                                        "born_frac": 60 * pairs / (born_ms * 1e-3) / 1e12 / tf.value,
+                                        "kernels_ms_per_step": {k: v[0] / v[1] for k, v in prof.items()},
+                                        "autotune": tune}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -642,7 +725,8 @@ def main():
     ap.add_argument("--no-sasa", action="store_true", help="leave out the PowerSasa surface term")
     ap.add_argument("--plain-only", action="store_true", help="time the plain-GB engine only (no network)")
     ap.add_argument("--judge-interval", type=int, default=500)
-    ap.add_argument("--train-frames", type=int, default=16)
+    # 32 frames x 64 replicas x 997 atoms = 2.04 M (descriptor, radius) samples
+    ap.add_argument("--train-frames", type=int, default=32)
     ap.add_argument("--train-stride", type=int, default=50)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--sasa-gamma-scale", type=float, default=0.25)
@@ -650,8 +734,10 @@ def main():
                     help="build and relax the system at start-up instead of reading the committed fixture")
     ap.add_argument("--reference-budget", type=float, default=150.0,
                     help="seconds of timed CPU steps after which the reference arm stops early")
-    ap.add_argument("--config", default="metric", choices=["metric", "c3a", "c3b"],
-                    help="metric: the headline workload; c3a: 64-replica REMD; c3b: 256 uneven chains")
+    ap.add_argument("--config", default="metric", choices=["metric", "c3a", "c3b", "c5"],
+                    help="metric: the headline workload; c3a: 64-replica REMD; c3b: 256 uneven chains; "
+                         "c5: co-translational growth")
+    ap.add_argument("--c5-residues", type=int, default=1000, help="chain length of the c5 run")
     ap.add_argument("--c3a-ps", type=float, default=100.0, help="simulated time of the c3a run per replica (ps)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default pair-pass launches")
     ap.add_argument("--tune-cache", default=None, help="JSON file caching the autotuner's choices")
@@ -665,6 +751,8 @@ def main():
         run_c3b(args)
     elif args.config == "c3a":
         run_c3a(args)
+    elif args.config == "c5":
+        run_c5(args)
     else:
         run_b200(args)
 

@@ -19,6 +19,7 @@ slice repeats another's noise.
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -94,16 +95,44 @@ def _temperature(velocities: np.ndarray, mass: np.ndarray) -> float:
     return 2.0 * ke / (dof * BOLTZMANN_KJ_PER_MOL_K) if dof > 0 else 0.0
 
 
+class CotranslateDiverged(RuntimeError):
+    """A slice diverged; residue_count and time_fs say where."""
+
+    def __init__(self, residue_count: int, time_fs: float, message: str):
+        super().__init__(f"slice after residue {residue_count} (t = {time_fs:.0f} fs) diverged: {message}")
+        self.residue_count = residue_count
+        self.time_fs = time_fs
+
+
+@dataclass
+class CotranslateTimings:
+    """Wall time of a run by part (seconds): the per-residue L-BFGS, engine
+    construction (tables, tile lists, graph), and the dynamics slices."""
+    minimize_s: float = 0.0
+    build_s: float = 0.0
+    steps_s: float = 0.0
+    steps: int = 0
+    slices: int = 0
+
+
 def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: CylindricalTunnel | None = None,
-                    callback=None, params: Params | None = None) -> Chain | None:
+                    callback=None, params: Params | None = None, lgb_params=None, judge_interval: int = 0,
+                    timings: CotranslateTimings | None = None) -> Chain | None:
     """Grows the ribosome's sequence residue by residue with dynamics in
     between (cotranslate.rs:174-313); returns the final chain (None for an
     empty sequence).  callback(CotranslateFrame) receives every save_every-th
-    step of each slice, and the emission moment of a slice with no steps."""
+    step of each slice, and the emission moment of a slice with no steps.
+    params.born_mode = 1 runs the slices with learned Born radii from
+    lgb_params (the network's parameter vector), judged by plain GB every
+    judge_interval steps; opts.constrain_h_bonds puts SHAKE on the slices
+    (the reference's run_slice has none).  `timings` collects where the wall
+    time went."""
     seq = ribosome.sequence
     if not seq:
         return None
     base = params or Params()
+    if base.born_mode == 1 and lgb_params is None:
+        raise ValueError("learned radii need the network's parameters")
     rng = Xoshiro256pp(opts.seed)
     chain: Chain | None = None
     velocities = np.zeros((0, 3))
@@ -115,8 +144,11 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
             chain = Chain.build(aa)
         else:
             chain.append(aa)
+        t0 = time.perf_counter()
         minimize_chain(chain, params=Params(nb_cutoff=base.nb_cutoff, born_cutoff=base.born_cutoff,
                                             gb_force_cutoff=base.gb_force_cutoff), opts=APPEND_MINIMIZE)
+        if timings is not None:
+            timings.minimize_s += time.perf_counter() - t0
         velocities = seed_new_atom_velocities(chain, velocities, opts.temperature_k, rng)
         target = ribosome.emission_time_fs(i + 1) if i + 1 < len(seq) else clock_fs + tail_steps * opts.dt_fs
         n_steps = int(round(max(target - clock_fs, 0.0) / opts.dt_fs))
@@ -126,35 +158,52 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
                                           _temperature(velocities, chain.topology().mass)))
             continue
         clock_fs, steps_done, velocities = _run_slice(chain, velocities, opts, n_steps, external, base, clock_fs,
-                                                      steps_done, i + 1, callback)
+                                                      steps_done, i + 1, callback, lgb_params, judge_interval,
+                                                      timings)
     return chain
 
 
 def _run_slice(chain: Chain, velocities: np.ndarray, opts: LangevinOptions, n_steps: int,
                external: CylindricalTunnel | None, base: Params, clock_fs: float, steps_done: int,
-               residue_count: int, callback):
+               residue_count: int, callback, lgb_params=None, judge_interval: int = 0,
+               timings: CotranslateTimings | None = None):
     p = Params(nb_cutoff=base.nb_cutoff, born_cutoff=base.born_cutoff, gb_force_cutoff=base.gb_force_cutoff,
-               dt_fs=opts.dt_fs, friction_ps_inv=opts.friction_ps_inv, constrain_h_bonds=False,
-               include_sasa=opts.include_sasa, sasa_gamma_scale=base.sasa_gamma_scale, seed=opts.seed)
+               dt_fs=opts.dt_fs, friction_ps_inv=opts.friction_ps_inv, constrain_h_bonds=opts.constrain_h_bonds,
+               include_sasa=opts.include_sasa, sasa_gamma_scale=base.sasa_gamma_scale, seed=opts.seed,
+               born_mode=base.born_mode)
+    t0 = time.perf_counter()
     eng = Engine(p)
     try:
         eng.add_system(chain, chain.positions, opts.temperature_k)
         eng.finalize()
         if external is not None:
             external.apply_to(eng)
+        if base.born_mode == 1:
+            from . import lgb
+            lgb.set_params(eng, lgb_params)
+            lgb.set_judge(eng, judge_interval, 1e-3)
         eng.set_state({"velocities": np.ascontiguousarray(velocities, dtype=np.float64),
                        "steps": np.array([steps_done], dtype=np.int64)})
+        t1 = time.perf_counter()
         chunk = opts.save_every if opts.save_every > 0 else n_steps
         done = 0
         while done < n_steps:
             k = min(chunk, n_steps - done)
-            eng.step(k)
+            st = eng.step(k, check=False)
+            if st != 0:
+                raise CotranslateDiverged(residue_count, clock_fs + (done + k) * opts.dt_fs,
+                                          lib().og_last_error().decode())
             done += k
             if callback and opts.save_every > 0 and done % opts.save_every == 0:
                 _, t_inst = eng.kinetic(0)
                 callback(CotranslateFrame(clock_fs + done * opts.dt_fs, residue_count, eng.positions(0), t_inst))
         chain.positions = eng.positions(0)
         velocities = eng.velocities(0)
+        if timings is not None:
+            timings.build_s += t1 - t0
+            timings.steps_s += time.perf_counter() - t1
+            timings.steps += n_steps
+            timings.slices += 1
     finally:
         eng.close()
     return clock_fs + n_steps * opts.dt_fs, steps_done + n_steps, velocities

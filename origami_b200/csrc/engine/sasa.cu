@@ -493,38 +493,43 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
   int n_arcs = 0, n_verts = 0;
   bool bad = false;
   for (int b0 = 0; b0 < n_live && !bad;) {
-    // the batch: consecutive live circles whose (padded) lists fit
-    int b1 = b0, total = 0;
-    while (b1 < n_live && b1 - b0 < kSasaBatch) {
-      const int sz = max(circle_tally(w, b1, masks) & kCountMask, 1);
-      if (total + sz > W::kTrans) break;
-      total += sz;
-      ++b1;
+    // the batch: consecutive live circles whose (padded) lists fit.  Lane j
+    // takes circle b0 + j (kSasaBatch == 32): an inclusive warp prefix of
+    // the list sizes gives every circle's first slot, and the lanes whose
+    // prefix fits the buffer form the batch (a leading run, since the prefix
+    // grows with j).  (Lane 0 alone walking the circles took twice as long.)
+    static_assert(kSasaBatch == 32, "one batch circle per lane");
+    const int cj = b0 + lane;
+    const int tally = cj < n_live ? circle_tally(w, cj, masks) : 0;
+    const int cnt_j = tally & kCountMask;
+    const int sz = cj < n_live ? max(cnt_j, 1) : 0;
+    const int zero_j = (cj < n_live && cnt_j == 0) ? 1 : 0;
+    int incl = sz, zincl = zero_j;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(kFull, incl, d), z = __shfl_up_sync(kFull, zincl, d);
+      if (lane >= d) {
+        incl += v;
+        zincl += z;
+      }
     }
-    if (b1 == b0) {
+    const int nb = __popc(__ballot_sync(kFull, cj < n_live && incl <= W::kTrans));
+    if (nb == 0) {
       bad = true;  // one circle alone has more transitions than the buffer
       break;
     }
-    const int nb = b1 - b0;
-    if (lane == 0) {
-      int s0 = 0, z = 0;
-      for (int j = 0; j < nb; ++j) {
-        const int c = circle_tally(w, b0 + j, masks) & kCountMask;
-        w.sbeg[j] = static_cast<uint16_t>(s0);
-        w.zpre[j] = static_cast<uint8_t>(z);
-        s0 += max(c, 1);
-        z += c == 0 ? 1 : 0;
-      }
-      w.sbeg[nb] = static_cast<uint16_t>(s0);
-    }
-    for (int j = lane; j < nb; j += 32) {
-      const double c = w.cc[w.live[b0 + j]];
+    const int b1 = b0 + nb;
+    if (lane < nb) {
+      w.sbeg[lane] = static_cast<uint16_t>(incl - sz);
+      w.zpre[lane] = static_cast<uint8_t>(zincl - zero_j);
+      const double c = w.cc[w.live[cj]];
       const double sk = sqrt(fmax(1.0 - c * c, 0.0));
-      w.bsk[j] = sk;
-      w.binv[j] = sk > 0.0 ? 1.0 / sk : 0.0;
-      w.bmode[j] = (circle_tally(w, b0 + j, masks) & kContained) ? 1 : 0;
-      w.bbase[j] = 0;
+      w.bsk[lane] = sk;
+      w.binv[lane] = sk > 0.0 ? 1.0 / sk : 0.0;
+      w.bmode[lane] = (tally & kContained) ? 1 : 0;
+      w.bbase[lane] = 0;
     }
+    if (lane == nb - 1) w.sbeg[nb] = static_cast<uint16_t>(incl);
     __syncwarp();
     ph.mark(3);
 
@@ -685,7 +690,9 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
         const double as = w.ta[sl];
         if (!isfinite(as)) nonfinite = true;
         // one loop over the circle (two loops split at sl, one comparison
-        // each, measured slower: the split point differs between lanes)
+        // each, measured slower: the split point differs between lanes;
+        // four entries per trip with their loads issued together measured
+        // 1.8x slower)
         for (int t = sb; t < se; ++t) {
           const double at = w.ta[t];
           const bool before = (at < as) || (at == as && t < sl);
