@@ -96,12 +96,15 @@ def _temperature(velocities: np.ndarray, mass: np.ndarray) -> float:
 
 
 class CotranslateDiverged(RuntimeError):
-    """A slice diverged; residue_count and time_fs say where."""
+    """A slice diverged; residue_count and time_fs say where, positions and
+    velocities hold the slice's starting state."""
 
-    def __init__(self, residue_count: int, time_fs: float, message: str):
+    def __init__(self, residue_count: int, time_fs: float, message: str, positions=None, velocities=None):
         super().__init__(f"slice after residue {residue_count} (t = {time_fs:.0f} fs) diverged: {message}")
         self.residue_count = residue_count
         self.time_fs = time_fs
+        self.positions = positions
+        self.velocities = velocities
 
 
 @dataclass
@@ -117,7 +120,7 @@ class CotranslateTimings:
 
 def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: CylindricalTunnel | None = None,
                     callback=None, params: Params | None = None, lgb_params=None, judge_interval: int = 0,
-                    timings: CotranslateTimings | None = None) -> Chain | None:
+                    timings: CotranslateTimings | None = None, deadline: float | None = None) -> Chain | None:
     """Grows the ribosome's sequence residue by residue with dynamics in
     between (cotranslate.rs:174-313); returns the final chain (None for an
     empty sequence).  callback(CotranslateFrame) receives every save_every-th
@@ -126,7 +129,8 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
     lgb_params (the network's parameter vector), judged by plain GB every
     judge_interval steps; opts.constrain_h_bonds puts SHAKE on the slices
     (the reference's run_slice has none).  `timings` collects where the wall
-    time went."""
+    time went; with a deadline (time.perf_counter() value) the growth stops
+    after the residue during which it passes."""
     seq = ribosome.sequence
     if not seq:
         return None
@@ -139,6 +143,8 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
     clock_fs = 0.0
     steps_done = 0
     for i, aa in enumerate(seq):
+        if deadline is not None and time.perf_counter() > deadline:
+            break
         clock_fs = max(clock_fs, ribosome.emission_time_fs(i))
         if chain is None:
             chain = Chain.build(aa)
@@ -192,7 +198,8 @@ def _run_slice(chain: Chain, velocities: np.ndarray, opts: LangevinOptions, n_st
             st = eng.step(k, check=False)
             if st != 0:
                 raise CotranslateDiverged(residue_count, clock_fs + (done + k) * opts.dt_fs,
-                                          lib().og_last_error().decode())
+                                          lib().og_last_error().decode(), chain.positions,
+                                          np.ascontiguousarray(velocities, dtype=np.float64))
             done += k
             if callback and opts.save_every > 0 and done % opts.save_every == 0:
                 _, t_inst = eng.kinetic(0)

@@ -1146,7 +1146,7 @@ og_status finalize_impl(og_engine* e) {
   OG_CUDA(e->bonded_e.alloc(std::max(1, e->n_bonds + e->n_angles + e->n_dih + e->n_imp)));
   OG_CUDA(e->seg_begin.upload(sb, st));
   OG_CUDA(e->seg_end.upload(se, st));
-  OG_CUDA(e->seg_out.alloc(5 * n_sys));
+  OG_CUDA(e->seg_out.alloc(9 * static_cast<size_t>(n_sys)));  // energy terms: 5 per-atom + 4 bonded
 
   // ---- SHAKE clusters: constraints grouped by their heavy atom, in
   // constraint order inside a cluster.
@@ -1569,20 +1569,24 @@ og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
   }
   if ((st = launch_check("energy kernels")) != OG_OK) return st;
 
-  // Deterministic per-system sums.
-  std::vector<double> sums[5];
+  // Deterministic per-system sums, all on the device, then one copy back:
+  // seg_out = [lj | coulomb | gb pair | gb self | sasa | bond | angle |
+  // dihedral | improper], n_sys each.
   const double* per_atom[5] = {e->e_lj.p, e->e_coul.p, e->e_gb.p, e->e_self.p, e->sasa_energy.p};
   const int n_terms = e->p.include_sasa ? 5 : 4;
-  for (int k = 0; k < n_terms; ++k) {
-    ogk::launch_segment_sum(per_atom[k], e->seg_begin.p, e->seg_end.p, n_sys, e->seg_out.p + 0, stream);
-    sums[k].resize(n_sys);
-    OG_CUDA(cudaMemcpyAsync(sums[k].data(), e->seg_out.p, sizeof(double) * n_sys, cudaMemcpyDeviceToHost, stream));
-    OG_CUDA(cudaStreamSynchronize(stream));
-  }
-  std::vector<double> bonded(4 * static_cast<size_t>(n_sys));
-  ogk::launch_segment_sum(e->bonded_e.p, e->seg_begin.p + n_sys, e->seg_end.p + n_sys, 4 * n_sys, e->seg_out.p,
-                          stream);
-  OG_CUDA(cudaMemcpyAsync(bonded.data(), e->seg_out.p, sizeof(double) * 4 * n_sys, cudaMemcpyDeviceToHost, stream));
+  for (int k = 0; k < n_terms; ++k)
+    ogk::launch_segment_sum(per_atom[k], e->seg_begin.p, e->seg_end.p, n_sys, e->seg_out.p + k * n_sys, stream);
+  ogk::launch_segment_sum(e->bonded_e.p, e->seg_begin.p + n_sys, e->seg_end.p + n_sys, 4 * n_sys,
+                          e->seg_out.p + 5 * n_sys, stream);
+  std::vector<double> all(9 * static_cast<size_t>(n_sys), 0.0);
+  OG_CUDA(cudaMemcpyAsync(all.data(), e->seg_out.p, sizeof(double) * (n_terms == 5 ? 9 : 4) * n_sys,
+                          cudaMemcpyDeviceToHost, stream));
+  if (n_terms < 5)
+    OG_CUDA(cudaMemcpyAsync(all.data() + 5 * n_sys, e->seg_out.p + 5 * n_sys, sizeof(double) * 4 * n_sys,
+                            cudaMemcpyDeviceToHost, stream));
+  std::vector<double> sums[5];
+  for (int k = 0; k < 5; ++k) sums[k].assign(all.begin() + k * n_sys, all.begin() + (k + 1) * n_sys);
+  std::vector<double> bonded(all.begin() + 5 * n_sys, all.end());
   // Pair counts (int) summed on the host.
   std::vector<int32_t> clamp(n_sys);
   OG_CUDA(cudaMemcpyAsync(clamp.data(), e->clamp_count.p, sizeof(int32_t) * n_sys, cudaMemcpyDeviceToHost, stream));
