@@ -493,16 +493,19 @@ def run_b200(args):
                               if args.cutoff else None),
                      "traffic": FORCE_PASS_DRAM_BYTES_PER_REPLICA * args.replicas,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_force<1> at 4 "
-                                       "replicas (profiles/pair_kernels_4x4694_extended.md), per replica x replicas",
+                                       "replicas (profiles/pair_kernels_4x4694_extended.md; the relaxed chain gives the same 1.51 MB, "
+                                       "profiles/force_pass_instruction_mix_4x4694.md), per replica x replicas",
                      "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak); the pair math is FP32 "
                                     "CUDA-core work, so neither the HBM copy nor the BF16 tensor peak bounds it",
                      "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
         "dominant_kernel": {
             "kernel": "k_sasa_boundary + k_sasa_terms (PowerSasa, FP64)",
             "ms_per_step": (prof["sasa"][0] / prof["sasa"][1]) if "sasa" in prof else None,
-            "bound": "FP64 dependency latency at 16 warps per SM (ncu: issue active 45 %, FP64 pipe 16 %, "
-                     "DRAM 0.02 %); data-dependent geometry, no flop or byte roofline",
-            "profile": "profiles/sasa_boundary_4x4694_extended.md"},
+            "bound": "dependency latency at 16 warps per SM (ncu on the relaxed chain: issue active 47 %, "
+                     "FP64 pipe 17 %, DRAM 0.03 %, 24 of 32 lanes active); data-dependent geometry, no flop "
+                     "or byte roofline",
+            "profile": "profiles/sasa_boundary_4x4694_relaxed.md",
+            "launch_list": "profiles/launch_list_64x4694_plain_step.md"},
         "sasa_share_of_step": (prof["sasa"][0] / prof["sasa"][1] / plain_ms) if "sasa" in prof else None,
         "born_pass_tflops": born_tflops,
         "pair_interactions_per_s": None if args.cutoff else pairs / (ms_per_step * 1e-3) * ws,
@@ -645,8 +648,8 @@ def run_c5(args):
     seq = seeded_sequence(args.c5_residues, args.seed)
     tunnel = CylindricalTunnel(axis_origin=(-5.0, 0.0, 0.0), axis_direction=(1.0, 0.0, 0.0), radius_a=10.0,
                                length_a=80.0, k_confine=10.0)
-    opts = og.LangevinOptions(dt_fs=2.0, temperature_k=310.0, friction_ps_inv=2.0, save_every=0, seed=args.seed,
-                              include_sasa=True, constrain_h_bonds=True)
+    opts = og.LangevinOptions(dt_fs=args.c5_dt, temperature_k=310.0, friction_ps_inv=2.0, save_every=0,
+                              seed=args.seed, include_sasa=True, constrain_h_bonds=not args.c5_no_shake)
     arms = {}
     lgb_params = None
     if not args.plain_only:
@@ -708,8 +711,9 @@ def run_c5(args):
             "ms_per_step": head["wall_s"] / max(head["steps"], 1) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{args.c5_residues}-residue seeded chain emitted one residue per 0.5 ps into a "
-                                   "tunnel (R 10 A, L 80 A, k 10 kJ/mol/A^2), BAOAB 310 K, dt 2 fs + SHAKE, GB + "
-                                   "PowerSasa 0.25, all pairs, L-BFGS after every append",
+                                   f"tunnel (R 10 A, L 80 A, k 10 kJ/mol/A^2), BAOAB 310 K, dt {args.c5_dt} fs"
+                                   f"{'' if args.c5_no_shake else ' + SHAKE'}, GB + PowerSasa 0.25, all pairs, "
+                                   "L-BFGS after every append",
                        "residues": args.c5_residues, "final_atoms": n},
             "arms": arms,
             "learned_vs_plain": (arms["learned"]["ns_per_day"] / arms["plain"]["ns_per_day"]) if "learned" in arms
@@ -755,6 +759,9 @@ def main():
                          "c5: co-translational growth")
     ap.add_argument("--c5-residues", type=int, default=1000, help="chain length of the c5 run")
     ap.add_argument("--c5-budget", type=float, default=900.0, help="wall seconds of growth per arm in the c5 run")
+    ap.add_argument("--c5-dt", type=float, default=2.0, help="time step of the c5 slices (fs)")
+    ap.add_argument("--c5-no-shake", action="store_true",
+                    help="c5 slices without SHAKE (the reference's run_slice integrator, with --c5-dt 1)")
     ap.add_argument("--c3a-ps", type=float, default=100.0, help="simulated time of the c3a run per replica (ps)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default pair-pass launches")
     ap.add_argument("--tune-cache", default=None, help="JSON file caching the autotuner's choices")
