@@ -317,15 +317,34 @@ struct IAtom2 {
   float2 nrc3;         // -1 / Rc^3
 };
 
-// Pair coefficients c (F_i = c * d) for two j atoms; d returned in dx/dy/dz.
-template <bool kAllPairs>
-__device__ __forceinline__ float2 coeff2(float2 xj, float2 yj, float2 zj, float2 qj, float2 rmj, float2 sej,
-                                         float2 Rj, float2 iRj, const IAtom2& ia, const PairArgs& a, float2& dx,
-                                         float2& dy, float2& dz) {
-  dx = add2(xj, ia.nx);
-  dy = add2(yj, ia.ny);
-  dz = add2(zj, ia.nz);
-  const float2 r2 = fma2(dx, dx, fma2(dy, dy, mul2(dz, dz)));
+// Separation d = x_j - x_i of two j atoms from the i atom, and r^2.
+struct Sep2 {
+  float2 dx, dy, dz, r2;
+};
+__device__ __forceinline__ Sep2 sep2(float2 xj, float2 yj, float2 zj, const IAtom2& ia) {
+  Sep2 s;
+  s.dx = add2(xj, ia.nx);
+  s.dy = add2(yj, ia.ny);
+  s.dz = add2(zj, ia.nz);
+  s.r2 = fma2(s.dx, s.dx, fma2(s.dy, s.dy, mul2(s.dz, s.dz)));
+  return s;
+}
+
+// Exponent of the GB kernel's exponential in base 2: -r^2 / (4 R_i R_j) log2(e).
+__device__ __forceinline__ float2 gb_arg2(const Sep2& s, float2 iRj, const IAtom2& ia) {
+  return mul2(mul2(s.r2, ia.nexp), iRj);
+}
+
+// Pair coefficients c (F_i = c * d) for two j atoms.  kFarGb: both pairs
+// have arg < -30, so e = 2^arg < 2^-30: R_i R_j e < r^2 / 83 * 2^-30 is below
+// half an ulp of r^2, so f^2 = fma(R_i R_j, e, r^2) rounds to r^2 and
+// 1 - e/4 to 1; the far form then evaluates exactly what the full form does
+// (same rsqrt input, same products), without the exponential and the
+// second reciprocal square root.
+template <bool kAllPairs, bool kFarGb>
+__device__ __forceinline__ float2 coeff2(const Sep2& s, float2 arg, float2 qj, float2 rmj, float2 sej, float2 Rj,
+                                         const IAtom2& ia, const PairArgs& a) {
+  const float2 r2 = s.r2;
   const float2 inv_r = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
   const float2 inv_r2 = mul2(inv_r, inv_r);
   const float2 rmin = add2(ia.rm, rmj);
@@ -334,12 +353,16 @@ __device__ __forceinline__ float2 coeff2(float2 xj, float2 yj, float2 zj, float2
   const float2 one_m_r6 = fma2(r6, bc(-1.0f), bc(1.0f));
   const float2 ljc = mul2(mul2(ia.se, sej), mul2(inv_r2, mul2(r6, one_m_r6)));
   const float2 coul = mul2(mul2(ia.cq, qj), fma2(inv_r2, inv_r, ia.nrc3));
-  const float2 arg = mul2(mul2(r2, ia.nexp), iRj);
-  const float2 e = make_float2(exp2f(arg.x), exp2f(arg.y));
-  const float2 f2 = fma2(mul2(ia.R, Rj), e, r2);
-  const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
-  const float2 wgt = fma2(bc(-0.25f), e, bc(1.0f));
-  const float2 gbc = mul2(mul2(ia.gq, qj), mul2(wgt, mul2(inv_f, mul2(inv_f, inv_f))));
+  float2 gbc;
+  if (kFarGb) {
+    gbc = mul2(mul2(ia.gq, qj), mul2(inv_r, mul2(inv_r, inv_r)));
+  } else {
+    const float2 e = make_float2(exp2f(arg.x), exp2f(arg.y));
+    const float2 f2 = fma2(mul2(ia.R, Rj), e, r2);
+    const float2 inv_f = make_float2(rsqrtf(f2.x), rsqrtf(f2.y));
+    const float2 wgt = fma2(bc(-0.25f), e, bc(1.0f));
+    gbc = mul2(mul2(ia.gq, qj), mul2(wgt, mul2(inv_f, mul2(inv_f, inv_f))));
+  }
   float2 c;
   if (kAllPairs) {
     c = add2(add2(ljc, coul), gbc);
@@ -442,15 +465,25 @@ OG_UNROLL(OG_FORCE_UNROLL)
         const float4 SE = *reinterpret_cast<const float4*>(&sl[32 + k0]);
         const float4 RB = *reinterpret_cast<const float4*>(&sg[k0]);
         const float4 IR = *reinterpret_cast<const float4*>(&sg[32 + k0]);
-        float2 dxa, dya, dza, dxb, dyb, dzb;
-        const float2 ca = coeff2<kAllPairs>(make_float2(X.x, X.y), make_float2(Y.x, Y.y), make_float2(Z.x, Z.y),
-                                            make_float2(Q.x, Q.y), make_float2(RM.x, RM.y), make_float2(SE.x, SE.y),
-                                            make_float2(RB.x, RB.y), make_float2(IR.x, IR.y), ia, a, dxa, dya, dza);
-        const float2 cb = coeff2<kAllPairs>(make_float2(X.z, X.w), make_float2(Y.z, Y.w), make_float2(Z.z, Z.w),
-                                            make_float2(Q.z, Q.w), make_float2(RM.z, RM.w), make_float2(SE.z, SE.w),
-                                            make_float2(RB.z, RB.w), make_float2(IR.z, IR.w), ia, a, dxb, dyb, dzb);
-        const float2 uxa = mul2(dxa, ca), uya = mul2(dya, ca), uza = mul2(dza, ca);
-        const float2 uxb = mul2(dxb, cb), uyb = mul2(dyb, cb), uzb = mul2(dzb, cb);
+        const Sep2 sa = sep2(make_float2(X.x, X.y), make_float2(Y.x, Y.y), make_float2(Z.x, Z.y), ia);
+        const Sep2 sb = sep2(make_float2(X.z, X.w), make_float2(Y.z, Y.w), make_float2(Z.z, Z.w), ia);
+        const float2 arga = gb_arg2(sa, make_float2(IR.x, IR.y), ia), argb = gb_arg2(sb, make_float2(IR.z, IR.w), ia);
+        // the far GB form when every pair of the warp's group allows it
+        const bool far = __all_sync(0xffffffffu, fmaxf(fmaxf(arga.x, arga.y), fmaxf(argb.x, argb.y)) < -30.0f);
+        float2 ca, cb;
+        if (far) {
+          ca = coeff2<kAllPairs, true>(sa, arga, make_float2(Q.x, Q.y), make_float2(RM.x, RM.y),
+                                       make_float2(SE.x, SE.y), make_float2(RB.x, RB.y), ia, a);
+          cb = coeff2<kAllPairs, true>(sb, argb, make_float2(Q.z, Q.w), make_float2(RM.z, RM.w),
+                                       make_float2(SE.z, SE.w), make_float2(RB.z, RB.w), ia, a);
+        } else {
+          ca = coeff2<kAllPairs, false>(sa, arga, make_float2(Q.x, Q.y), make_float2(RM.x, RM.y),
+                                        make_float2(SE.x, SE.y), make_float2(RB.x, RB.y), ia, a);
+          cb = coeff2<kAllPairs, false>(sb, argb, make_float2(Q.z, Q.w), make_float2(RM.z, RM.w),
+                                        make_float2(SE.z, SE.w), make_float2(RB.z, RB.w), ia, a);
+        }
+        const float2 uxa = mul2(sa.dx, ca), uya = mul2(sa.dy, ca), uza = mul2(sa.dz, ca);
+        const float2 uxb = mul2(sb.dx, cb), uyb = mul2(sb.dy, cb), uzb = mul2(sb.dz, cb);
         fx = add2(fx, add2(uxa, uxb));
         fy = add2(fy, add2(uya, uyb));
         fz = add2(fz, add2(uza, uzb));

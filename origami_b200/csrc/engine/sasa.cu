@@ -60,7 +60,8 @@ constexpr double kPi = 3.14159265358979323846;
 // clock64() differences per phase in registers and adds them to
 // g_sasa_phase when its atom is done; og_sasa_phase_clocks reads them.
 // Phases: 0 caps, 1 nested-cap cull, 2 pair counts, 3 batch set-up,
-// 4 transitions, 5 sort, 6 de-duplication, 7 exposure and arcs, 8 vertex
+// 4 transitions, 5 rank sort, 6 walk over the sorted order (ties,
+// duplicates, burial bookkeeping, toggle scan; de-duplication), 7 exposure and arcs, 8 vertex
 // signs and links, 9 term records; sums of 10 caps, 11 live circles,
 // 12 transitions, 13 atoms.
 constexpr int kPhases = 14;
@@ -139,20 +140,25 @@ __device__ __forceinline__ PairClass classify(Cap c1, Cap c2) {
 // The transition points of a pair with count 1 or 2 (q only for 2).  For
 // unit axes |a1 x a2|^2 = 1 - sigma^2 = denom, so one reciprocal square root
 // of denom gives both 1 / denom and the normalisation of a1 x a2 (equal to
-// the reference's division and norm up to rounding).
-__device__ __forceinline__ void transition_points(Cap c1, Cap c2, PairClass pc, D3* p, D3* q) {
+// the reference's division and norm up to rounding).  *rate_sk receives
+// sqrt(c_sq denom) = |(a1 x a2) . (p - base)|, the crossing rate times the
+// circle's sin(alpha) (0 for count 1).
+__device__ __forceinline__ void transition_points(Cap c1, Cap c2, PairClass pc, D3* p, D3* q, double* rate_sk) {
   const double rd = rsqrt(pc.denom);
   const double inv = rd * rd;
   const double a = (c1.c - pc.sigma * c2.c) * inv;
   const double b = (c2.c - pc.sigma * c1.c) * inv;
   const D3 base = c1.axis * a + c2.axis * b;
+  *rate_sk = 0.0;
   if (pc.count == 1) {
     *p = base;
     return;
   }
   const double c_sq = 1.0 - a * a - b * b - 2.0 * a * b * pc.sigma;
   const D3 nc = cross(c1.axis, c2.axis);
-  const D3 off = nc * (sqrt(fmax(c_sq, 0.0)) * rd);
+  const double root = sqrt(fmax(c_sq, 0.0));
+  *rate_sk = root * (pc.denom * rd);
+  const D3 off = nc * (root * rd);
   *p = base + off;
   *q = base - off;
 }
@@ -177,6 +183,46 @@ __device__ __forceinline__ double pseudo_angle(double x, double y) {
   const double r = x / d;
   return y >= 0.0 ? 1.0 - r : r - 1.0;
 }
+
+// The frame in which a circle's transitions are ordered: fu, fv span the
+// circle's plane (scale-free; only the angle matters).
+__device__ __forceinline__ void slot_frame(D3 axis, D3* fu, D3* fv) {
+  const D3 h = helper_axis(axis);
+  *fu = h - axis * dot(h, axis);
+  *fv = cross(axis, *fu);
+}
+
+// Pseudo-angle of unit radial direction u in the frame (fu, fv), in [-2, 2].
+__device__ __forceinline__ double slot_angle(D3 u, D3 fu, D3 fv) { return pseudo_angle(dot(u, fu), dot(u, fv)); }
+
+// Sort key of transition slot sl: its pseudo-angle shifted to [0, 4] and
+// quantised (quantum Q = 2^-19), the slot below it (ties of equal quanta in
+// slot order).  The quantum is taken in FP32 from the FP64 coordinates
+// (x, y) of the point in the circle's frame; converting x and y, |x| + |y|,
+// the approximate quotient (2 ulp), 1 -+ r and the shift by 2 leave the
+// shifted angle within E = 13 * 2^-24 of the FP64 pseudo-angle.  Keys whose
+// quanta differ by 2 or more are more than Q apart, so their angles differ
+// by more than Q - 2E > 0 in the same direction: they order as the FP64
+// angles do.  Neighbours in key order whose quanta differ by at most 1 are
+// found after the sort and their circle ordered again from the FP64 angles
+// (ties: slot order).  7 slot bits for buffers of up to 128 slots, else 8;
+// the quantum needs 22 bits.
+template <int kTrans>
+struct SlotKey {
+  static constexpr int kShift = kTrans <= 128 ? 7 : 8;
+  static constexpr float kScale = 524288.0f;  // 1 / Q = 2^19: 4 * 2^19 < 2^22 <= 2^(32 - kShift)
+  static __device__ __forceinline__ uint32_t pack(float shifted, int sl) {
+    const float q = fminf(fmaxf(shifted, 0.0f), 4.0f) * kScale;
+    return (__float2uint_rz(q) << kShift) | static_cast<uint32_t>(sl);
+  }
+  // the key of the point with frame coordinates (x, y)
+  static __device__ __forceinline__ uint32_t make(double x, double y, int sl) {
+    const float xf = __double2float_rn(x), yf = __double2float_rn(y);
+    const float d = fabsf(xf) + fabsf(yf);
+    const float r = d > 0.0f ? __fdividef(xf, d) : 0.0f;
+    return pack((y >= 0.0 ? 1.0f - r : r - 1.0f) + 2.0f, sl);
+  }
+};
 
 // identify_root_sign (derivatives.rs:117).
 __device__ int identify_root_sign(Cap c1, Cap c2, D3 ref) {
@@ -208,12 +254,18 @@ struct WarpSmemT {
     int32_t tcnt[kCaps];
     uint64_t xmask[kCaps / 2];
   };
-  // transitions of the batch of circles being processed: sort key, unit
-  // radial direction, the other cap, the batch circle, the sorted order
-  double ta[kTrans], tx[kTrans], ty[kTrans], tz[kTrans];
+  // transitions of the batch of circles being processed: unit radial
+  // direction, sort key (quantised angle and slot, slot_key), the other
+  // cap, the batch circle, the sorted order and each entry's rank in it
+  double tx[kTrans], ty[kTrans], tz[kTrans];
+  uint32_t tkey[kTrans];
   uint8_t tother[kTrans];
   uint8_t tseg[kTrans];
   uint8_t torder[kTrans];
+  uint8_t trank[kTrans];
+  // a leaving crossing's entering partner (the other slot of its pair), or
+  // kNoOther when the pair is not one clean enter/leave crossing
+  uint8_t tpart[kTrans];
   // per batch circle: first entry, entries kept after de-duplication,
   // transition-free circles before it, sin(alpha) and 1 / sin(alpha)
   uint16_t sbeg[kSasaBatch + 1];
@@ -343,34 +395,38 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       hit = dx * dx + dy * dy + dz * dz <= lim * lim;
     }
     unsigned hits = __ballot_sync(kFull, hit);
-    while (hits) {
-      const int b = __ffs(hits) - 1;
-      hits &= hits - 1;
-      const int j = (st.x + t0 + b) * 32 + lane;
-      bool is_cap = false;
-      double ax = 0.0, ay = 0.0, az = 0.0, ca = 0.0;
-      if (j != i && a.atom_sys[j] >= 0) {
-        const double dx = a.x[j] - pi.x, dy = a.y[j] - pi.y, dz = a.z[j] - pi.z;
-        const double rj = a.radius[j];
-        // d and 1/d from one reciprocal square root (d = 0 exactly for
-        // coincident centres); the quotients by d as products
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        const double inv_d = rsqrt(d2);
-        const double d = d2 > 0.0 ? d2 * inv_d : 0.0;
-        if (d <= ri + rj) {
-          if (d + ri <= rj) {
-            enclosed = true;
-          } else if (!(d + rj <= ri || d >= ri + rj)) {
-            ca = (d2 + ri * ri - rj * rj) * (inv_d * half_inv_ri);
-            if (ca >= -1.0 && ca <= 1.0) {
-              is_cap = true;
-              ax = dx * inv_d;
-              ay = dy * inv_d;
-              az = dz * inv_d;
-            }
-          }
-        }
+    // the atoms of two hit tiles per trip (independent loads in flight); the
+    // caps are written in ascending atom order, the first tile's first
+    struct Nb {
+      double x, y, z, r;
+      bool ok;
+    };
+    auto load = [&](int j) {
+      return Nb{a.x[j], a.y[j], a.z[j], a.radius[j], j != i && a.atom_sys[j] >= 0};
+    };
+    auto probe = [&](const Nb& n, double* ax, double* ay, double* az, double* ca) {
+      if (!n.ok) return false;
+      const double dx = n.x - pi.x, dy = n.y - pi.y, dz = n.z - pi.z;
+      const double rj = n.r;
+      // d and 1/d from one reciprocal square root (d = 0 exactly for
+      // coincident centres); the quotients by d as products
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      const double inv_d = rsqrt(d2);
+      const double d = d2 > 0.0 ? d2 * inv_d : 0.0;
+      if (d > ri + rj) return false;
+      if (d + ri <= rj) {
+        enclosed = true;
+        return false;
       }
+      if (d + rj <= ri || d >= ri + rj) return false;
+      *ca = (d2 + ri * ri - rj * rj) * (inv_d * half_inv_ri);
+      if (!(*ca >= -1.0 && *ca <= 1.0)) return false;
+      *ax = dx * inv_d;
+      *ay = dy * inv_d;
+      *az = dz * inv_d;
+      return true;
+    };
+    auto put_cap = [&](bool is_cap, int j, double ax, double ay, double az, double ca) {
       const unsigned caps = __ballot_sync(kFull, is_cap);
       if (is_cap) {
         const int slot = n_caps + __popc(caps & ((1u << lane) - 1u));
@@ -383,6 +439,20 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
         }
       }
       n_caps += __popc(caps);
+    };
+    while (hits) {
+      const int b = __ffs(hits) - 1;
+      hits &= hits - 1;
+      const int b2 = hits ? __ffs(hits) - 1 : -1;
+      if (b2 >= 0) hits &= hits - 1;
+      const int j = (st.x + t0 + b) * 32 + lane;
+      const int j2 = (st.x + t0 + b2) * 32 + lane;
+      double ax = 0.0, ay = 0.0, az = 0.0, ca = 0.0, ax2 = 0.0, ay2 = 0.0, az2 = 0.0, ca2 = 0.0;
+      const Nb n1 = load(j), n2 = load(b2 >= 0 ? j2 : j);
+      const bool c1 = probe(n1, &ax, &ay, &az, &ca);
+      const bool c2 = b2 >= 0 && probe(n2, &ax2, &ay2, &az2, &ca2);
+      put_cap(c1, j, ax, ay, az, ca);
+      if (b2 >= 0) put_cap(c2, j2, ax2, ay2, az2, ca2);
     }
   }
   ph.mark(0);
@@ -455,13 +525,23 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     }
     __syncwarp();
     // the counts are symmetric (circle k crosses cap m where circle m
-    // crosses cap k), so each unordered pair is classified once: row li,
-    // columns lm > li
-    const int n_pairs = n_live * n_live;
+    // crosses cap k), so each unordered pair is classified once: pair p of
+    // the n(n-1)/2 with li < lm, row-major.  Row l starts at
+    // S(l) = l (2n - 1 - l) / 2; the row of p is the floor of the smaller
+    // root of S(l) = p, corrected by one step for the rounding of sqrtf
+    // (the discriminant is an exact float: below 2^24).
+    const int n_pairs = n_live * (n_live - 1) / 2;
+    const float tn = static_cast<float>(2 * n_live - 1);
     bool tangent = false;
     for (int p = lane; p < n_pairs; p += 32) {
-      const int li = __float2int_rz((static_cast<float>(p) + 0.5f) * inv_live), lm = p - li * n_live;
-      if (lm <= li) continue;
+      int li = static_cast<int>((tn - sqrtf(tn * tn - 8.0f * static_cast<float>(p))) * 0.5f);
+      li = max(0, min(li, n_live - 2));
+      if ((li + 1) * (2 * n_live - 2 - li) / 2 <= p) {
+        ++li;
+      } else if (li * (2 * n_live - 1 - li) / 2 > p) {
+        --li;
+      }
+      const int lm = li + 1 + p - li * (2 * n_live - 1 - li) / 2;
       const Cap ck = cap_at(w, w.live[li]), cm = cap_at(w, w.live[lm]);
       const PairClass pc = classify(ck, cm);
       // a circle inside the other cap without crossing its rim
@@ -541,31 +621,42 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     // output positions, go to a warp queue (one entry per lane) whose full
     // rounds build the points with every lane busy.
     int run = 0;
-    bool mismatch = false;
+    bool mismatch = false, nonfinite = false;
+    using Key = SlotKey<W::kTrans>;
     // the transitions of batch circle j with cap m from slot base on
     // batch circle j's transitions on its crossing with cap m, the points
     // in the order of the pair (circle j, cap m), from slot base on
-    auto put = [&](int j, int m, int count, D3 pt, D3 qt, int base) {
-      const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
+    // (the two slots of a pair unrolled side by side)
+    // Crossing direction: moving counter-clockwise (along axis_k x u) the
+    // point enters cap m where the rate (axis_k x u).axis_m is positive and
+    // leaves it where negative; a tangent or a shallow crossing (|rate| <=
+    // 1e-4) gets 0.  The rate is -u.(axis_k x axis_m), and with
+    // u = (base - axis_k c_k +- (axis_k x axis_m) sqrt(c_sq)/sqrt(denom)) / sin(alpha)
+    // and base in the plane of the two axes, it is -+ sqrt(c_sq denom) /
+    // sin(alpha): p (the + root) leaves, q enters.
+    auto put = [&](int j, int m, const Cap& ck, double rate_sk, int count, D3 pt, D3 qt, int base) {
+      const int end = w.sbeg[j + 1];
       const double inv = w.binv[j];
-      const D3 h = helper_axis(ck.axis);
-      const D3 fu = h - ck.axis * dot(h, ck.axis);  // the angle is scale-free
-      const D3 fv = cross(ck.axis, fu);
-      for (int e = 0; e < count; ++e) {
+      D3 fu, fv;
+      slot_frame(ck.axis, &fu, &fv);
+      const bool clean = count == 2 && rate_sk * inv > 1e-4;
+      const int tg[2] = {clean ? -1 : 0, clean ? 1 : 0};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
         const int sl = base + e;
-        if (sl >= w.sbeg[j + 1]) break;  // never expected: the counts agree
+        if (e >= count || sl >= end) continue;  // sl >= end never expected: the counts agree
         const D3 u = ((e == 0 ? pt : qt) - ck.axis * ck.c) * inv;
-        w.ta[sl] = pseudo_angle(dot(u, fu), dot(u, fv));
+        const double x = dot(u, fu), y = dot(u, fv);
+        if (!isfinite(x) || !isfinite(y)) nonfinite = true;
+        w.tkey[sl] = Key::make(x, y, sl);
         w.tx[sl] = u.x;
         w.ty[sl] = u.y;
         w.tz[sl] = u.z;
         w.tother[sl] = static_cast<uint8_t>(m);
         w.tseg[sl] = static_cast<uint8_t>(j);
-        // crossing direction: moving counter-clockwise (along axis x u)
-        // the point enters cap m where the rate is positive and leaves it
-        // where negative; a tangent or a shallow crossing gets 0
-        const double rate = dot(cross(ck.axis, u), cm.axis);
-        w.ttog[sl] = count == 1 ? 0 : (rate > 1e-4 ? 1 : (rate < -1e-4 ? -1 : 0));
+        w.ttog[sl] = static_cast<int8_t>(tg[e]);
+        // the leaving crossing's entering partner (read for leaving ones only)
+        w.tpart[sl] = (e == 0 && clean) ? static_cast<uint8_t>(base + 1) : kNoOther;
       }
     };
     if (masks) {
@@ -601,8 +692,9 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
           const PairClass pc = classify(ck, cm);
           if (pc.count != 2) mismatch = true;  // never expected: classify is symmetric
           D3 pt{}, qt{};
-          transition_points(ck, cm, pc, &pt, &qt);
-          put(j, m, pc.count, pt, qt, w.sbeg[j] + 2 * r);
+          double rate_sk = 0.0;
+          transition_points(ck, cm, pc, &pt, &qt, &rate_sk);
+          put(j, m, ck, rate_sk, pc.count, pt, qt, w.sbeg[j] + 2 * r);
         }
       }
       run = 2 * n_ent;
@@ -618,8 +710,9 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
           const Cap ck = cap_at(w, w.live[b0 + j]), cm = cap_at(w, m);
           const PairClass pc = classify(ck, cm);
           D3 pt{}, qt{};
-          transition_points(ck, cm, pc, &pt, &qt);
-          put(j, m, pc.count, pt, qt, base);
+          double rate_sk = 0.0;
+          transition_points(ck, cm, pc, &pt, &qt, &rate_sk);
+          put(j, m, ck, rate_sk, pc.count, pt, qt, base);
         }
       };
       for (int p0 = 0; p0 < np; p0 += 32) {
@@ -658,7 +751,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       }
       drain(queued);
     }
-    if (__any_sync(kFull, mismatch)) {
+    if (__any_sync(kFull, mismatch || nonfinite)) {
       bad = true;
       break;
     }
@@ -671,7 +764,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
       const int sl = w.sbeg[j];
       w.tseg[sl] = static_cast<uint8_t>(j);
       w.tother[sl] = kNoOther;
-      w.ta[sl] = 0.0;
+      w.tkey[sl] = Key::pack(2.0f, sl);
       w.ttog[sl] = 0;
     }
     __syncwarp();
@@ -679,73 +772,125 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     ph.mark(4);
     ph.count(12, n_tr);
 
-    // stable sort of each circle's transitions by angle (ties: push order),
-    // summing the toggles met on the way
-    bool nonfinite = false;
+    // stable sort of each circle's transitions by angle (ties: push order):
+    // an entry's rank is the number of the circle's keys below its own.
+    // (This replaced FP64 angle comparisons with slot tie-breaks, summing the
+    // toggles on the way; four of those per trip with their loads issued
+    // together had measured 1.8x slower.)
+    constexpr int kShift = Key::kShift;
     for (int sl = lane; sl < n_tr; sl += 32) {
       const int j = w.tseg[sl];
       const int sb = w.sbeg[j], se = w.sbeg[j + 1];
-      int rank = 0, dep = 0;
-      if (w.tother[sl] != kNoOther) {
-        const double as = w.ta[sl];
-        if (!isfinite(as)) nonfinite = true;
-        // one loop over the circle (two loops split at sl, one comparison
-        // each, measured slower: the split point differs between lanes;
-        // four entries per trip with their loads issued together measured
-        // 1.8x slower)
-        for (int t = sb; t < se; ++t) {
-          const double at = w.ta[t];
-          const bool before = (at < as) || (at == as && t < sl);
-          rank += before;
-          dep += before ? w.ttog[t] : 0;
-        }
-        const int tg = w.ttog[sl];
-        if (tg == 0) {
-          atomicOr(&w.bmode[j], 1);
-        } else if (tg == -1) {
-          // burial depth (below): a leaving crossing wraps around the start
-          // of the circle when its pair's entering crossing -- the
-          // neighbouring slot of the same circle and cap -- sorts after it
-          const int m = w.tother[sl];
-          const int q = (sl + 1 < se && w.tother[sl + 1] == m) ? sl + 1 : sl - 1;
-          if (q < sb || w.ttog[q] != 1 || w.tother[q] != m) {
-            atomicOr(&w.bmode[j], 1);
-          } else {
-            const double aq = w.ta[q];
-            if (!((aq < as) || (aq == as && q < sl))) atomicAdd(&w.bbase[j], 1);
-          }
-        }
-      }
+      const uint32_t ks = w.tkey[sl];
+      int rank = 0;
+#pragma unroll 4
+      for (int t = sb; t < se; ++t) rank += w.tkey[t] < ks ? 1 : 0;
       rank = min(rank, se - sb - 1);
-      // the crossings up to and including this one, in angular order
-      w.tdep[sl] = static_cast<int8_t>(dep + w.ttog[sl]);
       w.torder[sb + rank] = static_cast<uint8_t>(sl);
-    }
-    if (__any_sync(kFull, nonfinite)) {
-      bad = true;
-      break;
+      w.trank[sl] = static_cast<uint8_t>(rank);
     }
     __syncwarp();
     ph.mark(5);
-
-    // consecutive de-duplication within each circle (|dp|^2 < 1e-12 against
-    // the last kept; |dp| = sin(alpha) |du|)
+    // One walk over the sorted positions finds circles with neighbours in
+    // key order less than two quanta apart, consecutive duplicates
+    // (|dp|^2 < 1e-12 against the entry before; |dp| = sin(alpha) |du|; the
+    // kept entries are picked below), and does the burial-depth bookkeeping:
+    // a tangent or shallow crossing sends its circle to explicit tests, a
+    // leaving crossing wraps around the start of the circle when its pair's
+    // entering crossing -- the neighbouring slot of the same circle and cap
+    // -- sorts after it, and a segmented inclusive scan of the toggles gives
+    // the crossings up to and including each entry in angular order.  A
+    // circle with such neighbours (rare: the quantum is 2^-21 of the angle's
+    // range) is ordered again from the FP64 angles and the walk repeated.
     bool dup = false;
-    for (int r = lane; r < n_tr; r += 32) {
-      const int j = w.tseg[w.torder[r]];
-      if (r == w.sbeg[j]) continue;
-      if (norm2(tpoint(w, w.torder[r]) - tpoint(w, w.torder[r - 1])) * (w.bsk[j] * w.bsk[j]) < 1e-12) {
-        dup = true;
-        atomicOr(&w.bmode[j], 1);
+    for (int walk = 0; walk < 2; ++walk) {
+      unsigned tied = 0;
+      int carry = 0;
+      dup = false;
+      for (int r0 = 0; r0 < n_tr; r0 += 32) {
+        const int r = r0 + lane;
+        int sl = 0, v = 0;
+        bool head = true;
+        if (r < n_tr) {
+          sl = w.torder[r];
+          const int j = w.tseg[sl], sb = w.sbeg[j];
+          head = r == sb;
+          v = w.ttog[sl];
+          if (!head) {
+            const int pv = w.torder[r - 1];
+            const uint32_t dq = (w.tkey[sl] >> kShift) - (w.tkey[pv] >> kShift);
+            if (dq <= 1) tied |= 1u << j;
+            // a duplicate is within (pi/2) 1e-6 / sin(alpha) of angle, so
+            // within that many quanta (+2, the quantisation and the FP32
+            // error); only those are measured
+            const double sk = w.bsk[j];
+            if (static_cast<double>(dq) * sk <= 2e-6 * Key::kScale + 2.0 &&
+                norm2(tpoint(w, sl) - tpoint(w, pv)) * (sk * sk) < 1e-12) {
+              dup = true;
+              atomicOr(&w.bmode[j], 1);
+            }
+          }
+          if (w.tother[sl] != kNoOther) {
+            if (v == 0) {
+              atomicOr(&w.bmode[j], 1);
+            } else if (v == -1) {
+              const int q = w.tpart[sl];
+              if (q == kNoOther) {
+                atomicOr(&w.bmode[j], 1);
+              } else if (w.trank[q] > w.trank[sl]) {
+                atomicAdd(&w.bbase[j], 1);
+              }
+            }
+          }
+        }
+        if (lane == 0 && !head) v += carry;
+        const unsigned heads = __ballot_sync(kFull, head) & ((2u << lane) - 1u);
+        const int first = heads ? 31 - __clz(heads) : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int y = __shfl_up_sync(kFull, v, d);
+          if (lane - d >= first) v += y;
+        }
+        if (r < n_tr) w.tdep[sl] = static_cast<int8_t>(v);
+        carry = __shfl_sync(kFull, v, 31);
       }
+      tied = __reduce_or_sync(kFull, tied);
+      if (walk == 1 || tied == 0) break;
+      // order the tied circles from the FP64 angles (ties: slot order) and
+      // start the bookkeeping of the batch again
+      __syncwarp();
+      if (lane < nb) {
+        w.bmode[lane] = (circle_tally(w, b0 + lane, masks) & kContained) ? 1 : 0;
+        w.bbase[lane] = 0;
+      }
+      while (tied) {
+        const int j = __ffs(tied) - 1;
+        tied &= tied - 1;
+        const int sb = w.sbeg[j], se = w.sbeg[j + 1];
+        D3 fu, fv;
+        slot_frame(cap_at(w, w.live[b0 + j]).axis, &fu, &fv);
+        for (int sl = sb + lane; sl < se; sl += 32) {
+          const double as = slot_angle(tpoint(w, sl), fu, fv);
+          int rank = 0;
+          for (int t = sb; t < se; ++t) {
+            const double at = slot_angle(tpoint(w, t), fu, fv);
+            rank += (at < as || (at == as && t < sl)) ? 1 : 0;
+          }
+          rank = min(rank, se - sb - 1);
+          w.torder[sb + rank] = static_cast<uint8_t>(sl);
+          w.trank[sl] = static_cast<uint8_t>(rank);
+        }
+      }
+      __syncwarp();
     }
+
     // Burial depth.  Along a circle whose crossings are all clean (no
     // tangent, no shallow crossing, nothing merged by de-duplication, no cap
     // holding it without a crossing), the point enters and leaves each
     // crossing cap once, so the depth just after a transition is the toggles
     // up to it plus the depth before the first transition -- the number of
     // caps whose leaving crossing comes before their entering one in angular
-    // order, counted during the sort.  A segment is exposed where the depth
+    // order, counted in the walk above.  A segment is exposed where the depth
     // is 0.  The other circles test every segment's midpoint against every
     // cap.
     __syncwarp();
@@ -783,27 +928,28 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
           j = jr;
           sa = w.torder[r];
           k = w.live[b0 + j];
-          const Cap ck = cap_at(w, k);
+          const int nxt = pos + 1 == kept ? 0 : pos + 1;
           if (w.tother[sa] == kNoOther) {
             // no transitions: exposed unless a probe on the circle is buried
             full = true;
-            probe = sample_circle_point(ck);
+            probe = sample_circle_point(cap_at(w, k));
             exposed = true;
             for (int lm = 0; lm < n_live && exposed; ++lm) {
               const int m = w.live[lm];
               if (m != k && contains_strict(cap_at(w, m), probe)) exposed = false;
             }
           } else if (w.bmode[j] == 0) {
-            sbn = w.torder[w.sbeg[j] + (pos + 1) % kept];
+            sbn = w.torder[w.sbeg[j] + nxt];
             if (w.bbase[j] + w.tdep[sa] == 0) {
               // the reference's skip of a vanishing segment (ccw < 1e-9)
               const D3 ua = tpoint(w, sa), ub = tpoint(w, sbn);
               cos_ccw = dot(ua, ub);
-              sin_ccw = dot(ck.axis, cross(ua, ub));
+              sin_ccw = dot(D3{w.cx[k], w.cy[k], w.cz[k]}, cross(ua, ub));
               exposed = !(cos_ccw > 0.0 && sin_ccw >= 0.0 && sin_ccw < 2e-9 && atan2(sin_ccw, cos_ccw) < 1e-9);
             }
           } else {
-            sbn = w.torder[w.sbeg[j] + (pos + 1) % kept];
+            sbn = w.torder[w.sbeg[j] + nxt];
+            const Cap ck = cap_at(w, k);
             D3 mid;
             if (segment_midpoint(tpoint(w, sa), tpoint(w, sbn), ck, w.bsk[j], kept == 1, &mid, &cos_ccw,
                                  &sin_ccw)) {
@@ -1004,7 +1150,9 @@ __global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
 
 // The queued atoms, one warp per block at the large capacities (persistent:
 // the queue length is known only on the device).
-__global__ void __launch_bounds__(32) k_sasa_boundary_big(SasaArgs a) {
+// (One-warp blocks leave registers to spare; the cap keeps the compiler from
+// choosing a smaller allocation with spills.)
+__global__ void __maxnreg__(168) k_sasa_boundary_big(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSmemBig& w = *reinterpret_cast<WarpSmemBig*>(smem_raw);
   const int n = min(a.counts[2], a.overflow_cap);
@@ -1119,8 +1267,8 @@ __device__ void walk_faces(W& w, int n_arcs, int lane, int* loops_out, double* v
 // the components are found).
 template <class W>
 __device__ int count_components(const SasaArgs& a, W& w, int n_live, int lane) {
-  static_assert(sizeof(w.ta) >= kSasaProbes * sizeof(int16_t) && sizeof(w.tx) >= kSasaProbes, "probe scratch");
-  volatile int16_t* lab = reinterpret_cast<int16_t*>(w.ta);
+  static_assert(sizeof(w.ty) >= kSasaProbes * sizeof(int16_t) && sizeof(w.tx) >= kSasaProbes, "probe scratch");
+  volatile int16_t* lab = reinterpret_cast<int16_t*>(w.ty);
   uint8_t* acc = reinterpret_cast<uint8_t*>(w.tx);
   bool any = false;
   for (int p = lane; p < kSasaProbes; p += 32) {
