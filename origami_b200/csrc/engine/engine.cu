@@ -786,10 +786,10 @@ og_status build_pass_list(og_engine* e, int first_offset, int W, int chunk, DVec
 }
 
 og_status build_pair_lists(og_engine* e, cudaStream_t st) {
-  og_status s = build_pass_list(e, 0, ogk::pair_shape_warps(e->born_launch.shape), e->chunk_b, &e->work, &e->n_work,
+  og_status s = build_pass_list(e, 0, ogk::pair_shape_tiles(e->born_launch.shape), e->chunk_b, &e->work, &e->n_work,
                                 &e->jlist, &e->cut_b, &e->n_cut_b, &e->jlist_cut_b, &e->seg_end_b, st);
   if (s != OG_OK) return s;
-  return build_pass_list(e, 1, ogk::pair_shape_warps(e->force_launch.shape), e->chunk_f, &e->work_f, &e->n_work_f,
+  return build_pass_list(e, 1, ogk::pair_shape_tiles(e->force_launch.shape), e->chunk_f, &e->work_f, &e->n_work_f,
                          &e->jlist_f, &e->cut_f, &e->n_cut_f, &e->jlist_cut_f, &e->seg_end_f, st);
 }
 
@@ -921,7 +921,7 @@ og_status finalize_impl(og_engine* e) {
     }
     // counters and the queue of atoms beyond the default arrangement
     // capacities: used by the force path and by area queries alike
-    OG_CUDA(e->sasa_counts.alloc(3));
+    OG_CUDA(e->sasa_counts.alloc(4));
     OG_CUDA(e->sasa_overflow.alloc(std::max(1, std::max(e->n_sasa_all, e->n_sasa_tasks))));
     // Component probes: Fibonacci points, golden angle pi (3 - sqrt 5),
     // joined when their dot product exceeds cos(2.5 sqrt(4 pi / N))
@@ -2232,7 +2232,7 @@ og_status time_pass(og_engine* e, bool born, const ogk::PairLaunch& lc, int chun
   DVec<int32_t> jl, jl_cut, seg;
   DVec<ogk::CutBlock> cut;
   int n_work = 0, n_cut = 0;
-  og_status s = build_pass_list(e, born ? 0 : 1, ogk::pair_shape_warps(lc.shape), chunk, &work, &n_work, &jl, &cut,
+  og_status s = build_pass_list(e, born ? 0 : 1, ogk::pair_shape_tiles(lc.shape), chunk, &work, &n_work, &jl, &cut,
                                 &n_cut, &jl_cut, &seg, st);
   if (s != OG_OK) return s;
   ogk::PairArgs a = e->pair_args();
@@ -2292,8 +2292,9 @@ og_status apply_launch(og_engine* e, const TuneEntry& t) {
   return OG_OK;
 }
 
-bool valid_launch(int shape, int persistent, int chunk) {
-  return shape >= 0 && shape <= 2 && (persistent == 0 || persistent == 1) && chunk >= 1 && chunk <= 4096;
+bool valid_launch(int pass, int shape, int persistent, int chunk) {
+  return shape >= 0 && shape < (pass == 0 ? ogk::kBornShapes : ogk::kForceShapes) &&
+         (persistent == 0 || persistent == 1) && chunk >= 1 && chunk <= 4096;
 }
 
 }  // namespace
@@ -2301,8 +2302,9 @@ bool valid_launch(int shape, int persistent, int chunk) {
 og_status og_engine_set_pair_launch(og_engine* e, int32_t pass, int32_t shape, int32_t persistent, int32_t chunk) {
   og_status s = check_ready(e);
   if (s != OG_OK) return s;
-  if ((pass != 0 && pass != 1) || !valid_launch(shape, persistent, chunk))
-    return og_fail(OG_E_BADARG, "og_engine_set_pair_launch: pass 0/1, shape 0..2, persistent 0/1, chunk >= 1");
+  if ((pass != 0 && pass != 1) || !valid_launch(pass, shape, persistent, chunk))
+    return og_fail(OG_E_BADARG,
+                   "og_engine_set_pair_launch: pass 0/1, shape 0..2 (Born) or 0..4 (force), persistent 0/1, chunk >= 1");
   TuneEntry t{{e->born_launch.shape, e->born_launch.persistent ? 1 : 0, e->chunk_b},
               {e->force_launch.shape, e->force_launch.persistent ? 1 : 0, e->chunk_f}, 0.0, 0.0};
   int* dst = pass == 0 ? t.b : t.f;
@@ -2321,8 +2323,8 @@ og_status og_engine_autotune(og_engine* e, const char* cache_path, og_autotune_r
   bool from_cache = false;
   double b_def = -1.0, f_def = -1.0;
   auto it = cache.find(key);
-  if (it != cache.end() && valid_launch(it->second.b[0], it->second.b[1], it->second.b[2]) &&
-      valid_launch(it->second.f[0], it->second.f[1], it->second.f[2])) {
+  if (it != cache.end() && valid_launch(0, it->second.b[0], it->second.b[1], it->second.b[2]) &&
+      valid_launch(1, it->second.f[0], it->second.f[1], it->second.f[2])) {
     best = it->second;
     from_cache = true;
   } else {
@@ -2344,7 +2346,7 @@ og_status og_engine_autotune(og_engine* e, const char* cache_path, og_autotune_r
     for (int pass = 0; pass < 2; ++pass) {
       double bt = 1e30;
       int bc[3] = {0, 0, 16};
-      for (int shape = 0; shape <= 2; ++shape)
+      for (int shape = 0; shape < (pass == 0 ? ogk::kBornShapes : ogk::kForceShapes); ++shape)
         for (int pers = 0; pers <= 1; ++pers)
           for (int chunk : chunks) {
             double ms = 0.0;

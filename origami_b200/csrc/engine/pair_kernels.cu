@@ -515,6 +515,196 @@ OG_UNROLL(OG_FORCE_UNROLL)
   }
 }
 
+// ------------------------------------------------------ force, i pairs
+// The same pair terms with two i-tiles per warp: lane l holds atom l of the
+// block's tiles 2w and 2w + 1 in the two halves of every float2, so one
+// FP32x2 instruction evaluates a j atom against both, and the stage's j
+// columns are expanded in shared memory to (v, v) pairs to feed it.  A j
+// atom's contributions from the two i atoms are summed in the lane before
+// the warp reduce-scatter, which then serves eight pairs instead of four
+// (in k_force the reduce-scatter is about a third of all instructions).
+// Sums and their order per i atom and per j atom are as in k_force's
+// structure: FP32 per j-tile and 4-atom group, FP64 across tiles, warps
+// summed in a fixed order, fixed point at the end.
+template <bool kAllPairs, int W, int kMinBlocks, bool kPersistent>
+__global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
+  __shared__ __align__(128) float s_buf[2][3][kStageFloats];   // raw columns of pq, lj, gb (TMA)
+  __shared__ __align__(16) float s_dup[3][2 * kStageFloats];    // the stage's columns, each value twice
+  __shared__ float s_part[W][3][kStageTiles * kTile];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_item;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t g = 0;  // stages this CTA has consumed
+  for (int item = next_item<kPersistent>(a, &s_item, -1); item < a.n_work;
+       item = next_item<kPersistent>(a, &s_item, item)) {
+  PairWork w = a.work[item];
+  if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
+  if (w.j_begin >= w.j_end) continue;  // chunk culled by the cutoff (block-uniform)
+  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar, g};
+  const float* src[3] = {a.pq, a.lj, a.gb};
+  if (threadIdx.x == 0) {
+    if (st.n_stages > 0) st.issue<3>(0, s_buf, src);
+    if (st.n_stages > 1) st.issue<3>(1, s_buf, src);
+  }
+
+  // tiles 2w (half x) and 2w + 1 (half y); a missing second tile repeats the
+  // first, with its pairs masked out
+  const bool act_a = 2 * warp < w.n_i_tiles, act_b = 2 * warp + 1 < w.n_i_tiles;
+  const int it_a = w.i_tile0 + (act_a ? 2 * warp : 0);
+  const int it_b = act_b ? it_a + 1 : it_a;
+  const int i_a = it_a * kTile + lane, i_b = it_b * kTile + lane;
+  const float2 px = make_float2(a.pq[soa_index(i_a, 0)], a.pq[soa_index(i_b, 0)]);
+  const float2 py = make_float2(a.pq[soa_index(i_a, 1)], a.pq[soa_index(i_b, 1)]);
+  const float2 pz = make_float2(a.pq[soa_index(i_a, 2)], a.pq[soa_index(i_b, 2)]);
+  IAtom2 ia;
+  {
+    const float2 qi = make_float2(a.pq[soa_index(i_a, 3)], a.pq[soa_index(i_b, 3)]);
+    const float2 Ri = make_float2(a.gb[soa_index(i_a, 0)], a.gb[soa_index(i_b, 0)]);
+    const float2 iRi = make_float2(a.gb[soa_index(i_a, 1)], a.gb[soa_index(i_b, 1)]);
+    ia.rm = make_float2(a.lj[soa_index(i_a, 0)], a.lj[soa_index(i_b, 0)]);
+    ia.se = mul2(bc(a.lj_kj12), make_float2(a.lj[soa_index(i_a, 1)], a.lj[soa_index(i_b, 1)]));
+    ia.cq = mul2(bc(-a.coul_kj), qi);
+    ia.gq = mul2(bc(a.gb_pref_kj), qi);
+    ia.R = Ri;
+    ia.nexp = mul2(bc(-0.25f * kLog2e), iRi);
+    ia.nrc3 = bc(-a.inv_rc3);
+  }
+  int mref_a = a.mask_begin[it_a], mref_b = a.mask_begin[it_b];
+  const int mend_a = a.mask_begin[it_a + 1], mend_b = a.mask_begin[it_b + 1];
+  double acc_ax = 0.0, acc_ay = 0.0, acc_az = 0.0, acc_bx = 0.0, acc_by = 0.0, acc_bz = 0.0;
+
+  for (int s = 0; s < st.n_stages; ++s) {
+    const uint32_t gs = g + s;
+    const int b = gs & 1;
+    const bool ok = mbar_wait_bounded(&s_bar[b], (gs >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
+      return;
+    }
+    const int t0 = w.j_begin + s * kStageTiles;
+    const int cnt = min(kStageTiles, w.j_end - t0);
+    // expand the stage's columns: value q of an array to entries 2q, 2q + 1
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      for (int q = threadIdx.x; q < cnt * 128; q += W * 32) {
+        const float v = s_buf[b][c][q];
+        *reinterpret_cast<float2*>(&s_dup[c][2 * q]) = make_float2(v, v);
+      }
+    __syncthreads();  // s_dup is complete and raw buffer b is free
+    if (threadIdx.x == 0 && s + 2 < st.n_stages) st.issue<3>(s + 2, s_buf, src);
+    for (int t = 0; t < cnt; ++t) {
+      const int jt = a.jlist[t0 + t];
+      while (mref_a < mend_a && a.mask_refs[mref_a].j_tile < jt) ++mref_a;
+      while (mref_b < mend_b && a.mask_refs[mref_b].j_tile < jt) ++mref_b;
+      const bool va = act_a && jt > it_a && !(mref_a < mend_a && a.mask_refs[mref_a].j_tile == jt);
+      const bool vb = act_b && jt > it_b && !(mref_b < mend_b && a.mask_refs[mref_b].j_tile == jt);
+      float* jfx = &s_part[warp][0][t * kTile];
+      float* jfy = &s_part[warp][1][t * kTile];
+      float* jfz = &s_part[warp][2][t * kTile];
+      if (!(va || vb)) {
+        jfx[lane] = 0.0f;
+        jfy[lane] = 0.0f;
+        jfz[lane] = 0.0f;
+        continue;
+      }
+      const bool both = va && vb;
+      const double4 oj = a.origin[jt], oa = a.origin[it_a], ob = a.origin[it_b];
+      ia.nx = make_float2(-(px.x - static_cast<float>(oj.x - oa.x)), -(px.y - static_cast<float>(oj.x - ob.x)));
+      ia.ny = make_float2(-(py.x - static_cast<float>(oj.y - oa.y)), -(py.y - static_cast<float>(oj.y - ob.y)));
+      ia.nz = make_float2(-(pz.x - static_cast<float>(oj.z - oa.z)), -(pz.y - static_cast<float>(oj.z - ob.z)));
+      const float* dp = &s_dup[0][t * 256];
+      const float* dl = &s_dup[1][t * 256];
+      const float* dg = &s_dup[2][t * 256];
+      float2 fx = bc(0.0f), fy = bc(0.0f), fz = bc(0.0f);
+      for (int k0 = 0; k0 < kTile; k0 += 4) {
+        float tjx[4], tjy[4], tjz[4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int k2 = 2 * (k0 + 2 * h);  // two j atoms: entries k2 .. k2 + 3
+          const float4 X = *reinterpret_cast<const float4*>(&dp[k2]);
+          const float4 Y = *reinterpret_cast<const float4*>(&dp[64 + k2]);
+          const float4 Z = *reinterpret_cast<const float4*>(&dp[128 + k2]);
+          const float4 Q = *reinterpret_cast<const float4*>(&dp[192 + k2]);
+          const float4 RM = *reinterpret_cast<const float4*>(&dl[k2]);
+          const float4 SE = *reinterpret_cast<const float4*>(&dl[64 + k2]);
+          const float4 RB = *reinterpret_cast<const float4*>(&dg[k2]);
+          const float4 IR = *reinterpret_cast<const float4*>(&dg[64 + k2]);
+          const Sep2 s0 = sep2(make_float2(X.x, X.y), make_float2(Y.x, Y.y), make_float2(Z.x, Z.y), ia);
+          const Sep2 s1 = sep2(make_float2(X.z, X.w), make_float2(Y.z, Y.w), make_float2(Z.z, Z.w), ia);
+          const float2 arg0 = gb_arg2(s0, make_float2(IR.x, IR.y), ia);
+          const float2 arg1 = gb_arg2(s1, make_float2(IR.z, IR.w), ia);
+          const bool far = __all_sync(0xffffffffu, fmaxf(fmaxf(arg0.x, arg0.y), fmaxf(arg1.x, arg1.y)) < -30.0f);
+          float2 c0, c1;
+          if (far) {
+            c0 = coeff2<kAllPairs, true>(s0, arg0, make_float2(Q.x, Q.y), make_float2(RM.x, RM.y),
+                                         make_float2(SE.x, SE.y), make_float2(RB.x, RB.y), ia, a);
+            c1 = coeff2<kAllPairs, true>(s1, arg1, make_float2(Q.z, Q.w), make_float2(RM.z, RM.w),
+                                         make_float2(SE.z, SE.w), make_float2(RB.z, RB.w), ia, a);
+          } else {
+            c0 = coeff2<kAllPairs, false>(s0, arg0, make_float2(Q.x, Q.y), make_float2(RM.x, RM.y),
+                                          make_float2(SE.x, SE.y), make_float2(RB.x, RB.y), ia, a);
+            c1 = coeff2<kAllPairs, false>(s1, arg1, make_float2(Q.z, Q.w), make_float2(RM.z, RM.w),
+                                          make_float2(SE.z, SE.w), make_float2(RB.z, RB.w), ia, a);
+          }
+          if (!both) {  // one tile's pairs with this j-tile are near field or counted elsewhere
+            c0 = make_float2(va ? c0.x : 0.0f, vb ? c0.y : 0.0f);
+            c1 = make_float2(va ? c1.x : 0.0f, vb ? c1.y : 0.0f);
+          }
+          const float2 ux0 = mul2(s0.dx, c0), uy0 = mul2(s0.dy, c0), uz0 = mul2(s0.dz, c0);
+          const float2 ux1 = mul2(s1.dx, c1), uy1 = mul2(s1.dy, c1), uz1 = mul2(s1.dz, c1);
+          fx = add2(fx, add2(ux0, ux1));
+          fy = add2(fy, add2(uy0, uy1));
+          fz = add2(fz, add2(uz0, uz1));
+          tjx[2 * h] = ux0.x + ux0.y;
+          tjy[2 * h] = uy0.x + uy0.y;
+          tjz[2 * h] = uz0.x + uz0.y;
+          tjx[2 * h + 1] = ux1.x + ux1.y;
+          tjy[2 * h + 1] = uy1.x + uy1.y;
+          tjz[2 * h + 1] = uz1.x + uz1.y;
+        }
+        const float tx = reduce_scatter4(tjx[0], tjx[1], tjx[2], tjx[3], lane);
+        const float ty = reduce_scatter4(tjy[0], tjy[1], tjy[2], tjy[3], lane);
+        const float tz = reduce_scatter4(tjz[0], tjz[1], tjz[2], tjz[3], lane);
+        if ((lane & 7) == 0) {
+          jfx[k0 + (lane >> 3)] = -tx;
+          jfy[k0 + (lane >> 3)] = -ty;
+          jfz[k0 + (lane >> 3)] = -tz;
+        }
+      }
+      acc_ax += static_cast<double>(fx.x);
+      acc_ay += static_cast<double>(fy.x);
+      acc_az += static_cast<double>(fz.x);
+      acc_bx += static_cast<double>(fx.y);
+      acc_by += static_cast<double>(fy.y);
+      acc_bz += static_cast<double>(fz.y);
+    }
+    __syncthreads();  // every warp is done with s_dup and has written its j partials
+    unsigned long long* dst[3] = {a.fx, a.fy, a.fz};
+    flush_j<W, 3>(a, a.jlist, t0, cnt, s_part, dst, kForceScale);
+  }
+  g += st.n_stages;
+  if (act_a && a.atom_valid[i_a]) {
+    if (!(isfinite(acc_ax) && isfinite(acc_ay) && isfinite(acc_az))) atomicOr(a.sys_nonfinite + a.atom_sys[i_a], 1);
+    add_fixed(a.fx + i_a, acc_ax, kForceScale);
+    add_fixed(a.fy + i_a, acc_ay, kForceScale);
+    add_fixed(a.fz + i_a, acc_az, kForceScale);
+  }
+  if (act_b && a.atom_valid[i_b]) {
+    if (!(isfinite(acc_bx) && isfinite(acc_by) && isfinite(acc_bz))) atomicOr(a.sys_nonfinite + a.atom_sys[i_b], 1);
+    add_fixed(a.fx + i_b, acc_bx, kForceScale);
+    add_fixed(a.fy + i_b, acc_by, kForceScale);
+    add_fixed(a.fz + i_b, acc_bz, kForceScale);
+  }
+  }
+}
+
 }  // namespace
 
 
@@ -596,18 +786,37 @@ void force_variant(const PairArgs& a, cudaStream_t s) {
   }
 }
 
+template <bool AP, int W, int MB, bool P>
+void force_ip_variant(const PairArgs& a, cudaStream_t s) {
+  auto k = k_force_ip<AP, W, MB, P>;
+  if (P) {
+    cudaMemsetAsync(a.queue, 0, sizeof(int32_t), s);
+    k<<<persistent_grid(k, W * 32, a.n_work), W * 32, 0, s>>>(a);
+  } else {
+    k<<<a.n_work, W * 32, 0, s>>>(a);
+  }
+}
+
 template <bool AP, bool P>
 void force_shape(const PairArgs& a, int shape, cudaStream_t s) {
   switch (shape) {
     case 1: force_variant<AP, 4, 4, P>(a, s); break;
     case 2: force_variant<AP, 8, 3, P>(a, s); break;
+    case 3: force_ip_variant<AP, 8, 2, P>(a, s); break;
+    case 4: force_ip_variant<AP, 4, 4, P>(a, s); break;
     default: force_variant<AP, 8, 2, P>(a, s); break;
   }
 }
 
 }  // namespace
 
-int pair_shape_warps(int shape) { return shape == 1 ? 4 : 8; }
+int pair_shape_tiles(int shape) {
+  switch (shape) {
+    case 1: return 4;
+    case 3: return 16;
+    default: return 8;
+  }
+}
 
 void launch_born_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s) {
   if (a.n_work <= 0) return;

@@ -28,6 +28,7 @@
 //    exposed arcs' central angles.
 //  * The gradient of A_i is taken term by term in reverse mode (sasa_geom.h)
 //    instead of one forward directional derivative per (atom, axis).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -1139,13 +1140,22 @@ __device__ void boundary_task(const SasaArgs& a, W& w, int i, int lane, bool big
   ph.flush(lane);
 }
 
+// Each warp takes atoms from the queue counts[3] until none are left (a
+// persistent grid of resident blocks): atoms differ several-fold in work,
+// and a warp whose atom was quick takes the next one instead of holding its
+// slot until the slowest warp of its block is done.
+__device__ __forceinline__ int next_task(const SasaArgs& a, int lane) {
+  int task = 0;
+  if (lane == 0) task = atomicAdd(&a.counts[3], 1);
+  return __shfl_sync(kFull, task, 0);
+}
+
 __global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  const int task = blockIdx.x * kWarps + warp;
-  if (task >= a.n_tasks) return;
-  boundary_task(a, w, a.tasks[task], lane, false);
+  for (int task = next_task(a, lane); task < a.n_tasks; task = next_task(a, lane))
+    boundary_task(a, w, a.tasks[task], lane, false);
 }
 
 // The queued atoms, one warp per block at the large capacities (persistent:
@@ -1338,13 +1348,12 @@ __device__ void areas_task(const SasaArgs& a, W& w, int i, int lane, bool big) {
   }
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_sasa_areas(SasaArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_areas(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
-  const int task = blockIdx.x * kWarps + warp;
-  if (task >= a.n_tasks) return;
-  areas_task(a, w, a.tasks[task], lane, false);
+  for (int task = next_task(a, lane); task < a.n_tasks; task = next_task(a, lane))
+    areas_task(a, w, a.tasks[task], lane, false);
 }
 
 __global__ void __launch_bounds__(32) k_sasa_areas_big(SasaArgs a) {
@@ -1452,18 +1461,33 @@ cudaError_t sasa_prepare() {
   return e;
 }
 
+// Resident blocks of a queue-driven kernel: the SM count times the blocks
+// that fit (no more than the atoms need).
+template <class K>
+int resident_grid(K kernel, int n_tasks) {
+  static int n_sm = 0;
+  if (n_sm == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, kWarpSmemBytes);
+  return std::max(1, std::min((n_tasks + kWarps - 1) / kWarps, std::max(per_sm, 1) * std::max(n_sm, 1)));
+}
+
 void launch_sasa_forces(const SasaArgs& a, cudaStream_t s) {
   if (a.n_tasks <= 0) return;
-  cudaMemsetAsync(a.counts, 0, 3 * sizeof(int32_t), s);
-  k_sasa_boundary<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  cudaMemsetAsync(a.counts, 0, 4 * sizeof(int32_t), s);
+  k_sasa_boundary<<<resident_grid(k_sasa_boundary, a.n_tasks), kWarps * 32, kWarpSmemBytes, s>>>(a);
   k_sasa_boundary_big<<<kBigGrid, 32, kBigSmemBytes, s>>>(a);
   k_sasa_terms<<<148 * 8, 128, 0, s>>>(a);
 }
 
 void launch_sasa_areas(const SasaArgs& a, cudaStream_t s) {
   if (a.n_tasks <= 0) return;
-  cudaMemsetAsync(a.counts + 2, 0, sizeof(int32_t), s);
-  k_sasa_areas<<<(a.n_tasks + kWarps - 1) / kWarps, kWarps * 32, kWarpSmemBytes, s>>>(a);
+  cudaMemsetAsync(a.counts + 2, 0, 2 * sizeof(int32_t), s);
+  k_sasa_areas<<<resident_grid(k_sasa_areas, a.n_tasks), kWarps * 32, kWarpSmemBytes, s>>>(a);
   k_sasa_areas_big<<<kBigGrid, 32, kBigSmemBytes, s>>>(a);
 }
 

@@ -68,7 +68,8 @@ struct SasaArgs {
   // force path: term records of every atom's boundary, appended through
   // counts[0] (arcs) and counts[1] (vertices), capacity `term_cap` each;
   // counts[2] counts the atoms queued in overflow[] (capacity overflow_cap)
-  // for the large-capacity kernels
+  // for the large-capacity kernels; counts[3] is the next atom of the
+  // default-capacity kernels' work queue
   SasaArcTerm* arc_terms;
   SasaVertexTerm* vertex_terms;
   int32_t* counts;
