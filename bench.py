@@ -295,7 +295,10 @@ def make_engine(og, args, topo, xyz, rank: int, born_mode: int, stream):
     eng.set_stream(stream.cuda_stream)
     for r in range(args.replicas):
         eng.init_velocities(r, replica_seed(args.seed, rank, args.replicas, r), remove_com=False)
-    if not args.no_autotune:  # untimed set-up: pick the pair passes' launch variants
+    if args.force_launch:  # a fixed variant (shape,persistent,chunk), e.g. for a profile of one kernel
+        shape, pers, chunk = (int(v) for v in args.force_launch.split(","))
+        eng.set_pair_launch("force", shape, bool(pers), chunk)
+    elif not args.no_autotune:  # untimed set-up: pick the pair passes' launch variants
         eng.tune = eng.autotune(args.tune_cache)
     return eng
 
@@ -764,6 +767,8 @@ def main():
                     help="c5 slices without SHAKE (the reference's run_slice integrator, with --c5-dt 1)")
     ap.add_argument("--c3a-ps", type=float, default=100.0, help="simulated time of the c3a run per replica (ps)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default pair-pass launches")
+    ap.add_argument("--force-launch", default=None,
+                    help="force-pass launch variant 'shape,persistent,chunk' instead of the autotuner's")
     ap.add_argument("--tune-cache", default=None, help="JSON file caching the autotuner's choices")
     ap.add_argument("--no-relax", action="store_true",
                     help="start from the extended build (profiling runs: fixed launch sequence before the timed steps)")
