@@ -496,8 +496,9 @@ def run_b200(args):
                               if args.cutoff else None),
                      "traffic": FORCE_PASS_DRAM_BYTES_PER_REPLICA * args.replicas,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_force<1> at 4 "
-                                       "replicas (profiles/pair_kernels_4x4694_extended.md; the relaxed chain gives the same 1.51 MB, "
-                                       "profiles/force_pass_instruction_mix_4x4694.md), per replica x replicas",
+                                       "replicas (profiles/pair_kernels_4x4694_extended.md; the relaxed chain and the "
+                                       "two-i-tile k_force_ip give the same 1.51 MB, "
+                                       "profiles/force_ip_instruction_mix_4x4694.md), per replica x replicas",
                      "peak_source": "measured FP32 FMA chain (og_measure_fp32_peak); the pair math is FP32 "
                                     "CUDA-core work, so neither the HBM copy nor the BF16 tensor peak bounds it",
                      "work": "55 flop per unordered pair (include/flops.h) x N(N-1)/2 x replicas"},
