@@ -29,6 +29,7 @@
 //  * The gradient of A_i is taken term by term in reverse mode (sasa_geom.h)
 //    instead of one forward directional derivative per (atom, axis).
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 
 #include "common.cuh"
@@ -51,8 +52,9 @@ constexpr int kSasaBatch = 32;        // circles per arrangement batch
 constexpr uint8_t kNoOther = 0xFF;    // pseudo entry of a transition-free circle
 constexpr int32_t kContained = 1 << 16;  // circle inside a cap it does not cross
 constexpr int32_t kCountMask = kContained - 1;
-// crossing masks: one bit per live circle below 63, bit 63 for kContained
-constexpr int kMaskCircles = 63;
+// crossing masks: one bit per live circle below kMaskCircles, bit 63 for
+// kContained
+constexpr int kMaskCircles = 56;
 constexpr uint64_t kMaskContained = 1ull << 63;
 constexpr double kPi = 3.14159265358979323846;
 
@@ -1150,7 +1152,7 @@ __device__ __forceinline__ int next_task(const SasaArgs& a, int lane) {
   return __shfl_sync(kFull, task, 0);
 }
 
-__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_boundary(SasaArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 5) k_sasa_boundary(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
@@ -1277,7 +1279,11 @@ __device__ void walk_faces(W& w, int n_arcs, int lane, int* loops_out, double* v
 // the components are found).
 template <class W>
 __device__ int count_components(const SasaArgs& a, W& w, int n_live, int lane) {
-  static_assert(sizeof(w.ty) >= kSasaProbes * sizeof(int16_t) && sizeof(w.tx) >= kSasaProbes, "probe scratch");
+  // labels over ty and tz (adjacent), acceptance flags over tx: the
+  // transition arrays are free once the arrangement is done
+  static_assert(offsetof(W, tz) == offsetof(W, ty) + sizeof(w.ty) &&
+                    sizeof(w.ty) + sizeof(w.tz) >= kSasaProbes * sizeof(int16_t) && sizeof(w.tx) >= kSasaProbes,
+                "probe scratch");
   volatile int16_t* lab = reinterpret_cast<int16_t*>(w.ty);
   uint8_t* acc = reinterpret_cast<uint8_t*>(w.tx);
   bool any = false;
@@ -1348,7 +1354,7 @@ __device__ void areas_task(const SasaArgs& a, W& w, int i, int lane, bool big) {
   }
 }
 
-__global__ void __launch_bounds__(kWarps * 32, 4) k_sasa_areas(SasaArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 5) k_sasa_areas(SasaArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
@@ -1441,8 +1447,10 @@ __global__ void __launch_bounds__(kWarps * 32) k_shrake_rupley(SasaArgs a, const
 constexpr size_t kWarpSmemBytes = sizeof(WarpSmem) * kWarps;
 constexpr size_t kBigSmemBytes = sizeof(WarpSmemBig);
 constexpr int kBigGrid = 148 * 4;  // persistent one-warp blocks for the queue
-// four resident CTAs per SM (228 KB, 1 KB reserved per CTA)
-static_assert(4 * (kWarpSmemBytes + 1024) <= 228 * 1024, "boundary kernel no longer fits four CTAs per SM");
+// five resident CTAs per SM (228 KB, 1 KB reserved per CTA): 20 warps; at
+// four (the capacities 128 caps, 128 transitions, 48 arcs) the kernel was
+// 1.6 % slower
+static_assert(5 * (kWarpSmemBytes + 1024) <= 228 * 1024, "boundary kernel no longer fits five CTAs per SM");
 
 }  // namespace
 

@@ -17,11 +17,12 @@ namespace ogk {
 // about 90 caps, 46 of them left after contained caps are dropped, 72
 // transitions on one circle and 19 exposed arcs.
 // Arrangement capacities per atom: the default kernels' (four warps per
-// block) and the large ones for the atoms that exceed them (caps cutting the
-// atom's sphere, transitions of one batch of circles, exposed arcs).
-constexpr int kSasaMaxCaps = 128;
-constexpr int kSasaMaxTrans = 128;
-constexpr int kSasaMaxArcs = 48;
+// block, five blocks per SM) and the large ones for the atoms that exceed
+// them (caps cutting the atom's sphere, transitions of one batch of circles,
+// exposed arcs).
+constexpr int kSasaMaxCaps = 112;
+constexpr int kSasaMaxTrans = 96;
+constexpr int kSasaMaxArcs = 36;
 constexpr int kSasaBigCaps = 254;
 constexpr int kSasaBigTrans = 254;
 constexpr int kSasaBigArcs = 128;
