@@ -505,8 +505,8 @@ def run_b200(args):
         "dominant_kernel": {
             "kernel": "k_sasa_boundary + k_sasa_terms (PowerSasa, FP64)",
             "ms_per_step": (prof["sasa"][0] / prof["sasa"][1]) if "sasa" in prof else None,
-            "bound": "dependency latency at 16 warps per SM (ncu on the relaxed chain: issue active 47 %, "
-                     "FP64 pipe 17 %, DRAM 0.03 %, 24 of 32 lanes active); data-dependent geometry, no flop "
+            "bound": "dependency latency at 20 warps per SM (ncu on the relaxed chain: issue active 52 %, "
+                     "FP64 pipe 14 %, DRAM 0.03 %, 23 of 32 lanes active); data-dependent geometry, no flop "
                      "or byte roofline",
             "profile": "profiles/sasa_boundary_4x4694_relaxed.md",
             "launch_list": "profiles/launch_list_64x4694_plain_step.md"},
