@@ -88,16 +88,17 @@ __device__ __forceinline__ float reduce_scatter4(float v0, float v1, float v2, f
 // Stage s of a work item is the CTA's stage g0 + s overall: buffer and
 // mbarrier (g0 + s) & 1, wait parity ((g0 + s) >> 1) & 1, so a persistent
 // CTA keeps alternating its two barriers across items.
-struct Stager {
+template <int kST = kStageTiles>
+struct StagerT {
   const int32_t* jlist;
   int j_begin, j_end, n_stages;
   uint64_t* bar;
   uint32_t g0;
   template <int kArrays>
-  __device__ __forceinline__ void issue(int s, float (*buf)[kArrays][kStageFloats], const float* const* src) const {
+  __device__ __forceinline__ void issue(int s, float (*buf)[kArrays][kST * 128], const float* const* src) const {
     const int b = (g0 + s) & 1;
-    const int t0 = j_begin + s * kStageTiles;
-    const int cnt = min(kStageTiles, j_end - t0);
+    const int t0 = j_begin + s * kST;
+    const int cnt = min(kST, j_end - t0);
     mbar_arrive_expect_tx(&bar[b], static_cast<uint32_t>(cnt) * kTileBytes * kArrays);
     for (int t = 0; t < cnt; ++t) {
       const size_t base = static_cast<size_t>(jlist[t0 + t]) * 128;
@@ -107,11 +108,13 @@ struct Stager {
   }
 };
 
+using Stager = StagerT<>;
+
 // Adds the stage's j partials (s_part[w][c][q], summed over warps in a fixed
 // order) to the fixed-point accumulators.
-template <int W, int kComps>
+template <int W, int kComps, int kST = kStageTiles>
 __device__ __forceinline__ void flush_j(const PairArgs& a, const int32_t* jlist, int t0, int cnt,
-                                        float (*s_part)[kComps][kStageTiles * kTile], unsigned long long* const* dst,
+                                        float (*s_part)[kComps][kST * kTile], unsigned long long* const* dst,
                                         double scale) {
   for (int q = threadIdx.x; q < cnt * kTile; q += blockDim.x) {
     const int j = jlist[t0 + q / kTile] * kTile + (q % kTile);
@@ -526,11 +529,18 @@ OG_UNROLL(OG_FORCE_UNROLL)
 // Sums and their order per i atom and per j atom are as in k_force's
 // structure: FP32 per j-tile and 4-atom group, FP64 across tiles, warps
 // summed in a fixed order, fixed point at the end.
+// Four-warp blocks stage six j-tiles at a time (four in the other pair
+// kernels): two block-wide barriers per stage, so a third fewer per pair;
+// eight-warp blocks keep four, within the 48 KB of static shared memory.
+template <int W>
+constexpr int ip_stage_tiles() { return W <= 4 ? 6 : kStageTiles; }
+
 template <bool kAllPairs, int W, int kMinBlocks, bool kPersistent>
 __global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
-  __shared__ __align__(128) float s_buf[2][3][kStageFloats];   // raw columns of pq, lj, gb (TMA)
-  __shared__ __align__(16) float s_dup[3][2 * kStageFloats];    // the stage's columns, each value twice
-  __shared__ float s_part[W][3][kStageTiles * kTile];
+  constexpr int kST = ip_stage_tiles<W>();
+  __shared__ __align__(128) float s_buf[2][3][kST * 128];   // raw columns of pq, lj, gb (TMA)
+  __shared__ __align__(16) float s_dup[3][2 * kST * 128];    // the stage's columns, each value twice
+  __shared__ float s_part[W][3][kST * kTile];
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ int s_item;
 
@@ -547,7 +557,7 @@ __global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
   PairWork w = a.work[item];
   if (a.seg_end) w.j_end = min(w.j_end, a.seg_end[w.i_tile0]);
   if (w.j_begin >= w.j_end) continue;  // chunk culled by the cutoff (block-uniform)
-  const Stager st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kStageTiles - 1) / kStageTiles, s_bar, g};
+  const StagerT<kST> st{a.jlist, w.j_begin, w.j_end, (w.j_end - w.j_begin + kST - 1) / kST, s_bar, g};
   const float* src[3] = {a.pq, a.lj, a.gb};
   if (threadIdx.x == 0) {
     if (st.n_stages > 0) st.issue<3>(0, s_buf, src);
@@ -588,8 +598,8 @@ __global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
       if (threadIdx.x == 0) atomicOr(a.error_flag, kStatusTimeout);
       return;
     }
-    const int t0 = w.j_begin + s * kStageTiles;
-    const int cnt = min(kStageTiles, w.j_end - t0);
+    const int t0 = w.j_begin + s * kST;
+    const int cnt = min(kST, w.j_end - t0);
     // expand the stage's columns: value q of an array to entries 2q, 2q + 1
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -687,7 +697,7 @@ __global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
     }
     __syncthreads();  // every warp is done with s_dup and has written its j partials
     unsigned long long* dst[3] = {a.fx, a.fy, a.fz};
-    flush_j<W, 3>(a, a.jlist, t0, cnt, s_part, dst, kForceScale);
+    flush_j<W, 3, kST>(a, a.jlist, t0, cnt, s_part, dst, kForceScale);
   }
   g += st.n_stages;
   if (act_a && a.atom_valid[i_a]) {
