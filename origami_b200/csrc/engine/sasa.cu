@@ -988,12 +988,10 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
         } else {
           const Cap ck = cap_at(w, k);
           const double sk = w.bsk[j];
-          double ccw = atan2(sin_ccw, cos_ccw);
-          if (ccw <= 0.0) ccw += 2.0 * kPi;
           const int v = n_verts + __popc(exv & below);
           const D3 pb = circle_point(ck, sk, tpoint(w, sbn)), pa = circle_point(ck, sk, tpoint(w, sa));
           w.a_full[e] = 0;
-          w.a_theta[e] = -ccw;
+          w.a_theta[e] = 0.0;  // the ccw angle, taken below for all arcs at once
           w.a_sx[e] = pb.x;
           w.a_sy[e] = pb.y;
           w.a_sz[e] = pb.z;
@@ -1013,6 +1011,22 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     b0 = b1;
   }
   if (bad) return kInvalid;
+  __syncwarp();
+  // The arcs' ccw angles from their end points (the exposure rounds hold an
+  // exposed segment or two each, so the arc tangents run side by side here
+  // instead of one lane at a time there): the cosine and sine of the angle
+  // from p_start - a c to p_end - a c about the axis, as segment_midpoint
+  // takes them from the unit radial directions, up to a positive factor.
+  for (int e = lane; e < n_arcs; e += 32) {
+    if (w.a_full[e]) continue;
+    const Cap ck = cap_at(w, w.a_cap[e]);
+    const int v = w.a_own[e];
+    const D3 c0 = ck.axis * ck.c;
+    const D3 ua = D3{w.v_x[v], w.v_y[v], w.v_z[v]} - c0, ub = D3{w.a_sx[e], w.a_sy[e], w.a_sz[e]} - c0;
+    double ccw = atan2(dot(ck.axis, cross(ua, ub)), dot(ua, ub));
+    if (ccw <= 0.0) ccw += 2.0 * kPi;
+    w.a_theta[e] = -ccw;
+  }
   __syncwarp();
   *n_arcs_out = n_arcs;
   *n_verts_out = n_verts;
@@ -1172,7 +1186,7 @@ __global__ void __maxnreg__(168) k_sasa_boundary_big(SasaArgs a) {
 }
 
 // Force path, stage 2: one term per thread, F_x += gamma_i R_i^2 dTerm/dr_x.
-__global__ void __launch_bounds__(128) k_sasa_terms(SasaArgs a) {
+__global__ void __launch_bounds__(128, 4) k_sasa_terms(SasaArgs a) {
   const int n_arc = min(a.counts[0], a.term_cap), n_vert = min(a.counts[1], a.term_cap);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_arc + n_vert; t += gridDim.x * blockDim.x) {
     D3 gi = {0.0, 0.0, 0.0}, g1 = gi, g2 = gi, g3 = gi;
