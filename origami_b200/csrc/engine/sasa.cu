@@ -173,7 +173,7 @@ __device__ __forceinline__ D3 helper_axis(D3 axis) {
   return {0.0, 0.0, 1.0};
 }
 
-__device__ D3 sample_circle_point(Cap c) {
+__device__ __noinline__ D3 sample_circle_point(Cap c) {
   const D3 h = helper_axis(c.axis);
   const D3 perp = normalize(h - c.axis * dot(h, c.axis));
   return c.axis * c.c + perp * sqrt(fmax(1.0 - c.c * c.c, 0.0));
@@ -347,7 +347,7 @@ __device__ __forceinline__ D3 circle_point(Cap ck, double sk, D3 u) { return ck.
 // (ccw < 1e-9); else the exposure test point *mid (ua rotated by half the ccw
 // angle, midpoint_on_circle) and the cosine / sine of the ccw angle.
 // single = the circle's only transition (the whole circle, ccw = 2 pi).
-__device__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D3* mid, double* cos_ccw,
+__device__ __noinline__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D3* mid, double* cos_ccw,
                                  double* sin_ccw) {
   if (single) {
     *cos_ccw = 1.0;
@@ -372,6 +372,49 @@ __device__ bool segment_midpoint(D3 ua, D3 ub, Cap ck, double sk, bool single, D
   }
   *mid = circle_point(ck, sk, ua * ch + cross(ck.axis, ua) * sh);
   return true;
+}
+
+// Rarely taken parts of the arrangement, kept out of line so that they do
+// not weigh on the register allocation of the loops around them.
+// The circles of `tied` (a bit per batch circle) ordered from the FP64
+// angles of their transitions, ties in slot order.
+template <class W>
+__device__ __noinline__ void reorder_tied(W& w, unsigned tied, int b0, int lane) {
+  while (tied) {
+    const int j = __ffs(tied) - 1;
+    tied &= tied - 1;
+    const int sb = w.sbeg[j], se = w.sbeg[j + 1];
+    D3 fu, fv;
+    slot_frame(cap_at(w, w.live[b0 + j]).axis, &fu, &fv);
+    for (int sl = sb + lane; sl < se; sl += 32) {
+      const double as = slot_angle(tpoint(w, sl), fu, fv);
+      int rank = 0;
+      for (int t = sb; t < se; ++t) {
+        const double at = slot_angle(tpoint(w, t), fu, fv);
+        rank += (at < as || (at == as && t < sl)) ? 1 : 0;
+      }
+      rank = min(rank, se - sb - 1);
+      w.torder[sb + rank] = static_cast<uint8_t>(sl);
+      w.trank[sl] = static_cast<uint8_t>(rank);
+    }
+  }
+}
+
+// Consecutive duplicates dropped from each batch circle's sorted order
+// (|dp|^2 < 1e-12 against the last kept entry), one lane.
+template <class W>
+__device__ __noinline__ void compact_duplicates(W& w, int nb) {
+  for (int j = 0; j < nb; ++j) {
+    const int sb = w.sbeg[j], se = w.sbeg[j + 1];
+    const double sk2 = w.bsk[j] * w.bsk[j];
+    int kept = 0;
+    for (int r = sb; r < se; ++r) {
+      const int sl = w.torder[r];
+      if (kept == 0 || norm2(tpoint(w, sl) - tpoint(w, w.torder[sb + kept - 1])) * sk2 >= 1e-12)
+        w.torder[sb + kept++] = static_cast<uint8_t>(sl);
+    }
+    w.skept[j] = static_cast<uint8_t>(kept);
+  }
 }
 
 // Builds caps and the exposed boundary of atom i in w.  Returns the outcome;
@@ -866,24 +909,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
         w.bmode[lane] = (circle_tally(w, b0 + lane, masks) & kContained) ? 1 : 0;
         w.bbase[lane] = 0;
       }
-      while (tied) {
-        const int j = __ffs(tied) - 1;
-        tied &= tied - 1;
-        const int sb = w.sbeg[j], se = w.sbeg[j + 1];
-        D3 fu, fv;
-        slot_frame(cap_at(w, w.live[b0 + j]).axis, &fu, &fv);
-        for (int sl = sb + lane; sl < se; sl += 32) {
-          const double as = slot_angle(tpoint(w, sl), fu, fv);
-          int rank = 0;
-          for (int t = sb; t < se; ++t) {
-            const double at = slot_angle(tpoint(w, t), fu, fv);
-            rank += (at < as || (at == as && t < sl)) ? 1 : 0;
-          }
-          rank = min(rank, se - sb - 1);
-          w.torder[sb + rank] = static_cast<uint8_t>(sl);
-          w.trank[sl] = static_cast<uint8_t>(rank);
-        }
-      }
+      reorder_tied(w, tied, b0, lane);
       __syncwarp();
     }
 
@@ -898,19 +924,7 @@ __device__ int build_boundary(const SasaArgs& a, W& w, int i, int lane, int* n_a
     // cap.
     __syncwarp();
     if (__any_sync(kFull, dup)) {
-      if (lane == 0) {
-        for (int j = 0; j < nb; ++j) {
-          const int sb = w.sbeg[j], se = w.sbeg[j + 1];
-          const double sk2 = w.bsk[j] * w.bsk[j];
-          int kept = 0;
-          for (int r = sb; r < se; ++r) {
-            const int sl = w.torder[r];
-            if (kept == 0 || norm2(tpoint(w, sl) - tpoint(w, w.torder[sb + kept - 1])) * sk2 >= 1e-12)
-              w.torder[sb + kept++] = static_cast<uint8_t>(sl);
-          }
-          w.skept[j] = static_cast<uint8_t>(kept);
-        }
-      }
+      if (lane == 0) compact_duplicates(w, nb);
     } else {
       for (int j = lane; j < nb; j += 32) w.skept[j] = static_cast<uint8_t>(w.sbeg[j + 1] - w.sbeg[j]);
     }
