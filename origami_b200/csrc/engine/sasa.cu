@@ -258,7 +258,7 @@ struct WarpSmemT {
     uint64_t xmask[kCaps / 2];
   };
   // transitions of the batch of circles being processed: unit radial
-  // direction, sort key (quantised angle and slot, slot_key), the other
+  // direction, sort key (quantised angle over the slot, SlotKey), the other
   // cap, the batch circle, the sorted order and each entry's rank in it
   double tx[kTrans], ty[kTrans], tz[kTrans];
   uint32_t tkey[kTrans];
