@@ -529,15 +529,16 @@ OG_UNROLL(OG_FORCE_UNROLL)
 // Sums and their order per i atom and per j atom are as in k_force's
 // structure: FP32 per j-tile and 4-atom group, FP64 across tiles, warps
 // summed in a fixed order, fixed point at the end.
-// Four-warp blocks stage six j-tiles at a time (four in the other pair
-// kernels): two block-wide barriers per stage, so a third fewer per pair;
-// eight-warp blocks keep four, within the 48 KB of static shared memory.
-template <int W>
-constexpr int ip_stage_tiles() { return W <= 4 ? 6 : kStageTiles; }
+// Four-warp blocks at up to four per SM stage six j-tiles at a time (four in
+// the other pair kernels): two block-wide barriers per stage, so a third
+// fewer per pair; eight-warp blocks keep four, within the 48 KB of static
+// shared memory, and so do five four-warp blocks per SM, within the SM's.
+template <int W, int kMinBlocks>
+constexpr int ip_stage_tiles() { return W <= 4 && kMinBlocks <= 4 ? 6 : kStageTiles; }
 
 template <bool kAllPairs, int W, int kMinBlocks, bool kPersistent>
 __global__ void __launch_bounds__(W * 32, kMinBlocks) k_force_ip(PairArgs a) {
-  constexpr int kST = ip_stage_tiles<W>();
+  constexpr int kST = ip_stage_tiles<W, kMinBlocks>();
   __shared__ __align__(128) float s_buf[2][3][kST * 128];   // raw columns of pq, lj, gb (TMA)
   __shared__ __align__(16) float s_dup[3][2 * kST * 128];    // the stage's columns, each value twice
   __shared__ float s_part[W][3][kST * kTile];
@@ -814,6 +815,7 @@ void force_shape(const PairArgs& a, int shape, cudaStream_t s) {
     case 2: force_variant<AP, 8, 3, P>(a, s); break;
     case 3: force_ip_variant<AP, 8, 2, P>(a, s); break;
     case 4: force_ip_variant<AP, 4, 4, P>(a, s); break;
+    case 5: force_ip_variant<AP, 4, 5, P>(a, s); break;
     default: force_variant<AP, 8, 2, P>(a, s); break;
   }
 }
