@@ -377,11 +377,11 @@ og_status og_compute_sasa(og_engine* e, int32_t sys, int32_t method, int32_t n_d
  *               per CTA at twice the CTAs per SM; 2: 8 i-tiles at 3 CTAs/SM;
  *               force pass only: 3: two i-tiles per warp, 16 per CTA at 2
  *               CTAs/SM; 4: two i-tiles per warp, 8 per CTA at 4 CTAs/SM;
- *               5: as 4 at 5 CTAs/SM
+ *               5, 6: as 4 at 5 or 6 CTAs/SM
  *   persistent  0: one CTA per work item; 1: resident CTAs taking items from
  *               an atomic work queue
  *   chunk       j-tiles per work item (default 16)
- * og_engine_autotune times every combination (3 Born / 6 force shapes x 2 x
+ * og_engine_autotune times every combination (3 Born / 7 force shapes x 2 x
  * chunks 8, 16, 32) of each pass on the engine's systems at their current positions and
  * keeps the fastest; the choice is cached in the JSON file cache_path (NULL
  * = no cache) under the workload's bucket (mode, total 32-atom tiles and

@@ -2304,7 +2304,7 @@ og_status og_engine_set_pair_launch(og_engine* e, int32_t pass, int32_t shape, i
   if (s != OG_OK) return s;
   if ((pass != 0 && pass != 1) || !valid_launch(pass, shape, persistent, chunk))
     return og_fail(OG_E_BADARG,
-                   "og_engine_set_pair_launch: pass 0/1, shape 0..2 (Born) or 0..5 (force), persistent 0/1, chunk >= 1");
+                   "og_engine_set_pair_launch: pass 0/1, shape 0..2 (Born) or 0..6 (force), persistent 0/1, chunk >= 1");
   TuneEntry t{{e->born_launch.shape, e->born_launch.persistent ? 1 : 0, e->chunk_b},
               {e->force_launch.shape, e->force_launch.persistent ? 1 : 0, e->chunk_f}, 0.0, 0.0};
   int* dst = pass == 0 ? t.b : t.f;

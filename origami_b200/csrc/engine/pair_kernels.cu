@@ -816,6 +816,7 @@ void force_shape(const PairArgs& a, int shape, cudaStream_t s) {
     case 3: force_ip_variant<AP, 8, 2, P>(a, s); break;
     case 4: force_ip_variant<AP, 4, 4, P>(a, s); break;
     case 5: force_ip_variant<AP, 4, 5, P>(a, s); break;
+    case 6: force_ip_variant<AP, 4, 6, P>(a, s); break;
     default: force_variant<AP, 8, 2, P>(a, s); break;
   }
 }

@@ -91,7 +91,7 @@ void launch_cut_lists(const CutBlock* blocks, int32_t n_blocks, const int32_t* j
 // per CTA (128 atoms) at twice the CTAs, 2 = 8 i-tiles at 3 CTAs/SM; force
 // pass only: 3 = two i-tiles per warp (k_force_ip), 8 warps, 16 i-tiles per
 // CTA at 2 CTAs/SM, 4 = the same with 4 warps (8 i-tiles) at 4 CTAs/SM, 5 =
-// 4 warps at 5 CTAs/SM (96 registers);
+// 4 warps at 5 CTAs/SM (96 registers), 6 = at 6 CTAs/SM (80 registers);
 // persistent: resident CTAs taking items from PairArgs::queue instead of
 // one CTA per item.  The work list must be built for
 // pair_shape_tiles(shape) i-tiles per item.
@@ -101,7 +101,7 @@ struct PairLaunch {
 };
 int pair_shape_tiles(int shape);
 constexpr int kBornShapes = 3;   // shapes 0..2
-constexpr int kForceShapes = 6;  // shapes 0..5
+constexpr int kForceShapes = 7;  // shapes 0..6
 
 void launch_born_pass(const PairArgs& a, const PairLaunch& c, cudaStream_t s);
 // Far field (tiles without exclusion masks), FP32.

@@ -56,7 +56,7 @@ def test_pair_launch_variants_match_oracle(origami, mode):
     cut = (INF, INF, INF) if mode == "all_pairs" else (10.0, 20.0, 10.0)
     eng, chains, xs = _uneven_batch(origami, params)
     refs = [Orc(c).total_force(x, *cut) for c, x in zip(chains, xs)]
-    for shape in (0, 1, 2, 3, 4, 5):
+    for shape in (0, 1, 2, 3, 4, 5, 6):
         for chunk in (8, 32):
             got = {}
             for persistent in (False, True):
@@ -75,7 +75,7 @@ def test_autotune_picks_a_variant_and_caches_it(origami, tmp_path):
     eng, chains, xs = _uneven_batch(origami, origami.Params.all_pairs())
     r = eng.autotune(cache)
     assert r["from_cache"] == 0
-    assert 0 <= r["born_shape"] <= 2 and 0 <= r["force_shape"] <= 5
+    assert 0 <= r["born_shape"] <= 2 and 0 <= r["force_shape"] <= 6
     assert r["born_chunk"] in (8, 16, 32) and r["force_chunk"] in (8, 16, 32)
     # the chosen variant is the fastest timed, so no slower than the default
     assert r["born_ms"] <= r["born_ms_default"] and r["force_ms"] <= r["force_ms_default"]
