@@ -215,6 +215,28 @@ og_status og_engine_create(const og_params* params, og_engine** out);
 og_status og_engine_add_system(og_engine* e, const og_topology* topo, const double* xyz,
                                double temperature_k, int32_t* system_index);
 og_status og_engine_finalize(og_engine* e);
+/* Co-translational growth in place: replaces the per-slice rebuild of
+ * run_slice (cotranslate.rs:318-319, ForceScratch::new, scratch.rs:196-251).
+ * System `sys` -- the engine's last -- takes the atoms and terms that
+ * `grown` adds to its topology (the topology of the same chain after
+ * og_chain_append; og_topology_extends states the rule).  xyz_new holds
+ * the new atoms' positions, v_new their velocities (NULL = zero), 3 doubles
+ * per new atom.  Only the new atoms' data crosses to the device: their
+ * parameters, the exclusion-mask blocks and rows their exclusions reach,
+ * their bonded terms and SHAKE clusters (appended), the system's atom count
+ * and degrees of freedom; the existing atoms' positions, velocities and the
+ * step count stay on the device.  Device arrays grow by half again when
+ * full; the step graph is re-captured at the next og_step.  The force and
+ * energy results equal those of an engine built from `grown` (forces bit
+ * for bit).  OG_E_BADARG when `grown` does not extend the system. */
+og_status og_engine_append_atoms(og_engine* e, int32_t sys, const og_topology* grown, const double* xyz_new,
+                                 const double* v_new);
+/* Host-only check (no GPU): *extends = 1 when `grown` extends `base` --
+ * more atoms; the first base->n_atoms with bit-identical parameters; in
+ * each term list (bonds, angles, dihedrals with their terms, impropers,
+ * exclusions, constraints) the records among those atoms equal to base's
+ * records, in base's order -- else 0, with the reason in og_last_error. */
+og_status og_topology_extends(const og_topology* base, const og_topology* grown, int32_t* extends);
 og_status og_engine_n_systems(const og_engine* e, int32_t* n);
 /* Runs kernels on this CUDA stream (cudaStream_t as void*; NULL = the
  * engine's own stream). */

@@ -179,6 +179,24 @@ def build_extended_chain(sequence: str) -> Chain:
     return Chain.build(sequence)
 
 
+def topology_extends(base, grown) -> tuple[bool, str]:
+    """Whether `grown` (Chain or Topology) extends `base` so that an engine
+    system built from base can take it by Engine.append_atoms, and if not,
+    why (og_topology_extends; host only)."""
+    keep = []
+
+    def ptr(t):
+        if isinstance(t, Chain):
+            return t.topology_ptr()
+        s = t.to_struct()
+        keep.append(s)
+        return C.pointer(s)
+
+    ok = C.c_int32()
+    _check(lib().og_topology_extends(ptr(base), ptr(grown), C.byref(ok)))
+    return bool(ok.value), ("" if ok.value else lib().og_last_error().decode())
+
+
 @dataclass
 class Topology:
     """NumPy copy of an og_topology (per-atom params, term lists, exclusions)."""
@@ -352,6 +370,23 @@ class Engine:
         _check(lib().og_engine_finalize(self._h))
         self._finalized = True
         return self
+
+    def append_atoms(self, sys: int, grown, xyz_new: np.ndarray, v_new: np.ndarray | None = None) -> None:
+        """Grow system `sys` (the last) in place to the topology `grown`
+        (a Chain after Chain.append, or a Topology) that extends it; xyz_new
+        and v_new (None = zero) hold the new atoms only (og_engine_append_atoms)."""
+        tp = grown.topology_ptr() if isinstance(grown, Chain) else C.pointer(grown.to_struct())
+        x = np.ascontiguousarray(xyz_new, dtype=np.float64).reshape(-1, 3)
+        vp = None
+        if v_new is not None:
+            v = np.ascontiguousarray(v_new, dtype=np.float64).reshape(-1, 3)
+            if v.shape != x.shape:
+                raise ValueError("velocity and position arrays differ in shape")
+            vp = _dptr(v)
+        if self._n_atoms[sys] + x.shape[0] != tp.contents.n_atoms:
+            raise ValueError("xyz_new must hold exactly the new atoms")
+        _check(lib().og_engine_append_atoms(self._h, sys, tp, _dptr(x), vp))
+        self._n_atoms[sys] += x.shape[0]
 
     @property
     def n_systems(self) -> int:

@@ -114,6 +114,8 @@ SIGNATURES = [
     ("og_engine_create", C.c_int, [C.POINTER(og_params), C.POINTER(C.c_void_p)]),
     ("og_engine_add_system", C.c_int, [C.c_void_p, C.POINTER(og_topology), c_double_p, C.c_double, c_int32_p]),
     ("og_engine_finalize", C.c_int, [C.c_void_p]),
+    ("og_engine_append_atoms", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(og_topology), c_double_p, c_double_p]),
+    ("og_topology_extends", C.c_int, [C.POINTER(og_topology), C.POINTER(og_topology), c_int32_p]),
     ("og_engine_n_systems", C.c_int, [C.c_void_p, c_int32_p]),
     ("og_engine_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
     ("og_engine_synchronize", C.c_int, [C.c_void_p]),

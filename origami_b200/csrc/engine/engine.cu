@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <numeric>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -52,16 +53,18 @@ og_status cuda_fail(cudaError_t e, const char* what) {
 template <class T>
 struct DVec {
   T* p = nullptr;
-  size_t n = 0;
+  size_t n = 0, cap = 0;
   ~DVec() { release(); }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
+    cap = 0;
   }
   cudaError_t alloc(size_t count) {
     release();
     n = count;
+    cap = count;
     if (count == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
     // OG_DEBUG_POISON=1 fills new buffers with 0xFF bytes (NaN as float or
@@ -83,6 +86,36 @@ struct DVec {
     cudaError_t e = alloc(h.size());
     if (e != cudaSuccess || h.empty()) return e;
     return cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+  // Resizes to `count` elements keeping the first min(n, count) on the
+  // device; a larger buffer (half again as large, so that a run of small
+  // appends reallocates rarely) is made only when the capacity is exceeded.
+  cudaError_t grow(size_t count, cudaStream_t s) {
+    if (count <= cap && p) {
+      n = count;
+      return cudaSuccess;
+    }
+    DVec<T> fresh;
+    cudaError_t e = fresh.alloc(std::max(count, cap + cap / 2));
+    if (e == cudaSuccess && n > 0)
+      e = cudaMemcpyAsync(fresh.p, p, n * sizeof(T), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the old buffer is read until here
+    if (e != cudaSuccess) return e;
+    std::swap(p, fresh.p);
+    std::swap(cap, fresh.cap);
+    n = count;
+    return cudaSuccess;  // `fresh` frees the old buffer
+  }
+  // h[from, h.size()) to the same positions on the device (grown to
+  // h.size() elements first); h[0, from) is taken to be there already.
+  cudaError_t upload_tail(const std::vector<T>& h, size_t from, cudaStream_t s) {
+    cudaError_t e = grow(h.size(), s);
+    if (e != cudaSuccess || from >= h.size()) return e;
+    return cudaMemcpyAsync(p + from, h.data() + from, (h.size() - from) * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+  cudaError_t upload_range(const std::vector<T>& h, size_t from, size_t to, cudaStream_t s) {
+    if (from >= to) return cudaSuccess;
+    return cudaMemcpyAsync(p + from, h.data() + from, (to - from) * sizeof(T), cudaMemcpyHostToDevice, s);
   }
 };
 
@@ -188,6 +221,21 @@ struct og_engine {
   DVec<int32_t> excl_row, excl_col;
   DVec<int8_t> excl_kind;
   DVec<int4> near;
+  // Host side of the exclusion tables, kept so that an append
+  // (og_engine_append_atoms) adds only the new exclusions' bits: mask block
+  // of each ordered tile pair, the blocks' words, per-tile block references
+  // (sorted by j tile) and their CSR, per-atom exclusion rows and their CSR,
+  // the unordered near-field block list.
+  std::map<std::pair<int, int>, int> mask_of;
+  std::vector<uint32_t> h_mex, h_m14;
+  std::vector<std::vector<ogk::TileMaskRef>> tile_refs;
+  std::vector<int32_t> h_mask_begin;
+  std::vector<ogk::TileMaskRef> h_mask_refs;
+  std::vector<std::vector<std::pair<int, int8_t>>> excl_rows;
+  std::vector<int32_t> h_excl_row, h_excl_col;
+  std::vector<int8_t> h_excl_kind;
+  std::vector<int4> h_near;
+  int n_terms = 0;  // dihedral Fourier terms on the device
   DVec<ogk::PairWork> work_f;   // far-field force: upper-triangle tile pairs
   DVec<int32_t> jlist_f;
   // cutoff mode: i-blocks of the two lists, their culled j lists and ends
@@ -793,6 +841,413 @@ og_status build_pair_lists(og_engine* e, cudaStream_t st) {
                          &e->jlist_f, &e->cut_f, &e->n_cut_f, &e->jlist_cut_f, &e->seg_end_f, st);
 }
 
+template <class T>
+cudaError_t put(DVec<T>& d, size_t at, const std::vector<T>& h, cudaStream_t st) {
+  if (h.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(d.p + at, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// Appends h to the device array (grown to n + h.size() elements).
+template <class T>
+cudaError_t append(DVec<T>& d, const std::vector<T>& h, cudaStream_t st) {
+  const size_t at = d.n;
+  cudaError_t e = d.grow(at + h.size(), st);
+  if (e != cudaSuccess || h.empty()) return e;
+  return cudaMemcpyAsync(d.p + at, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// The system owning padded atom i (-1 for padding past the last system).
+int system_of(const og_engine* e, int i) {
+  auto it = std::upper_bound(e->sys.begin(), e->sys.end(), i,
+                             [](int v, const SysHost& s) { return v < s.atom_begin; });
+  if (it == e->sys.begin()) return -1;
+  const int si = static_cast<int>(it - e->sys.begin()) - 1;
+  return i < e->sys[si].atom_begin + e->sys[si].topo.n ? si : -1;
+}
+
+// Static per-atom tables of the padded atoms [a0, a1), a0 on a tile
+// boundary: force-field parameters, the tile-SoA LJ and GB columns, owner
+// system, local index and valid flag, the SASA radius (Bondi vdW + 1.4 A
+// probe) and surface tension (0.005 kcal/mol/A^2 on C and S,
+// powersasa/mod.rs:27-52, times sasa_gamma_scale, analytical.rs:607-614),
+// and the learned-radius descriptor class (C,S -> 0; N,P -> 1; O -> 2;
+// H -> 3).  Padding atoms get unit mass, no charge and R = rho~ = 1.  The
+// device arrays must hold at least a1 atoms.
+og_status fill_atoms(og_engine* e, int a0, int a1, cudaStream_t st) {
+  static const double kVdw[6] = {1.20, 1.70, 1.55, 1.52, 1.80, 1.80};
+  static const int32_t kClass[6] = {3, 0, 1, 2, 1, 0};
+  const double g_cs = 0.005 * ogk::kKcalToKj * e->p.sasa_gamma_scale;
+  const size_t m = static_cast<size_t>(a1 - a0);
+  std::vector<double> hm(m, 1.0), him(m, 1.0), hq(m, 0.0), hrm(m, 0.0), hep(m, 0.0), hrm14(m, 0.0),
+      hep14(m, 0.0), hrho(m, 1.0), hrt(m, 1.0), hsr(m, 0.0), hr(m, 0.0), hg(m, 0.0);
+  std::vector<int32_t> hsys(m, -1), hloc(m, 0), hvalid(m, 0), hcls(m, 0);
+  std::vector<float> hlj(4 * m, 0.0f), hgb(4 * m);
+  for (size_t r = 0; r < m; ++r) {
+    const int i = a0 + static_cast<int>(r);
+    const int si = system_of(e, i);
+    if (si >= 0) {
+      const TopoCopy& t = e->sys[si].topo;
+      const int k = i - e->sys[si].atom_begin;
+      const int el = t.element[k];
+      if (el < 0 || el > 5) return og_fail(OG_E_BADARG, "element code out of range");
+      hm[r] = t.mass[k];
+      him[r] = 1.0 / t.mass[k];
+      hq[r] = t.charge[k];
+      hrm[r] = t.rmin[k];
+      hep[r] = t.eps[k];
+      hrm14[r] = t.rmin14[k];
+      hep14[r] = t.eps14[k];
+      hrho[r] = t.rho[k];
+      hrt[r] = t.rho[k] - ogk::kObcOffset;
+      hsr[r] = t.scale[k] * hrt[r];
+      hsys[r] = si;
+      hloc[r] = k;
+      hvalid[r] = 1;
+      hr[r] = kVdw[el] + 1.4;
+      hg[r] = (el == 1 || el == 5) ? g_cs : 0.0;
+      hcls[r] = kClass[el];
+    }
+    const int ri = static_cast<int>(r);
+    hlj[ogk::soa_index(ri, 0)] = static_cast<float>(hrm[r]);
+    hlj[ogk::soa_index(ri, 1)] = static_cast<float>(std::sqrt(hep[r]));
+    hlj[ogk::soa_index(ri, 2)] = static_cast<float>(hrm14[r]);
+    hlj[ogk::soa_index(ri, 3)] = static_cast<float>(std::sqrt(hep14[r]));
+    // The Born pass reads rho~ and s*rho~ before the first radii exist, so
+    // the gb columns start out fully defined (R = rho~ until then).
+    const bool real = si >= 0;
+    hgb[ogk::soa_index(ri, 0)] = real ? static_cast<float>(hrt[r]) : 1.0f;
+    hgb[ogk::soa_index(ri, 1)] = real ? static_cast<float>(1.0 / hrt[r]) : 1.0f;
+    hgb[ogk::soa_index(ri, 2)] = real ? static_cast<float>(hrt[r]) : 1.0f;
+    hgb[ogk::soa_index(ri, 3)] = real ? static_cast<float>(hsr[r]) : 0.0f;
+  }
+  OG_CUDA(put(e->mass, a0, hm, st)); OG_CUDA(put(e->inv_mass, a0, him, st)); OG_CUDA(put(e->q, a0, hq, st));
+  OG_CUDA(put(e->rmin, a0, hrm, st)); OG_CUDA(put(e->eps, a0, hep, st));
+  OG_CUDA(put(e->rmin14, a0, hrm14, st)); OG_CUDA(put(e->eps14, a0, hep14, st));
+  OG_CUDA(put(e->rho, a0, hrho, st)); OG_CUDA(put(e->rho_tilde, a0, hrt, st)); OG_CUDA(put(e->srho, a0, hsr, st));
+  OG_CUDA(put(e->atom_sys, a0, hsys, st)); OG_CUDA(put(e->local_idx, a0, hloc, st));
+  OG_CUDA(put(e->atom_valid, a0, hvalid, st));
+  OG_CUDA(put(e->lj, 4 * static_cast<size_t>(a0), hlj, st));
+  OG_CUDA(put(e->gb, 4 * static_cast<size_t>(a0), hgb, st));
+  OG_CUDA(put(e->sasa_r, a0, hr, st)); OG_CUDA(put(e->sasa_gamma, a0, hg, st));
+  OG_CUDA(put(e->lgb_class, a0, hcls, st));
+  for (double v : hr) e->sasa_rmax = std::max(e->sasa_rmax, v);
+  return OG_OK;
+}
+
+// Positions of the padded atoms [a0, a1) from the systems' host copies
+// (0 for padding); velocities and SHAKE reference positions zero.
+og_status fill_positions(og_engine* e, int a0, int a1, cudaStream_t st) {
+  const size_t m = static_cast<size_t>(a1 - a0);
+  std::vector<double> hx(m, 0.0), hy(m, 0.0), hz(m, 0.0), zeros(m, 0.0);
+  for (size_t r = 0; r < m; ++r) {
+    const int i = a0 + static_cast<int>(r);
+    const int si = system_of(e, i);
+    if (si < 0) continue;
+    const int k = i - e->sys[si].atom_begin;
+    hx[r] = e->sys[si].xyz[3 * k];
+    hy[r] = e->sys[si].xyz[3 * k + 1];
+    hz[r] = e->sys[si].xyz[3 * k + 2];
+  }
+  OG_CUDA(put(e->x, a0, hx, st)); OG_CUDA(put(e->y, a0, hy, st)); OG_CUDA(put(e->z, a0, hz, st));
+  for (auto* v : {&e->vx, &e->vy, &e->vz, &e->rx, &e->ry, &e->rz}) OG_CUDA(put(*v, a0, zeros, st));
+  return OG_OK;
+}
+
+// SASA task lists of system si's atoms [k0, k1): atoms with non-zero
+// tension (force and energy tasks) and every real atom (area queries).
+void sasa_lists(const og_engine* e, int si, int k0, int k1, std::vector<int32_t>* tasks,
+                std::vector<int32_t>* all) {
+  const SysHost& s = e->sys[si];
+  for (int k = k0; k < k1; ++k) {
+    const int el = s.topo.element[k];
+    all->push_back(s.atom_begin + k);
+    if (el == 1 || el == 5) tasks->push_back(s.atom_begin + k);
+  }
+}
+
+// ---- exclusion tables.  One 32-word block per ordered tile pair holding an
+// exclusion (bit c of word a: atoms a, c excluded; 1-4 pairs in the second
+// array), each tile's blocks referenced in j-tile order; per-atom exclusion
+// rows for the FP64 paths; the unordered block list of the near field.
+
+// The block of (ti, tj), made (and referenced) when missing; *t_min takes
+// the lowest tile whose reference list changed.
+int mask_block(og_engine* e, int ti, int tj, int* t_min) {
+  auto it = e->mask_of.find({ti, tj});
+  if (it != e->mask_of.end()) return it->second;
+  const int b = static_cast<int>(e->mask_of.size());
+  e->mask_of[{ti, tj}] = b;
+  e->h_mex.resize(static_cast<size_t>(b + 1) * kTile, 0u);
+  e->h_m14.resize(static_cast<size_t>(b + 1) * kTile, 0u);
+  auto& refs = e->tile_refs[ti];
+  auto pos = std::lower_bound(refs.begin(), refs.end(), tj,
+                              [](const ogk::TileMaskRef& r, int j) { return r.j_tile < j; });
+  refs.insert(pos, ogk::TileMaskRef{tj, b});
+  *t_min = std::min(*t_min, ti);
+  if (ti <= tj) e->h_near.push_back(make_int4(ti, tj, b, 0));
+  return b;
+}
+
+// Self pairs of tiles [t0, t1) (every lane of the diagonal block).
+void mask_diagonal(og_engine* e, int t0, int t1, int* t_min, std::set<int>* touched) {
+  for (int t = t0; t < t1; ++t) {
+    const int b = mask_block(e, t, t, t_min);
+    for (int l = 0; l < kTile; ++l) e->h_mex[static_cast<size_t>(b) * kTile + l] |= 1u << l;
+    touched->insert(b);
+  }
+}
+
+// Exclusion k of system si (kind 1: excluded, else a scaled 1-4 pair).
+void mask_exclusion(og_engine* e, int si, size_t k, int* t_min, int* a_min, std::set<int>* touched) {
+  const SysHost& s = e->sys[si];
+  const int i = s.atom_begin + s.topo.excl[2 * k], j = s.atom_begin + s.topo.excl[2 * k + 1];
+  const int8_t kind = s.topo.excl_kind[k];
+  e->excl_rows[i].push_back({j, kind});
+  e->excl_rows[j].push_back({i, kind});
+  *a_min = std::min(*a_min, std::min(i, j));
+  for (int dir = 0; dir < 2; ++dir) {
+    const int a = dir ? j : i, c = dir ? i : j;
+    const int b = mask_block(e, a / kTile, c / kTile, t_min);
+    const size_t w = static_cast<size_t>(b) * kTile + (a % kTile);
+    if (kind == 1) e->h_mex[w] |= 1u << (c % kTile);
+    else e->h_m14[w] |= 1u << (c % kTile);
+    touched->insert(b);
+  }
+}
+
+// Device copies of the exclusion tables after blocks up to n_blocks_before
+// existed on the device: the touched old blocks, the new blocks, the tile
+// CSR from tile t_min on, the atom CSR from atom a_min on and the near-field
+// blocks past n_near_before.
+og_status upload_exclusions(og_engine* e, int n_blocks_before, int t_min, int a_min, int n_near_before,
+                            const std::set<int>& touched, cudaStream_t st) {
+  const int nt = e->n_tiles, np = e->n_padded;
+  // tile CSR
+  t_min = std::min(t_min, std::max(static_cast<int>(e->h_mask_begin.size()) - 1, 0));
+  if (e->h_mask_begin.empty()) t_min = 0;
+  e->h_mask_refs.resize(e->h_mask_begin.empty() ? 0 : e->h_mask_begin[t_min]);
+  e->h_mask_begin.resize(t_min);
+  for (int t = t_min; t < nt; ++t) {
+    e->h_mask_begin.push_back(static_cast<int32_t>(e->h_mask_refs.size()));
+    e->h_mask_refs.insert(e->h_mask_refs.end(), e->tile_refs[t].begin(), e->tile_refs[t].end());
+  }
+  e->h_mask_begin.push_back(static_cast<int32_t>(e->h_mask_refs.size()));
+  OG_CUDA(e->mask_begin.upload_tail(e->h_mask_begin, t_min, st));
+  OG_CUDA(e->mask_refs.upload_tail(e->h_mask_refs, e->h_mask_begin[t_min], st));
+  // blocks
+  OG_CUDA(e->mask_ex.upload_tail(e->h_mex, static_cast<size_t>(n_blocks_before) * kTile, st));
+  OG_CUDA(e->mask_14.upload_tail(e->h_m14, static_cast<size_t>(n_blocks_before) * kTile, st));
+  for (int b : touched)
+    if (b < n_blocks_before) {
+      const size_t w0 = static_cast<size_t>(b) * kTile, w1 = w0 + kTile;
+      OG_CUDA(e->mask_ex.upload_range(e->h_mex, w0, w1, st));
+      OG_CUDA(e->mask_14.upload_range(e->h_m14, w0, w1, st));
+    }
+  e->n_near = static_cast<int>(e->h_near.size());
+  OG_CUDA(e->near.upload_tail(e->h_near, n_near_before, st));
+  // atom CSR (rows sorted by partner)
+  a_min = std::min(a_min, std::max(static_cast<int>(e->h_excl_row.size()) - 1, 0));
+  if (e->h_excl_row.empty()) a_min = 0;
+  e->h_excl_col.resize(e->h_excl_row.empty() ? 0 : e->h_excl_row[a_min]);
+  e->h_excl_kind.resize(e->h_excl_col.size());
+  e->h_excl_row.resize(a_min);
+  for (int i = a_min; i < np; ++i) {
+    auto& r = e->excl_rows[i];
+    std::sort(r.begin(), r.end());
+    e->h_excl_row.push_back(static_cast<int32_t>(e->h_excl_col.size()));
+    for (auto& pr : r) {
+      e->h_excl_col.push_back(pr.first);
+      e->h_excl_kind.push_back(pr.second);
+    }
+  }
+  e->h_excl_row.push_back(static_cast<int32_t>(e->h_excl_col.size()));
+  OG_CUDA(e->excl_row.upload_tail(e->h_excl_row, a_min, st));
+  OG_CUDA(e->excl_col.upload_tail(e->h_excl_col, e->h_excl_row[a_min], st));
+  OG_CUDA(e->excl_kind.upload_tail(e->h_excl_kind, e->h_excl_row[a_min], st));
+  return OG_OK;
+}
+
+// ---- bonded terms of system si (global atom indices, angles in radians),
+// the terms listed in `sel` of each kind, appended to the device lists.
+struct TermSel {
+  std::vector<int> bonds, angles, dihedrals, impropers, excl, cons;
+  static TermSel all(const TopoCopy& t) {
+    TermSel s;
+    auto iota = [](std::vector<int>* v, size_t n) {
+      v->resize(n);
+      for (size_t k = 0; k < n; ++k) (*v)[k] = static_cast<int>(k);
+    };
+    iota(&s.bonds, t.bond_k.size());
+    iota(&s.angles, t.angle_k.size());
+    iota(&s.dihedrals, t.dihedrals.size() / 4);
+    iota(&s.impropers, t.imp_k.size());
+    iota(&s.excl, t.excl_kind.size());
+    iota(&s.cons, t.cons_d.size());
+    return s;
+  }
+};
+
+og_status append_bonded(og_engine* e, int si, const TermSel& sel, cudaStream_t st) {
+  const TopoCopy& t = e->sys[si].topo;
+  const int o = e->sys[si].atom_begin;
+  std::vector<int2> hb, hdt;
+  std::vector<int4> ha, hd, hi;
+  std::vector<double> hbk, hbr, hak, hat, htk, htd, hik, hip;
+  std::vector<int32_t> htn;
+  for (int k : sel.bonds) {
+    hb.push_back(make_int2(o + t.bonds[2 * k], o + t.bonds[2 * k + 1]));
+    hbk.push_back(t.bond_k[k]);
+    hbr.push_back(t.bond_r0[k]);
+  }
+  for (int k : sel.angles) {
+    ha.push_back(make_int4(o + t.angles[3 * k], o + t.angles[3 * k + 1], o + t.angles[3 * k + 2], 0));
+    hak.push_back(t.angle_k[k]);
+    hat.push_back(deg2rad(t.angle_t0[k]));
+  }
+  for (int k : sel.dihedrals) {
+    hd.push_back(make_int4(o + t.dihedrals[4 * k], o + t.dihedrals[4 * k + 1], o + t.dihedrals[4 * k + 2],
+                           o + t.dihedrals[4 * k + 3]));
+    const int base = e->n_terms + static_cast<int>(htk.size());
+    for (int m = t.dih_start[k]; m < t.dih_start[k + 1]; ++m) {
+      htk.push_back(t.term_k[m]);
+      htn.push_back(t.term_n[m]);
+      htd.push_back(deg2rad(t.term_delta[m]));
+    }
+    hdt.push_back(make_int2(base, e->n_terms + static_cast<int>(htk.size())));
+  }
+  for (int k : sel.impropers) {
+    hi.push_back(make_int4(o + t.impropers[4 * k], o + t.impropers[4 * k + 1], o + t.impropers[4 * k + 2],
+                           o + t.impropers[4 * k + 3]));
+    hik.push_back(t.imp_k[k]);
+    hip.push_back(deg2rad(t.imp_psi0[k]));
+  }
+  OG_CUDA(append(e->bond_atoms, hb, st)); OG_CUDA(append(e->bond_k, hbk, st));
+  OG_CUDA(append(e->bond_r0, hbr, st));
+  OG_CUDA(append(e->angle_atoms, ha, st)); OG_CUDA(append(e->angle_k, hak, st));
+  OG_CUDA(append(e->angle_t0, hat, st));
+  OG_CUDA(append(e->dih_atoms, hd, st)); OG_CUDA(append(e->dih_terms, hdt, st));
+  OG_CUDA(append(e->term_k, htk, st)); OG_CUDA(append(e->term_n, htn, st));
+  OG_CUDA(append(e->term_delta, htd, st));
+  OG_CUDA(append(e->imp_atoms, hi, st)); OG_CUDA(append(e->imp_k, hik, st));
+  OG_CUDA(append(e->imp_psi0, hip, st));
+  e->n_bonds += static_cast<int>(hb.size());
+  e->n_angles += static_cast<int>(ha.size());
+  e->n_dih += static_cast<int>(hd.size());
+  e->n_imp += static_cast<int>(hi.size());
+  e->n_terms += static_cast<int>(htk.size());
+  return OG_OK;
+}
+
+// Reduction segments: [atoms | bonds | angles | dihedrals | impropers] per
+// system, the bonded ones as ranges of the bonded energy array (bonds, then
+// angles, dihedrals, impropers); every system's terms of one kind are
+// contiguous, in system order.
+og_status upload_segments(og_engine* e, cudaStream_t st) {
+  const int n_sys = static_cast<int>(e->sys.size());
+  std::vector<int32_t> sb(5 * n_sys), se(5 * n_sys);
+  int ob = 0, oa = e->n_bonds, od = e->n_bonds + e->n_angles, oi = e->n_bonds + e->n_angles + e->n_dih;
+  for (int si = 0; si < n_sys; ++si) {
+    const SysHost& s = e->sys[si];
+    const TopoCopy& t = s.topo;
+    sb[si] = s.atom_begin;
+    se[si] = s.atom_begin + t.n;
+    const int nb = static_cast<int>(t.bond_k.size()), na = static_cast<int>(t.angle_k.size());
+    const int nd = static_cast<int>(t.dihedrals.size() / 4), ni = static_cast<int>(t.imp_k.size());
+    sb[n_sys + si] = ob; se[n_sys + si] = ob += nb;
+    sb[2 * n_sys + si] = oa; se[2 * n_sys + si] = oa += na;
+    sb[3 * n_sys + si] = od; se[3 * n_sys + si] = od += nd;
+    sb[4 * n_sys + si] = oi; se[4 * n_sys + si] = oi += ni;
+  }
+  OG_CUDA(e->bonded_e.grow(std::max(1, e->n_bonds + e->n_angles + e->n_dih + e->n_imp), st));
+  OG_CUDA(e->seg_begin.upload(sb, st));
+  OG_CUDA(e->seg_end.upload(se, st));
+  return OG_OK;
+}
+
+// SHAKE clusters of system si from its constraints listed in `cons`: each
+// cluster is one heavy atom's X-H constraints in constraint order, clusters
+// in order of their heavy atom's first constraint.  `taken` holds the heavy
+// atoms (system-local) that already have a cluster on the device; a
+// constraint on one of those cannot be appended.
+og_status append_clusters(og_engine* e, int si, const std::vector<int>& cons, const std::set<int>& taken,
+                          cudaStream_t st) {
+  const SysHost& s = e->sys[si];
+  const TopoCopy& t = s.topo;
+  std::map<int, std::vector<int>> by_heavy;
+  std::vector<int> order;
+  for (int k : cons) {
+    const int a = t.cons[2 * k], b = t.cons[2 * k + 1];
+    const int heavy = (t.element[a] == 0) ? b : a;
+    if (taken.count(heavy)) return og_fail(OG_E_BADARG, "a new constraint joins an existing SHAKE cluster");
+    if (by_heavy.find(heavy) == by_heavy.end()) order.push_back(heavy);
+    by_heavy[heavy].push_back(k);
+  }
+  std::vector<int32_t> hcs, hcsys;
+  std::vector<int2> hca;
+  std::vector<double> hcd;
+  const int base = static_cast<int>(e->cons_atoms.n);
+  for (int h : order) {
+    for (int k : by_heavy[h]) {
+      hca.push_back(make_int2(s.atom_begin + t.cons[2 * k], s.atom_begin + t.cons[2 * k + 1]));
+      hcd.push_back(t.cons_d[k] * t.cons_d[k]);
+    }
+    hcs.push_back(base + static_cast<int32_t>(hca.size()));
+    hcsys.push_back(si);
+  }
+  OG_CUDA(append(e->cl_start, hcs, st));
+  OG_CUDA(append(e->cl_sys, hcsys, st));
+  OG_CUDA(append(e->cons_atoms, hca, st));
+  OG_CUDA(append(e->cons_d2, hcd, st));
+  e->n_clusters += static_cast<int>(hcsys.size());
+  return OG_OK;
+}
+
+og_status upload_sys_tiles(og_engine* e, cudaStream_t st) {
+  std::vector<int2> hst;
+  for (const auto& s : e->sys) hst.push_back(make_int2(s.tile_begin, s.n_tiles));
+  OG_CUDA(e->sys_tiles.upload(hst, st));
+  return OG_OK;
+}
+
+// Scratch of the surface term for the current task counts: the term records
+// of one force evaluation (proteins average a few exposed arcs per C/S atom
+// and reach 19; 16 per atom on average is the limit, exceeding it is
+// reported as a capacity overflow) and the queue of atoms beyond the default
+// arrangement capacities (force path and area queries alike).
+og_status size_sasa_scratch(og_engine* e, cudaStream_t st) {
+  if (e->p.include_sasa) {
+    e->sasa_term_cap = 16 * e->n_sasa_tasks + 1024;
+    OG_CUDA(e->sasa_arc_terms.grow(e->sasa_term_cap, st));
+    OG_CUDA(e->sasa_vertex_terms.grow(e->sasa_term_cap, st));
+  }
+  OG_CUDA(e->sasa_overflow.grow(std::max(1, std::max(e->n_sasa_all, e->n_sasa_tasks)), st));
+  return OG_OK;
+}
+
+// Per-atom buffers of the learned-radius network (born_mode 1).
+og_status size_lgb_scratch(og_engine* e, cudaStream_t st) {
+  const size_t np = static_cast<size_t>(e->n_padded);
+  OG_CUDA(e->lgb_x.grow(np * ogk::kLgbIn, st));
+  OG_CUDA(e->lgb_rcfa.grow(np, st));
+  OG_CUDA(e->lgb_ha.grow(np * ogk::kLgbHidden, st));
+  OG_CUDA(e->lgb_hb.grow(np * ogk::kLgbHidden, st));
+  for (auto* v : {&e->lgb_fx, &e->lgb_fy, &e->lgb_fz}) OG_CUDA(v->grow(np, st));
+  return OG_OK;
+}
+
+ogk::SysState sys_state_of(const og_engine* e, int si) {
+  const SysHost& s = e->sys[si];
+  const int ncons = static_cast<int>(s.topo.cons_d.size());
+  const double dof = 3.0 * s.topo.n;
+  ogk::SysState h{};
+  h.temperature = s.temperature;
+  h.kbt = ogk::kBoltzmann * s.temperature;
+  h.dof_corr = (e->p.constrain_h_bonds && ncons > 0) ? dof / std::max(dof - ncons, 1.0) : 1.0;
+  h.atom_begin = s.atom_begin;
+  h.n_atoms = s.topo.n;
+  return h;
+}
+
 og_status finalize_impl(og_engine* e) {
   const int n_sys = static_cast<int>(e->sys.size());
   if (n_sys == 0) return og_fail(OG_E_STATE, "no systems added");
@@ -811,44 +1266,18 @@ og_status finalize_impl(og_engine* e) {
   const int np = e->n_padded;
 
   // ---- per-atom arrays
-  std::vector<double> hx(np), hy(np), hz(np), hm(np, 1.0), him(np, 1.0), hq(np, 0.0), hrm(np, 0.0), hep(np, 0.0),
-      hrm14(np, 0.0), hep14(np, 0.0), hrho(np, 1.0), hrt(np, 1.0), hsr(np, 0.0);
-  std::vector<int32_t> hsys(np, -1), hloc(np, 0), hvalid(np, 0);
-  std::vector<float> hlj(4 * static_cast<size_t>(np), 0.0f);  // tile-SoA: rmin, sqrt eps, rmin14, sqrt eps14
-  for (int si = 0; si < n_sys; ++si) {
-    const SysHost& s = e->sys[si];
-    const TopoCopy& t = s.topo;
-    for (int k = 0; k < t.n; ++k) {
-      const int i = s.atom_begin + k;
-      hx[i] = s.xyz[3 * k];
-      hy[i] = s.xyz[3 * k + 1];
-      hz[i] = s.xyz[3 * k + 2];
-      hm[i] = t.mass[k];
-      him[i] = 1.0 / t.mass[k];
-      hq[i] = t.charge[k];
-      hrm[i] = t.rmin[k];
-      hep[i] = t.eps[k];
-      hrm14[i] = t.rmin14[k];
-      hep14[i] = t.eps14[k];
-      hrho[i] = t.rho[k];
-      hrt[i] = t.rho[k] - ogk::kObcOffset;
-      hsr[i] = t.scale[k] * hrt[i];
-      hsys[i] = si;
-      hloc[i] = k;
-      hvalid[i] = 1;
-      hlj[ogk::soa_index(i, 0)] = static_cast<float>(t.rmin[k]);
-      hlj[ogk::soa_index(i, 1)] = static_cast<float>(std::sqrt(t.eps[k]));
-      hlj[ogk::soa_index(i, 2)] = static_cast<float>(t.rmin14[k]);
-      hlj[ogk::soa_index(i, 3)] = static_cast<float>(std::sqrt(t.eps14[k]));
-    }
+  for (auto* v : {&e->mass, &e->inv_mass, &e->q, &e->rmin, &e->eps, &e->rmin14, &e->eps14, &e->rho, &e->rho_tilde,
+                  &e->srho, &e->sasa_r, &e->sasa_gamma, &e->x, &e->y, &e->z, &e->vx, &e->vy, &e->vz, &e->rx,
+                  &e->ry, &e->rz})
+    OG_CUDA(v->alloc(np));
+  for (auto* v : {&e->atom_sys, &e->local_idx, &e->atom_valid, &e->lgb_class}) OG_CUDA(v->alloc(np));
+  OG_CUDA(e->lj.alloc(4 * static_cast<size_t>(np)));
+  OG_CUDA(e->gb.alloc(4 * static_cast<size_t>(np)));
+  {
+    og_status fs = fill_atoms(e, 0, np, st);
+    if (fs == OG_OK) fs = fill_positions(e, 0, np, st);
+    if (fs != OG_OK) return fs;
   }
-  OG_CUDA(e->x.upload(hx, st)); OG_CUDA(e->y.upload(hy, st)); OG_CUDA(e->z.upload(hz, st));
-  OG_CUDA(e->mass.upload(hm, st)); OG_CUDA(e->inv_mass.upload(him, st)); OG_CUDA(e->q.upload(hq, st));
-  OG_CUDA(e->rmin.upload(hrm, st)); OG_CUDA(e->eps.upload(hep, st));
-  OG_CUDA(e->rmin14.upload(hrm14, st)); OG_CUDA(e->eps14.upload(hep14, st));
-  OG_CUDA(e->rho.upload(hrho, st)); OG_CUDA(e->rho_tilde.upload(hrt, st)); OG_CUDA(e->srho.upload(hsr, st));
-  OG_CUDA(e->atom_sys.upload(hsys, st)); OG_CUDA(e->local_idx.upload(hloc, st));
-  OG_CUDA(e->atom_valid.upload(hvalid, st)); OG_CUDA(e->lj.upload(hlj, st));
   {
     std::vector<int32_t> hmap;
     for (const auto& s : e->sys)
@@ -856,73 +1285,28 @@ og_status finalize_impl(og_engine* e) {
     e->n_real = static_cast<int64_t>(hmap.size());
     OG_CUDA(e->real_map.upload(hmap, st));
   }
-  std::vector<double> zeros(np, 0.0);
-  OG_CUDA(e->vx.upload(zeros, st)); OG_CUDA(e->vy.upload(zeros, st)); OG_CUDA(e->vz.upload(zeros, st));
-  OG_CUDA(e->rx.upload(zeros, st)); OG_CUDA(e->ry.upload(zeros, st)); OG_CUDA(e->rz.upload(zeros, st));
   for (auto* v : {&e->born_r, &e->born_r64, &e->integral64, &e->e_lj, &e->e_coul, &e->e_gb, &e->e_self})
     OG_CUDA(v->alloc(np));
   for (auto* v : {&e->fx, &e->fy, &e->fz, &e->born_sum}) OG_CUDA(v->alloc(np));
   OG_CUDA(e->n_pairs.alloc(np));
   OG_CUDA(e->pq.alloc(4 * static_cast<size_t>(np)));
-  // The Born pass reads rho~ and s*rho~ before the first radii exist, so the
-  // gb columns start out fully defined (R = rho~ until then).
-  std::vector<float> hgb(4 * static_cast<size_t>(np));
-  for (int i = 0; i < np; ++i) {
-    const bool real = hsys[i] >= 0;
-    hgb[ogk::soa_index(i, 0)] = real ? static_cast<float>(hrt[i]) : 1.0f;
-    hgb[ogk::soa_index(i, 1)] = real ? static_cast<float>(1.0 / hrt[i]) : 1.0f;
-    hgb[ogk::soa_index(i, 2)] = real ? static_cast<float>(hrt[i]) : 1.0f;
-    hgb[ogk::soa_index(i, 3)] = real ? static_cast<float>(hsr[i]) : 0.0f;
-  }
-  OG_CUDA(e->gb.upload(hgb, st));
   OG_CUDA(e->origin.alloc(e->n_tiles));
 
-  // ---- SASA tables: radius = Bondi vdW + 1.4 A probe, surface tension
-  // 0.005 kcal/mol/A^2 on C and S (powersasa/mod.rs:27-52), times
-  // sasa_gamma_scale (analytical.rs:607-614).
+  // ---- SASA task lists, term records, overflow queue (radius and tension
+  // per atom come with the per-atom arrays)
   {
-    static const double kVdw[6] = {1.20, 1.70, 1.55, 1.52, 1.80, 1.80};
-    const double g_cs = 0.005 * ogk::kKcalToKj * e->p.sasa_gamma_scale;
-    std::vector<double> hr(np, 0.0), hg(np, 0.0);
     std::vector<int32_t> htask, hall;
-    std::vector<int2> hst(n_sys);
-    double rmax = 0.0;
-    for (int si = 0; si < n_sys; ++si) {
-      const SysHost& s = e->sys[si];
-      hst[si] = make_int2(s.tile_begin, s.n_tiles);
-      for (int k = 0; k < s.topo.n; ++k) {
-        const int el = s.topo.element[k];
-        if (el < 0 || el > 5) return og_fail(OG_E_BADARG, "element code out of range");
-        const int i = s.atom_begin + k;
-        hr[i] = kVdw[el] + 1.4;
-        hg[i] = (el == 1 || el == 5) ? g_cs : 0.0;
-        rmax = std::max(rmax, hr[i]);
-        hall.push_back(i);
-        if (hg[i] != 0.0) htask.push_back(i);
-      }
-    }
-    e->sasa_rmax = rmax;
+    for (int si = 0; si < n_sys; ++si) sasa_lists(e, si, 0, e->sys[si].topo.n, &htask, &hall);
     e->n_sasa_tasks = static_cast<int>(htask.size());
     e->n_sasa_all = static_cast<int>(hall.size());
-    OG_CUDA(e->sasa_r.upload(hr, st));
-    OG_CUDA(e->sasa_gamma.upload(hg, st));
     OG_CUDA(e->sasa_tasks.upload(htask, st));
     OG_CUDA(e->sasa_all.upload(hall, st));
-    OG_CUDA(e->sys_tiles.upload(hst, st));
+    og_status ts = upload_sys_tiles(e, st);
+    if (ts != OG_OK) return ts;
     OG_CUDA(e->sasa_area.alloc(np));
     OG_CUDA(e->sasa_energy.alloc(np));
-    if (e->p.include_sasa) {
-      // Term records of one force evaluation: proteins average a few exposed
-      // arcs per C/S atom and reach 19; 16 per atom on average is the limit
-      // (exceeding it is reported as a capacity overflow).
-      e->sasa_term_cap = 16 * e->n_sasa_tasks + 1024;
-      OG_CUDA(e->sasa_arc_terms.alloc(e->sasa_term_cap));
-      OG_CUDA(e->sasa_vertex_terms.alloc(e->sasa_term_cap));
-    }
-    // counters and the queue of atoms beyond the default arrangement
-    // capacities: used by the force path and by area queries alike
     OG_CUDA(e->sasa_counts.alloc(4));
-    OG_CUDA(e->sasa_overflow.alloc(std::max(1, std::max(e->n_sasa_all, e->n_sasa_tasks))));
+    if ((ts = size_sasa_scratch(e, st)) != OG_OK) return ts;
     // Component probes: Fibonacci points, golden angle pi (3 - sqrt 5),
     // joined when their dot product exceeds cos(2.5 sqrt(4 pi / N))
     // (arrangement.rs:327-391).
@@ -957,14 +1341,9 @@ og_status finalize_impl(og_engine* e) {
     OG_CUDA(ogk::sasa_prepare());
   }
 
-  // ---- learned Born radii: descriptor class per atom (C,S -> 0; N,P -> 1;
-  // O -> 2; H -> 3), buffers when born_mode = 1
+  // ---- learned Born radii: buffers when born_mode = 1 (the descriptor
+  // class comes with the per-atom arrays)
   {
-    static const int32_t kClass[6] = {3, 0, 1, 2, 1, 0};
-    std::vector<int32_t> hc(np, 0);
-    for (int si = 0; si < n_sys; ++si)
-      for (int k = 0; k < e->sys[si].topo.n; ++k) hc[e->sys[si].atom_begin + k] = kClass[e->sys[si].topo.element[k]];
-    OG_CUDA(e->lgb_class.upload(hc, st));
     OG_CUDA(ogk::tc_gemm_prepare());
     OG_CUDA(ogk::lgb_mlp_prepare());
     int dev = 0;
@@ -973,29 +1352,16 @@ og_status finalize_impl(og_engine* e) {
     const char* unf = std::getenv("OG_LGB_UNFUSED");
     e->lgb_unfused = unf && unf[0] == '1';
     if (e->p.born_mode == 1) {
-      OG_CUDA(e->lgb_x.alloc(static_cast<size_t>(np) * ogk::kLgbIn));
-      OG_CUDA(e->lgb_rcfa.alloc(np));
-      OG_CUDA(e->lgb_ha.alloc(static_cast<size_t>(np) * ogk::kLgbHidden));
-      OG_CUDA(e->lgb_hb.alloc(static_cast<size_t>(np) * ogk::kLgbHidden));
+      og_status ls = size_lgb_scratch(e, st);
+      if (ls != OG_OK) return ls;
       OG_CUDA(e->lgb_params.alloc(ogk::kLgbNParams));
-      for (auto* v : {&e->lgb_fx, &e->lgb_fy, &e->lgb_fz}) OG_CUDA(v->alloc(np));
       OG_CUDA(e->lgb_part.alloc(2 * static_cast<size_t>(n_sys)));
     }
   }
 
   // ---- per-system state
   std::vector<ogk::SysState> hs(n_sys);
-  for (int si = 0; si < n_sys; ++si) {
-    const SysHost& s = e->sys[si];
-    const int ncons = static_cast<int>(s.topo.cons_d.size());
-    const double dof = 3.0 * s.topo.n;
-    hs[si] = ogk::SysState{};
-    hs[si].temperature = s.temperature;
-    hs[si].kbt = ogk::kBoltzmann * s.temperature;
-    hs[si].dof_corr = (e->p.constrain_h_bonds && ncons > 0) ? dof / std::max(dof - ncons, 1.0) : 1.0;
-    hs[si].atom_begin = s.atom_begin;
-    hs[si].n_atoms = s.topo.n;
-  }
+  for (int si = 0; si < n_sys; ++si) hs[si] = sys_state_of(e, si);
   OG_CUDA(e->sys_state.upload(hs, st));
 
   // ---- pair work lists (build_pair_lists) and the persistent-launch queues
@@ -1006,180 +1372,34 @@ og_status finalize_impl(og_engine* e) {
   }
 
   // ---- exclusion masks (per ordered tile pair) and the FP64 CSR
-  std::map<std::pair<int, int>, int> mask_of;  // (ti, tj) -> block
-  std::vector<uint32_t> mex, m14;
-  auto block = [&](int ti, int tj) {
-    auto it = mask_of.find({ti, tj});
-    if (it != mask_of.end()) return it->second;
-    int b = static_cast<int>(mask_of.size());
-    mask_of[{ti, tj}] = b;
-    mex.resize(static_cast<size_t>(b + 1) * kTile, 0u);
-    m14.resize(static_cast<size_t>(b + 1) * kTile, 0u);
-    return b;
-  };
-  std::vector<std::vector<std::pair<int, int8_t>>> rows(np);
-  for (const auto& s : e->sys) {
-    for (int t = 0; t < s.n_tiles; ++t) {  // self pairs on the diagonal
-      const int tile = s.tile_begin + t;
-      const int b = block(tile, tile);
-      for (int l = 0; l < kTile; ++l) mex[static_cast<size_t>(b) * kTile + l] |= 1u << l;
-    }
-    const auto& ex = s.topo.excl;
-    for (size_t k = 0; k < s.topo.excl_kind.size(); ++k) {
-      const int i = s.atom_begin + ex[2 * k], j = s.atom_begin + ex[2 * k + 1];
-      const int8_t kind = s.topo.excl_kind[k];
-      rows[i].push_back({j, kind});
-      rows[j].push_back({i, kind});
-      for (int dir = 0; dir < 2; ++dir) {
-        const int a = dir ? j : i, c = dir ? i : j;
-        const int b = block(a / kTile, c / kTile);
-        const size_t w = static_cast<size_t>(b) * kTile + (a % kTile);
-        if (kind == 1) mex[w] |= 1u << (c % kTile);
-        else m14[w] |= 1u << (c % kTile);
-      }
-    }
-  }
-  std::vector<int32_t> hmb(e->n_tiles + 1, 0);
-  std::vector<ogk::TileMaskRef> hmr;
   {
-    std::vector<std::vector<ogk::TileMaskRef>> per_tile(e->n_tiles);
-    for (const auto& kv : mask_of) per_tile[kv.first.first].push_back({kv.first.second, kv.second});
-    for (int t = 0; t < e->n_tiles; ++t) {
-      std::sort(per_tile[t].begin(), per_tile[t].end(),
-                [](const ogk::TileMaskRef& a, const ogk::TileMaskRef& b) { return a.j_tile < b.j_tile; });
-      hmb[t] = static_cast<int32_t>(hmr.size());
-      hmr.insert(hmr.end(), per_tile[t].begin(), per_tile[t].end());
-    }
-    hmb[e->n_tiles] = static_cast<int32_t>(hmr.size());
+    e->tile_refs.assign(e->n_tiles, {});
+    e->excl_rows.assign(np, {});
+    int t_min = 0, a_min = 0;
+    std::set<int> touched;
+    for (const auto& s : e->sys) mask_diagonal(e, s.tile_begin, s.tile_begin + s.n_tiles, &t_min, &touched);
+    for (int si = 0; si < n_sys; ++si)
+      for (size_t k = 0; k < e->sys[si].topo.excl_kind.size(); ++k) mask_exclusion(e, si, k, &t_min, &a_min, &touched);
+    og_status xs = upload_exclusions(e, 0, 0, 0, 0, touched, st);
+    if (xs != OG_OK) return xs;
   }
-  std::vector<int4> hnear;  // unordered: the (i_tile <= j_tile) orientation's block
-  for (const auto& kv : mask_of)
-    if (kv.first.first <= kv.first.second)
-      hnear.push_back(make_int4(kv.first.first, kv.first.second, kv.second, 0));
-  e->n_near = static_cast<int>(hnear.size());
-  OG_CUDA(e->near.upload(hnear, st));
-  OG_CUDA(e->mask_begin.upload(hmb, st));
-  OG_CUDA(e->mask_refs.upload(hmr, st));
-  OG_CUDA(e->mask_ex.upload(mex, st));
-  OG_CUDA(e->mask_14.upload(m14, st));
-  std::vector<int32_t> hrow(np + 1, 0), hcol;
-  std::vector<int8_t> hkind;
-  for (int i = 0; i < np; ++i) {
-    auto& r = rows[i];
-    std::sort(r.begin(), r.end());
-    hrow[i] = static_cast<int32_t>(hcol.size());
-    for (auto& pr : r) {
-      hcol.push_back(pr.first);
-      hkind.push_back(pr.second);
-    }
-  }
-  hrow[np] = static_cast<int32_t>(hcol.size());
-  OG_CUDA(e->excl_row.upload(hrow, st));
-  OG_CUDA(e->excl_col.upload(hcol, st));
-  OG_CUDA(e->excl_kind.upload(hkind, st));
 
-  // ---- bonded terms (global atom indices, angles in radians)
-  std::vector<int2> hb, hdt;
-  std::vector<int4> ha, hd, hi;
-  std::vector<double> hbk, hbr, hak, hat, htk, htd, hik, hip;
-  std::vector<int32_t> htn;
-  std::vector<int32_t> sb(5 * n_sys), se(5 * n_sys);
+  // ---- bonded terms, reduction segments, SHAKE clusters
   for (int si = 0; si < n_sys; ++si) {
-    const SysHost& s = e->sys[si];
-    const TopoCopy& t = s.topo;
-    const int o = s.atom_begin;
-    sb[si] = o;
-    se[si] = o + t.n;
-    sb[n_sys + si] = static_cast<int32_t>(hb.size());
-    for (size_t k = 0; k < t.bond_k.size(); ++k) {
-      hb.push_back(make_int2(o + t.bonds[2 * k], o + t.bonds[2 * k + 1]));
-      hbk.push_back(t.bond_k[k]);
-      hbr.push_back(t.bond_r0[k]);
-    }
-    se[n_sys + si] = static_cast<int32_t>(hb.size());
-    sb[2 * n_sys + si] = static_cast<int32_t>(ha.size());
-    for (size_t k = 0; k < t.angle_k.size(); ++k) {
-      ha.push_back(make_int4(o + t.angles[3 * k], o + t.angles[3 * k + 1], o + t.angles[3 * k + 2], 0));
-      hak.push_back(t.angle_k[k]);
-      hat.push_back(deg2rad(t.angle_t0[k]));
-    }
-    se[2 * n_sys + si] = static_cast<int32_t>(ha.size());
-    sb[3 * n_sys + si] = static_cast<int32_t>(hd.size());
-    const size_t ndih = t.dihedrals.size() / 4;
-    for (size_t k = 0; k < ndih; ++k) {
-      hd.push_back(make_int4(o + t.dihedrals[4 * k], o + t.dihedrals[4 * k + 1], o + t.dihedrals[4 * k + 2],
-                             o + t.dihedrals[4 * k + 3]));
-      const int base = static_cast<int>(htk.size());
-      for (int m = t.dih_start[k]; m < t.dih_start[k + 1]; ++m) {
-        htk.push_back(t.term_k[m]);
-        htn.push_back(t.term_n[m]);
-        htd.push_back(deg2rad(t.term_delta[m]));
-      }
-      hdt.push_back(make_int2(base, static_cast<int>(htk.size())));
-    }
-    se[3 * n_sys + si] = static_cast<int32_t>(hd.size());
-    sb[4 * n_sys + si] = static_cast<int32_t>(hi.size());
-    for (size_t k = 0; k < t.imp_k.size(); ++k) {
-      hi.push_back(make_int4(o + t.impropers[4 * k], o + t.impropers[4 * k + 1], o + t.impropers[4 * k + 2],
-                             o + t.impropers[4 * k + 3]));
-      hik.push_back(t.imp_k[k]);
-      hip.push_back(deg2rad(t.imp_psi0[k]));
-    }
-    se[4 * n_sys + si] = static_cast<int32_t>(hi.size());
+    og_status bs = append_bonded(e, si, TermSel::all(e->sys[si].topo), st);
+    if (bs != OG_OK) return bs;
   }
-  e->n_bonds = static_cast<int>(hb.size());
-  e->n_angles = static_cast<int>(ha.size());
-  e->n_dih = static_cast<int>(hd.size());
-  e->n_imp = static_cast<int>(hi.size());
-  // Segments of the bonded energy array: bonds, then angles, dihedrals, impropers.
-  for (int si = 0; si < n_sys; ++si) {
-    sb[2 * n_sys + si] += e->n_bonds; se[2 * n_sys + si] += e->n_bonds;
-    sb[3 * n_sys + si] += e->n_bonds + e->n_angles; se[3 * n_sys + si] += e->n_bonds + e->n_angles;
-    sb[4 * n_sys + si] += e->n_bonds + e->n_angles + e->n_dih;
-    se[4 * n_sys + si] += e->n_bonds + e->n_angles + e->n_dih;
+  {
+    og_status ss = upload_segments(e, st);
+    if (ss != OG_OK) return ss;
   }
-  OG_CUDA(e->bond_atoms.upload(hb, st)); OG_CUDA(e->bond_k.upload(hbk, st)); OG_CUDA(e->bond_r0.upload(hbr, st));
-  OG_CUDA(e->angle_atoms.upload(ha, st)); OG_CUDA(e->angle_k.upload(hak, st)); OG_CUDA(e->angle_t0.upload(hat, st));
-  OG_CUDA(e->dih_atoms.upload(hd, st)); OG_CUDA(e->dih_terms.upload(hdt, st));
-  OG_CUDA(e->term_k.upload(htk, st)); OG_CUDA(e->term_n.upload(htn, st)); OG_CUDA(e->term_delta.upload(htd, st));
-  OG_CUDA(e->imp_atoms.upload(hi, st)); OG_CUDA(e->imp_k.upload(hik, st)); OG_CUDA(e->imp_psi0.upload(hip, st));
-  OG_CUDA(e->bonded_e.alloc(std::max(1, e->n_bonds + e->n_angles + e->n_dih + e->n_imp)));
-  OG_CUDA(e->seg_begin.upload(sb, st));
-  OG_CUDA(e->seg_end.upload(se, st));
   OG_CUDA(e->seg_out.alloc(9 * static_cast<size_t>(n_sys)));  // energy terms: 5 per-atom + 4 bonded
-
-  // ---- SHAKE clusters: constraints grouped by their heavy atom, in
-  // constraint order inside a cluster.
-  std::vector<int32_t> hcs(1, 0), hcsys;
-  std::vector<int2> hca;
-  std::vector<double> hcd;
-  if (e->p.constrain_h_bonds) {
+  OG_CUDA(append(e->cl_start, std::vector<int32_t>(1, 0), st));
+  if (e->p.constrain_h_bonds)
     for (int si = 0; si < n_sys; ++si) {
-      const SysHost& s = e->sys[si];
-      const TopoCopy& t = s.topo;
-      std::map<int, std::vector<int>> by_heavy;
-      std::vector<int> order;
-      for (size_t k = 0; k < t.cons_d.size(); ++k) {
-        const int a = t.cons[2 * k], b = t.cons[2 * k + 1];
-        const int heavy = (t.element[a] == 0) ? b : a;
-        if (by_heavy.find(heavy) == by_heavy.end()) order.push_back(heavy);
-        by_heavy[heavy].push_back(static_cast<int>(k));
-      }
-      for (int h : order) {
-        for (int k : by_heavy[h]) {
-          hca.push_back(make_int2(s.atom_begin + t.cons[2 * k], s.atom_begin + t.cons[2 * k + 1]));
-          hcd.push_back(t.cons_d[k] * t.cons_d[k]);
-        }
-        hcs.push_back(static_cast<int32_t>(hca.size()));
-        hcsys.push_back(si);
-      }
+      og_status cs = append_clusters(e, si, TermSel::all(e->sys[si].topo).cons, {}, st);
+      if (cs != OG_OK) return cs;
     }
-  }
-  e->n_clusters = static_cast<int>(hcsys.size());
-  OG_CUDA(e->cl_start.upload(hcs, st));
-  OG_CUDA(e->cl_sys.upload(hcsys, st));
-  OG_CUDA(e->cons_atoms.upload(hca, st));
-  OG_CUDA(e->cons_d2.upload(hcd, st));
 
   OG_CUDA(e->clamp_count.alloc(n_sys));
   OG_CUDA(e->sys_nonfinite.alloc(n_sys));
@@ -1280,6 +1500,194 @@ og_status build_graph(og_engine* e) {
   return OG_OK;
 }
 
+// ---- co-translational growth
+
+// Whether `grown` extends `base`: more atoms, the first base.n with the same
+// parameters bit for bit, and, in every term list (bonds, angles, dihedrals
+// with their Fourier terms, impropers, exclusions, constraints), the records
+// among those atoms equal to base's records in base's order (a grown chain's
+// topology lists them so: appending a residue adds atoms after the old ones
+// and terms that touch them).  On success `d` lists the records of `grown`
+// that touch a new atom, in grown's order; else the reason is returned.
+std::string topology_delta(const TopoCopy& base, const TopoCopy& grown, TermSel* d) {
+  const int n_old = base.n;
+  if (grown.n <= n_old) return "the grown topology has no new atoms";
+  auto same_prefix = [n_old](const auto& a, const auto& b) {
+    return std::memcmp(a.data(), b.data(), sizeof(a[0]) * static_cast<size_t>(n_old)) == 0;
+  };
+  if (!same_prefix(base.charge, grown.charge) || !same_prefix(base.rmin, grown.rmin) ||
+      !same_prefix(base.eps, grown.eps) || !same_prefix(base.rmin14, grown.rmin14) ||
+      !same_prefix(base.eps14, grown.eps14) || !same_prefix(base.rho, grown.rho) ||
+      !same_prefix(base.scale, grown.scale) || !same_prefix(base.mass, grown.mass) ||
+      !same_prefix(base.element, grown.element))
+    return "the parameters of the existing atoms differ";
+  // One list: `arity` atom indices per record; same(g, b) compares the
+  // records' parameters.
+  auto split = [n_old](const char* what, int arity, const std::vector<int32_t>& ga, const std::vector<int32_t>& ba,
+                       auto same, std::vector<int>* out) -> std::string {
+    const size_t gn = ga.size() / arity, bn = ba.size() / arity;
+    size_t k = 0;
+    for (size_t g = 0; g < gn; ++g) {
+      bool is_new = false;
+      for (int c = 0; c < arity; ++c) is_new |= ga[g * arity + c] >= n_old;
+      if (is_new) {
+        out->push_back(static_cast<int>(g));
+        continue;
+      }
+      bool eq = k < bn && same(g, k);
+      for (int c = 0; eq && c < arity; ++c) eq = ga[g * arity + c] == ba[k * arity + c];
+      if (!eq) return std::string(what) + " among the existing atoms differ";
+      ++k;
+    }
+    if (k != bn) return std::string(what) + " among the existing atoms differ";
+    return "";
+  };
+  std::string why;
+  why = split("bonds", 2, grown.bonds, base.bonds, [&](size_t g, size_t b) {
+    return grown.bond_k[g] == base.bond_k[b] && grown.bond_r0[g] == base.bond_r0[b];
+  }, &d->bonds);
+  if (!why.empty()) return why;
+  why = split("angles", 3, grown.angles, base.angles, [&](size_t g, size_t b) {
+    return grown.angle_k[g] == base.angle_k[b] && grown.angle_t0[g] == base.angle_t0[b];
+  }, &d->angles);
+  if (!why.empty()) return why;
+  why = split("dihedrals", 4, grown.dihedrals, base.dihedrals, [&](size_t g, size_t b) {
+    const int g0 = grown.dih_start[g], g1 = grown.dih_start[g + 1], b0 = base.dih_start[b], b1 = base.dih_start[b + 1];
+    if (g1 - g0 != b1 - b0) return false;
+    for (int m = 0; m < g1 - g0; ++m)
+      if (grown.term_k[g0 + m] != base.term_k[b0 + m] || grown.term_n[g0 + m] != base.term_n[b0 + m] ||
+          grown.term_delta[g0 + m] != base.term_delta[b0 + m])
+        return false;
+    return true;
+  }, &d->dihedrals);
+  if (!why.empty()) return why;
+  why = split("impropers", 4, grown.impropers, base.impropers, [&](size_t g, size_t b) {
+    return grown.imp_k[g] == base.imp_k[b] && grown.imp_psi0[g] == base.imp_psi0[b];
+  }, &d->impropers);
+  if (!why.empty()) return why;
+  why = split("exclusions", 2, grown.excl, base.excl,
+              [&](size_t g, size_t b) { return grown.excl_kind[g] == base.excl_kind[b]; }, &d->excl);
+  if (!why.empty()) return why;
+  return split("constraints", 2, grown.cons, base.cons,
+               [&](size_t g, size_t b) { return grown.cons_d[g] == base.cons_d[b]; }, &d->cons);
+}
+
+// og_engine_append_atoms: system si (the engine's last) takes the atoms and
+// terms that `grown` adds.  Only what the new atoms touch changes on the
+// device: the per-atom tables from the tile holding the first new atom on,
+// the new atoms' positions and velocities, the exclusion-mask blocks and
+// CSR rows the new exclusions reach, the new bonded terms and SHAKE clusters
+// appended to their lists, the system's reduction segments and state.  The
+// existing atoms' positions, velocities and step count stay where they are
+// on the device.  The pair work lists are rebuilt only when the system gains
+// a tile.
+og_status append_impl(og_engine* e, int si, const TopoCopy& grown, const double* xyz_new, const double* v_new) {
+  SysHost& sh = e->sys[si];
+  TermSel d;
+  const std::string why = topology_delta(sh.topo, grown, &d);
+  if (!why.empty()) return og_fail(OG_E_BADARG, "og_engine_append_atoms: " + why);
+  cudaStream_t st = e->stream;
+  const int n_old = sh.topo.n, n_new = grown.n, n_add = n_new - n_old;
+  const int old_tiles = e->n_tiles, old_np = e->n_padded;
+  std::set<int> old_heavy;  // system-local heavy atoms with a SHAKE cluster on the device
+  for (size_t k = 0; k < sh.topo.cons_d.size(); ++k) {
+    const int a = sh.topo.cons[2 * k], b = sh.topo.cons[2 * k + 1];
+    old_heavy.insert(sh.topo.element[a] == 0 ? b : a);
+  }
+  sh.topo = grown;
+  sh.xyz.resize(3 * static_cast<size_t>(n_old));
+  sh.xyz.insert(sh.xyz.end(), xyz_new, xyz_new + 3 * static_cast<size_t>(n_add));
+  sh.n_tiles = (n_new + kTile - 1) / kTile;
+  const int np = sh.atom_begin + sh.n_tiles * kTile;
+  e->n_padded = np;
+  e->n_tiles = np / kTile;
+
+  // per-atom arrays: grown in place (contents kept), then the static tables
+  // of the tiles from the first new atom's on and the new atoms' state
+  for (auto* v : {&e->x, &e->y, &e->z, &e->vx, &e->vy, &e->vz, &e->rx, &e->ry, &e->rz, &e->mass, &e->inv_mass,
+                  &e->q, &e->rmin, &e->eps, &e->rmin14, &e->eps14, &e->rho, &e->rho_tilde, &e->srho, &e->born_r,
+                  &e->born_r64, &e->integral64, &e->e_lj, &e->e_coul, &e->e_gb, &e->e_self, &e->sasa_r,
+                  &e->sasa_gamma, &e->sasa_area, &e->sasa_energy})
+    OG_CUDA(v->grow(np, st));
+  for (auto* v : {&e->fx, &e->fy, &e->fz, &e->born_sum}) OG_CUDA(v->grow(np, st));
+  for (auto* v : {&e->atom_sys, &e->local_idx, &e->atom_valid, &e->n_pairs, &e->lgb_class})
+    OG_CUDA(v->grow(np, st));
+  for (auto* v : {&e->pq, &e->lj, &e->gb}) OG_CUDA(v->grow(4 * static_cast<size_t>(np), st));
+  OG_CUDA(e->origin.grow(e->n_tiles, st));
+  const int a_first = sh.atom_begin + n_old;
+  og_status s = fill_atoms(e, a_first / kTile * kTile, np, st);
+  if (s == OG_OK) s = fill_positions(e, a_first, np, st);
+  if (s != OG_OK) return s;
+  if (v_new) {
+    std::vector<double> hv[3];
+    for (int c = 0; c < 3; ++c) {
+      hv[c].resize(n_add);
+      for (int k = 0; k < n_add; ++k) hv[c][k] = v_new[3 * k + c];
+    }
+    OG_CUDA(put(e->vx, a_first, hv[0], st));
+    OG_CUDA(put(e->vy, a_first, hv[1], st));
+    OG_CUDA(put(e->vz, a_first, hv[2], st));
+  }
+  {
+    std::vector<int32_t> hmap(n_add);
+    for (int k = 0; k < n_add; ++k) hmap[k] = a_first + k;
+    OG_CUDA(append(e->real_map, hmap, st));
+    e->n_real += n_add;
+  }
+  if (e->p.born_mode == 1 && (s = size_lgb_scratch(e, st)) != OG_OK) return s;
+
+  // surface term: task lists, scratch
+  {
+    std::vector<int32_t> htask, hall;
+    sasa_lists(e, si, n_old, n_new, &htask, &hall);
+    OG_CUDA(append(e->sasa_tasks, htask, st));
+    OG_CUDA(append(e->sasa_all, hall, st));
+    e->n_sasa_tasks += static_cast<int>(htask.size());
+    e->n_sasa_all += static_cast<int>(hall.size());
+    if ((s = size_sasa_scratch(e, st)) != OG_OK) return s;
+    if ((s = upload_sys_tiles(e, st)) != OG_OK) return s;
+  }
+
+  // exclusions: the new tiles' diagonal blocks and the new exclusions
+  {
+    const int n_blocks = static_cast<int>(e->mask_of.size()), n_near = static_cast<int>(e->h_near.size());
+    e->tile_refs.resize(e->n_tiles);
+    e->excl_rows.resize(np);
+    int t_min = e->n_tiles, a_min = np;
+    std::set<int> touched;
+    mask_diagonal(e, old_tiles, e->n_tiles, &t_min, &touched);
+    for (int k : d.excl) mask_exclusion(e, si, static_cast<size_t>(k), &t_min, &a_min, &touched);
+    if ((s = upload_exclusions(e, n_blocks, std::min(t_min, old_tiles), std::min(a_min, old_np), n_near, touched,
+                               st)) != OG_OK)
+      return s;
+  }
+
+  // bonded terms and SHAKE clusters of the new atoms, appended
+  if ((s = append_bonded(e, si, d, st)) != OG_OK) return s;
+  if ((s = upload_segments(e, st)) != OG_OK) return s;
+  if (e->p.constrain_h_bonds && (s = append_clusters(e, si, d.cons, old_heavy, st)) != OG_OK) return s;
+
+  // the system's atom count and degrees of freedom (its step count, status
+  // and temperature stay)
+  {
+    std::vector<ogk::SysState> hs;
+    if ((s = read_status(e, &hs)) != OG_OK) return s;
+    const ogk::SysState fresh = sys_state_of(e, si);
+    hs[si].n_atoms = fresh.n_atoms;
+    hs[si].dof_corr = fresh.dof_corr;
+    OG_CUDA(cudaMemcpyAsync(e->sys_state.p + si, &hs[si], sizeof(ogk::SysState), cudaMemcpyHostToDevice, st));
+  }
+
+  if (e->n_tiles != old_tiles && (s = build_pair_lists(e, st)) != OG_OK) return s;
+  ogk::launch_pack(e->atoms(), true, st);
+  if ((s = launch_check("pack")) != OG_OK) return s;
+  OG_CUDA(cudaStreamSynchronize(st));
+  reset_graph(e);
+  e->remd_ready = false;
+  e->forces_valid = false;
+  return OG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1343,6 +1751,33 @@ og_status og_engine_finalize(og_engine* e) {
   if (!e) return og_fail(OG_E_BADARG, "null engine");
   if (e->finalized) return og_fail(OG_E_STATE, "engine already finalized");
   return finalize_impl(e);
+}
+
+og_status og_topology_extends(const og_topology* base, const og_topology* grown, int32_t* extends) {
+  if (!base || !grown || !extends) return og_fail(OG_E_BADARG, "null argument");
+  TopoCopy b, g;
+  og_status st = copy_topology(base, &b);
+  if (st == OG_OK) st = copy_topology(grown, &g);
+  if (st != OG_OK) return st;
+  TermSel d;
+  const std::string why = topology_delta(b, g, &d);
+  *extends = why.empty() ? 1 : 0;
+  if (!why.empty()) og_fail(OG_E_BADARG, why);  // the reason, for og_last_error
+  return OG_OK;
+}
+
+og_status og_engine_append_atoms(og_engine* e, int32_t s, const og_topology* grown, const double* xyz_new,
+                                 const double* v_new) {
+  og_status st = check_ready(e);
+  if (st != OG_OK) return st;
+  if (s != static_cast<int32_t>(e->sys.size()) - 1)
+    return og_fail(OG_E_BADARG, "og_engine_append_atoms: only the engine's last system can grow");
+  if (!grown || !xyz_new) return og_fail(OG_E_BADARG, "null argument");
+  TopoCopy g;
+  if ((st = copy_topology(grown, &g)) != OG_OK) return st;
+  for (int k = 3 * e->sys[s].topo.n; k < 3 * g.n; ++k)
+    if (!std::isfinite(xyz_new[k - 3 * e->sys[s].topo.n])) return og_fail(OG_E_BADARG, "non-finite position");
+  return append_impl(e, s, g, xyz_new, v_new);
 }
 
 og_status og_engine_n_systems(const og_engine* e, int32_t* n) {
