@@ -101,16 +101,28 @@ def _two_loop(g, hs, hy, hr):
 
 
 def lbfgs(engine, sys: int = 0, opts: MinimizeOptions | None = None) -> MinimizeResult:
-    """Minimise system `sys` of a finalised Engine in place."""
+    """Minimise system `sys` of a finalised Engine in place.
+
+    The reference evaluates the gradient at the top of every iteration and
+    the energy before every line search; both were already taken at that
+    point (the gradient for the last curvature pair y, the energy by the
+    accepted line-search trial).  Device forces and energies are
+    deterministic, so those values are reused instead of recomputed -- the
+    iterates are the same -- which halves the evaluations per iteration.
+    Positions are tracked on the host: the device holds exactly the array
+    last set."""
     o = opts or MinimizeOptions()
     S = _System(engine, sys)
     initial = S.energy()
     e_prev = initial
     hs, hy, hr = deque(), deque(), deque()
     failures, steps, converged, max_force = 0, 0, False, float("inf")
+    x = S.x()
+    g_known, e_known = None, initial
     for step in range(o.max_steps):
         steps = step
-        g = S.grad()
+        g = g_known if g_known is not None else S.grad()
+        g_known = None
         max_force = _norm(g, o.gradient_norm)
         if max_force < o.gradient_tol:
             converged = True
@@ -118,8 +130,7 @@ def lbfgs(engine, sys: int = 0, opts: MinimizeOptions | None = None) -> Minimize
         direction = -g if not hs else _two_loop(g, hs, hy, hr)
         md = float(np.max(np.abs(direction)))
         a0 = min(o.alpha0, o.max_step_a / md) if md > 0 else o.alpha0
-        x = S.x()
-        e_now = S.energy()
+        e_now = e_known if e_known is not None else S.energy()
         res = _backtracking(S, x, direction, g, e_now, a0, o)
         if res is None:
             failures += 1
@@ -130,14 +141,18 @@ def lbfgs(engine, sys: int = 0, opts: MinimizeOptions | None = None) -> Minimize
             if res2 is None:
                 failures += 1
                 break
-            S.set_x(x + res2[0] * sd)
+            x = x + res2[0] * sd
+            S.set_x(x)
             hs.clear(); hy.clear(); hr.clear()
-            e_prev = res2[1]
+            e_prev = e_known = res2[1]
             continue
         alpha, e_new = res
         step_vec = alpha * direction
-        S.set_x(x + step_vec)
-        y = S.grad() - g
+        x = x + step_vec
+        S.set_x(x)
+        g_known = S.grad()
+        e_known = e_new
+        y = g_known - g
         sy = float(step_vec @ y)
         if sy > 1e-12:
             if len(hs) == o.history:
@@ -148,7 +163,8 @@ def lbfgs(engine, sys: int = 0, opts: MinimizeOptions | None = None) -> Minimize
             steps = step + 1
             break
         e_prev = e_new
-    return MinimizeResult(steps, initial, S.energy(), max_force, converged, failures)
+    final = e_known if e_known is not None else S.energy()
+    return MinimizeResult(steps, initial, final, max_force, converged, failures)
 
 
 def minimize_chain(chain, params=None, opts: MinimizeOptions | None = None) -> MinimizeResult:
