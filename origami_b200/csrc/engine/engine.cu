@@ -236,6 +236,10 @@ struct og_engine {
   std::vector<int8_t> h_excl_kind;
   std::vector<int4> h_near;
   int n_terms = 0;  // dihedral Fourier terms on the device
+  // FP64 energy path: j ranges per i atom and their partial sums
+  int e_chunks = 1;
+  DVec<double> epart;
+  DVec<int32_t> epart_pairs;
   DVec<ogk::PairWork> work_f;   // far-field force: upper-triangle tile pairs
   DVec<int32_t> jlist_f;
   // cutoff mode: i-blocks of the two lists, their culled j lists and ends
@@ -1235,6 +1239,19 @@ og_status size_lgb_scratch(og_engine* e, cudaStream_t st) {
   return OG_OK;
 }
 
+// Partial-sum buffers of the FP64 energy path for the current layout.
+og_status size_energy_scratch(og_engine* e, cudaStream_t st) {
+  int max_n = 1;
+  for (const auto& s : e->sys) max_n = std::max(max_n, s.topo.n);
+  e->e_chunks = ogk::energy_chunks(e->n_padded, max_n, e->n_sm);
+  if (e->e_chunks > 1) {
+    const size_t m = static_cast<size_t>(e->e_chunks) * e->n_padded;
+    OG_CUDA(e->epart.grow(3 * m, st));
+    OG_CUDA(e->epart_pairs.grow(m, st));
+  }
+  return OG_OK;
+}
+
 ogk::SysState sys_state_of(const og_engine* e, int si) {
   const SysHost& s = e->sys[si];
   const int ncons = static_cast<int>(s.topo.cons_d.size());
@@ -1357,6 +1374,11 @@ og_status finalize_impl(og_engine* e) {
       OG_CUDA(e->lgb_params.alloc(ogk::kLgbNParams));
       OG_CUDA(e->lgb_part.alloc(2 * static_cast<size_t>(n_sys)));
     }
+  }
+
+  {
+    og_status es = size_energy_scratch(e, st);
+    if (es != OG_OK) return es;
   }
 
   // ---- per-system state
@@ -1635,6 +1657,7 @@ og_status append_impl(og_engine* e, int si, const TopoCopy& grown, const double*
     e->n_real += n_add;
   }
   if (e->p.born_mode == 1 && (s = size_lgb_scratch(e, st)) != OG_OK) return s;
+  if ((s = size_energy_scratch(e, st)) != OG_OK) return s;
 
   // surface term: task lists, scratch
   {
@@ -1990,6 +2013,7 @@ og_status og_compute_energies(og_engine* e, int32_t s, og_energies* out) {
   a.integral = e->integral64.p;
   a.e_lj = e->e_lj.p; a.e_coul = e->e_coul.p; a.e_gb = e->e_gb.p; a.e_self = e->e_self.p;
   a.n_pairs = e->n_pairs.p;
+  a.n_chunks = e->e_chunks; a.part = e->epart.p; a.part_pairs = e->epart_pairs.p;
 
   OG_CUDA(cudaMemsetAsync(e->clamp_count.p, 0, sizeof(int32_t) * n_sys, stream));
   ogk::launch_born64(a, stream);
@@ -2412,6 +2436,7 @@ void enqueue_energy_kernels(og_engine* e, cudaStream_t stream) {
   a.integral = e->integral64.p;
   a.e_lj = e->e_lj.p; a.e_coul = e->e_coul.p; a.e_gb = e->e_gb.p; a.e_self = e->e_self.p;
   a.n_pairs = e->n_pairs.p;
+  a.n_chunks = e->e_chunks; a.part = e->epart.p; a.part_pairs = e->epart_pairs.p;
   ogk::launch_born64(a, stream);
   ogk::launch_born_finalize(e->atoms(), e->integral64.p, e->born_r64.p, false, e->clamp_count.p, stream);
   ogk::launch_energy64(a, stream);

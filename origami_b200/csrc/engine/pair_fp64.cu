@@ -1,5 +1,6 @@
 // FP64 pair kernels: the near-field force tiles of the force path and the
 // energy path (Born radii and LJ / Coulomb / GB pair energies).
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -145,21 +146,38 @@ __device__ __forceinline__ double descreen64(double r, double rho_i, double s_rh
   return term1 + term2 + term3 + term4;
 }
 
+// j range `c` of `nc` over a system's atoms [b, b + n).
+__device__ __forceinline__ void chunk_range(int b, int n, int c, int nc, int* j0, int* j1) {
+  *j0 = b + static_cast<int>(static_cast<long long>(n) * c / nc);
+  *j1 = b + static_cast<int>(static_cast<long long>(n) * (c + 1) / nc);
+}
+
 __global__ void k_born64(EnergyArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
   if (i >= a.n_atoms_padded) return;
   const int sys = a.atom_sys[i];
   if (sys < 0) return;
-  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  int j0, j1;
+  chunk_range(a.sys_begin[sys], a.sys_count[sys], c, a.n_chunks, &j0, &j1);
   const double xi = a.x[i], yi = a.y[i], zi = a.z[i], rho = a.rho_tilde[i];
   double acc = 0.0;
-  for (int j = b; j < b + n; ++j) {
+  for (int j = j0; j < j1; ++j) {
     if (j == i) continue;
     const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
     const double r2 = dx * dx + dy * dy + dz * dz;
     if (r2 > a.born_c2 || r2 < 1e-18) continue;
     acc += descreen64(sqrt(r2), rho, a.srho[j]);
   }
+  if (a.n_chunks == 1) a.integral[i] = acc;
+  else a.part[static_cast<size_t>(c) * a.n_atoms_padded + i] = acc;
+}
+
+__global__ void k_born64_sum(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded || a.atom_sys[i] < 0) return;
+  double acc = 0.0;
+  for (int c = 0; c < a.n_chunks; ++c) acc += a.part[static_cast<size_t>(c) * a.n_atoms_padded + i];
   a.integral[i] = acc;
 }
 
@@ -169,21 +187,26 @@ __global__ void k_born64(EnergyArgs a) {
 // is seen from both ends, so the host halves the sums.
 __global__ void k_energy64(EnergyArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
   if (i >= a.n_atoms_padded) return;
   const int sys = a.atom_sys[i];
+  const double pref = -0.5 * (1.0 - 1.0 / kEpsWater) * kCoulomb;
   if (sys < 0) {
-    a.e_lj[i] = a.e_coul[i] = a.e_gb[i] = a.e_self[i] = 0.0;
-    a.n_pairs[i] = 0;
+    if (a.n_chunks == 1) {
+      a.e_lj[i] = a.e_coul[i] = a.e_gb[i] = a.e_self[i] = 0.0;
+      a.n_pairs[i] = 0;
+    }
     return;
   }
-  const int b = a.sys_begin[sys], n = a.sys_count[sys];
+  int j0, j1;
+  chunk_range(a.sys_begin[sys], a.sys_count[sys], c, a.n_chunks, &j0, &j1);
   const double xi = a.x[i], yi = a.y[i], zi = a.z[i], qi = a.q[i], Ri = a.born_r[i];
-  const double pref = -0.5 * (1.0 - 1.0 / kEpsWater) * kCoulomb;
   int ep = a.excl_row[i];
   const int ee = a.excl_row[i + 1];
+  while (ep < ee && a.excl_col[ep] < j0) ++ep;
   double lj = 0.0, coul = 0.0, gb = 0.0;
   int pairs = 0;
-  for (int j = b; j < b + n; ++j) {
+  for (int j = j0; j < j1; ++j) {
     if (j == i) continue;
     const double dx = a.x[j] - xi, dy = a.y[j] - yi, dz = a.z[j] - zi;
     const double r2 = dx * dx + dy * dy + dz * dz;
@@ -213,23 +236,66 @@ __global__ void k_energy64(EnergyArgs a) {
     if (qq != 0.0) coul += kCoulomb * qq * (1.0 / r + a.kappa * r * r - a.crf);
     ++pairs;
   }
+  if (a.n_chunks == 1) {
+    a.e_lj[i] = lj;
+    a.e_coul[i] = coul;
+    a.e_gb[i] = gb;
+    a.e_self[i] = (qi != 0.0) ? pref * (qi * qi) / Ri : 0.0;
+    a.n_pairs[i] = pairs;
+    return;
+  }
+  const size_t np = a.n_atoms_padded, nc = a.n_chunks;
+  a.part[(0 * nc + c) * np + i] = lj;
+  a.part[(1 * nc + c) * np + i] = coul;
+  a.part[(2 * nc + c) * np + i] = gb;
+  a.part_pairs[c * np + i] = pairs;
+}
+
+__global__ void k_energy64_sum(EnergyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_atoms_padded) return;
+  if (a.atom_sys[i] < 0) {
+    a.e_lj[i] = a.e_coul[i] = a.e_gb[i] = a.e_self[i] = 0.0;
+    a.n_pairs[i] = 0;
+    return;
+  }
+  const size_t np = a.n_atoms_padded, nc = a.n_chunks;
+  double lj = 0.0, coul = 0.0, gb = 0.0;
+  int pairs = 0;
+  for (size_t c = 0; c < nc; ++c) {
+    lj += a.part[(0 * nc + c) * np + i];
+    coul += a.part[(1 * nc + c) * np + i];
+    gb += a.part[(2 * nc + c) * np + i];
+    pairs += a.part_pairs[c * np + i];
+  }
+  const double pref = -0.5 * (1.0 - 1.0 / kEpsWater) * kCoulomb;
+  const double qi = a.q[i];
   a.e_lj[i] = lj;
   a.e_coul[i] = coul;
   a.e_gb[i] = gb;
-  a.e_self[i] = (qi != 0.0) ? pref * (qi * qi) / Ri : 0.0;
+  a.e_self[i] = (qi != 0.0) ? pref * (qi * qi) / a.born_r[i] : 0.0;
   a.n_pairs[i] = pairs;
 }
 
 }  // namespace
 
 void launch_born64(const EnergyArgs& a, cudaStream_t s) {
-  const int bs = 128;
-  k_born64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+  const int bs = 128, nb = (a.n_atoms_padded + bs - 1) / bs;
+  k_born64<<<dim3(nb, a.n_chunks), bs, 0, s>>>(a);
+  if (a.n_chunks > 1) k_born64_sum<<<nb, bs, 0, s>>>(a);
 }
 
 void launch_energy64(const EnergyArgs& a, cudaStream_t s) {
-  const int bs = 128;
-  k_energy64<<<(a.n_atoms_padded + bs - 1) / bs, bs, 0, s>>>(a);
+  const int bs = 128, nb = (a.n_atoms_padded + bs - 1) / bs;
+  k_energy64<<<dim3(nb, a.n_chunks), bs, 0, s>>>(a);
+  if (a.n_chunks > 1) k_energy64_sum<<<nb, bs, 0, s>>>(a);
+}
+
+int energy_chunks(int n_atoms_padded, int max_system_atoms, int n_sm) {
+  const int blocks = (n_atoms_padded + 127) / 128;
+  int nc = (8 * n_sm + blocks - 1) / std::max(blocks, 1);
+  nc = std::min(nc, std::max(1, max_system_atoms / 64));
+  return std::max(1, std::min(nc, 32));
 }
 
 }  // namespace ogk

@@ -131,9 +131,20 @@ struct EnergyArgs {
   // outputs, per padded atom
   double* integral;   // born64
   double* e_lj; double* e_coul; double* e_gb; double* e_self; int32_t* n_pairs;
+  // Each i atom's partners are split into n_chunks j ranges, one thread
+  // each (so that a single chain fills the GPU); with more than one, the
+  // range sums go to part ([3][n_chunks][n_atoms_padded] doubles: Born
+  // integral or LJ, Coulomb, GB) and part_pairs, and are added in range
+  // order by a second kernel.
+  int32_t n_chunks;
+  double* part;
+  int32_t* part_pairs;
 };
 
 void launch_born64(const EnergyArgs& a, cudaStream_t s);
 void launch_energy64(const EnergyArgs& a, cudaStream_t s);
+// j ranges per i atom for the FP64 energy path: enough threads for eight
+// 128-thread blocks per SM, at least 64 partners per range, at most 32.
+int energy_chunks(int n_atoms_padded, int max_system_atoms, int n_sm);
 
 }  // namespace ogk
