@@ -685,6 +685,7 @@ def run_c5(args):
                       "steps": t.steps, "slices": t.slices, "residues_emitted": residues, "stopped": stop,
                       "divergence": info,
                       "ns_per_day_dynamics_only": sim_ns / max(t.steps_s, 1e-9) * 86400.0,
+                      "minimisation_iterations": t.minimize_iterations,
                       "seconds": {"dynamics": t.steps_s, "minimisation": t.minimize_s, "engine_builds": t.build_s}}
     # the pair passes on the full-length chain (built extended, relaxed)
     from origami_b200.minimize import MinimizeOptions, minimize_chain

@@ -113,9 +113,11 @@ class CotranslateDiverged(RuntimeError):
 
 @dataclass
 class CotranslateTimings:
-    """Wall time of a run by part (seconds): the per-residue L-BFGS, engine
-    construction (tables, tile lists, graph), and the dynamics slices."""
+    """Wall time of a run by part (seconds): the per-residue L-BFGS (and its
+    iterations), engine construction or growth (tables, tile lists, graph),
+    and the dynamics slices."""
     minimize_s: float = 0.0
+    minimize_iterations: int = 0
     build_s: float = 0.0
     steps_s: float = 0.0
     steps: int = 0
@@ -161,11 +163,12 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
                 chain.append(aa)
             t0 = time.perf_counter()
             if grown is not None:
-                grown.minimize(chain)
+                mres = grown.minimize(chain)
             else:
-                minimize_chain(chain, params=_minimize_params(base), opts=APPEND_MINIMIZE)
+                mres = minimize_chain(chain, params=_minimize_params(base), opts=APPEND_MINIMIZE)
             if timings is not None:
                 timings.minimize_s += time.perf_counter() - t0
+                timings.minimize_iterations += mres.steps
             velocities = seed_new_atom_velocities(chain, velocities, opts.temperature_k, rng)
             target = ribosome.emission_time_fs(i + 1) if i + 1 < len(seq) else clock_fs + tail_steps * opts.dt_fs
             n_steps = int(round(max(target - clock_fs, 0.0) / opts.dt_fs))

@@ -215,8 +215,13 @@ __global__ void k_energy64(EnergyArgs a) {
     if (ep < ee && a.excl_col[ep] == j) kind = a.excl_kind[ep];
     const double qq = qi * a.q[j];
     if (qq != 0.0) {
+      // Once r2 / (4 rp) >= 40, rp exp(-r2 / (4 rp)) < r2 2^-54 (e^-40 <
+      // 160 2^-54, and the gap only widens), below half an ulp of r2, so
+      // r2 + rp exp(...) rounds to r2: the exponential is skipped there
+      // with the same result bit for bit.
       const double rp = Ri * a.born_r[j];
-      const double fgb = sqrt(r2 + rp * exp(-r2 / (4.0 * rp)));
+      const double xg = r2 / (4.0 * rp);
+      const double fgb = xg >= 40.0 ? sqrt(r2) : sqrt(r2 + rp * exp(-xg));
       gb += 2.0 * pref * qq / fgb;
     }
     if (r2 > a.nb_c2 || kind == 1) continue;
