@@ -660,7 +660,7 @@ def run_c5(args):
         stream = torch.cuda.current_stream()
         lgb_params, train_info = train_network(og, args, stream)
     from origami_b200.cotranslate import CotranslateDiverged
-    for born in ("plain", "learned"):
+    for born in args.c5_arms.split(","):
         if born == "learned" and lgb_params is None:
             continue
         p = og.Params.all_pairs(sasa_gamma_scale=0.25, born_mode=1 if born == "learned" else 0)
@@ -708,7 +708,7 @@ def run_c5(args):
     pairs = n * (n - 1) / 2
     force_ms = prof["force_pass"][0] / prof["force_pass"][1]
     born_ms = prof["born_pass"][0] / prof["born_pass"][1]
-    head = arms.get("learned", arms["plain"])
+    head = arms.get("learned") or arms["plain"]
     line = {"metric": "ns/day (cotranslation, 1000 residues into an exit tunnel, GB+SASA)",
             "value": head["ns_per_day"], "unit": "ns/day", "n_gpus": 1, "steps": head["steps"], "warmup": 0,
             "note": "growth stops at the wall budget or a diverged slice (arms[...].stopped); ns/day counts the "
@@ -721,7 +721,8 @@ def run_c5(args):
                                    "L-BFGS after every append",
                        "residues": args.c5_residues, "final_atoms": n},
             "arms": arms,
-            "learned_vs_plain": (arms["learned"]["ns_per_day"] / arms["plain"]["ns_per_day"]) if "learned" in arms
+            "learned_vs_plain": (arms["learned"]["ns_per_day"] / arms["plain"]["ns_per_day"])
+            if "learned" in arms and "plain" in arms
             else None,
             "full_length_pair_passes": {"atoms": n, "pairs": pairs, "force_ms": force_ms, "born_ms": born_ms,
                                         "force_tflops": 55 * pairs / (force_ms * 1e-3) / 1e12,
@@ -765,6 +766,7 @@ def main():
     ap.add_argument("--c5-residues", type=int, default=1000, help="chain length of the c5 run")
     ap.add_argument("--c5-budget", type=float, default=900.0, help="wall seconds of growth per arm in the c5 run")
     ap.add_argument("--c5-dt", type=float, default=2.0, help="time step of the c5 slices (fs)")
+    ap.add_argument("--c5-arms", default="plain,learned", help="Born radii of the c5 runs, in order: plain, learned")
     ap.add_argument("--c5-no-shake", action="store_true",
                     help="c5 slices without SHAKE (the reference's run_slice integrator, with --c5-dt 1)")
     ap.add_argument("--c3a-ps", type=float, default=100.0, help="simulated time of the c3a run per replica (ps)")
