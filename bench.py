@@ -686,6 +686,8 @@ def run_c5(args):
                       "divergence": info,
                       "ns_per_day_dynamics_only": sim_ns / max(t.steps_s, 1e-9) * 86400.0,
                       "minimisation_iterations": t.minimize_iterations,
+                      "judge": {"judgements": t.judges, "slices_ending_learned": t.learned_slices,
+                                "largest_last_error": t.judge_max_error} if born == "learned" else None,
                       "seconds": {"dynamics": t.steps_s, "minimisation": t.minimize_s, "engine_builds": t.build_s}}
     # the pair passes on the full-length chain (built extended, relaxed)
     from origami_b200.minimize import MinimizeOptions, minimize_chain

@@ -122,6 +122,11 @@ class CotranslateTimings:
     steps_s: float = 0.0
     steps: int = 0
     slices: int = 0
+    # learned radii: plain-GB judgements made, slices that ended with the
+    # network still in use, and the largest error a slice's last judgement saw
+    judges: int = 0
+    learned_slices: int = 0
+    judge_max_error: float = -1.0
 
 
 def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: CylindricalTunnel | None = None,
@@ -182,7 +187,8 @@ def run_cotranslate(ribosome, opts: LangevinOptions, tail_steps: int, external: 
                 eng = grown.dynamics(chain, velocities, steps_done)
                 if timings is not None:
                     timings.build_s += time.perf_counter() - t1
-                velocities = _step_slice(eng, chain, velocities, opts, n_steps, clock_fs, i + 1, callback, timings)
+                velocities = _step_slice(eng, chain, velocities, opts, n_steps, clock_fs, i + 1, callback, timings,
+                                         learned=base.born_mode == 1, cumulative_judges=True)
                 clock_fs, steps_done = clock_fs + n_steps * opts.dt_fs, steps_done + n_steps
             else:
                 clock_fs, steps_done, velocities = _run_slice(chain, velocities, opts, n_steps, external, base,
@@ -279,10 +285,13 @@ class _GrowingEngines:
 
 
 def _step_slice(eng: Engine, chain: Chain, velocities: np.ndarray, opts: LangevinOptions, n_steps: int,
-                clock_fs: float, residue_count: int, callback, timings: CotranslateTimings | None) -> np.ndarray:
+                clock_fs: float, residue_count: int, callback, timings: CotranslateTimings | None,
+                learned: bool = False, cumulative_judges: bool = False) -> np.ndarray:
     """n_steps BAOAB steps in save_every chunks (run_slice, cotranslate.rs:
     346-384); the chain takes the final positions, the velocities are
-    returned."""
+    returned.  With learned radii the judge's record goes to `timings`
+    (its judgement count is the engine's running total when
+    cumulative_judges)."""
     t1 = time.perf_counter()
     chunk = opts.save_every if opts.save_every > 0 else n_steps
     done = 0
@@ -303,6 +312,12 @@ def _step_slice(eng: Engine, chain: Chain, velocities: np.ndarray, opts: Langevi
         timings.steps_s += time.perf_counter() - t1
         timings.steps += n_steps
         timings.slices += 1
+        if learned:
+            from . import lgb
+            st = lgb.status(eng)
+            timings.judges = st["judged"] + (0 if cumulative_judges else timings.judges)
+            timings.learned_slices += int(st["active"])
+            timings.judge_max_error = max(timings.judge_max_error, st["last_error"])
     return velocities
 
 
@@ -316,7 +331,8 @@ def _run_slice(chain: Chain, velocities: np.ndarray, opts: LangevinOptions, n_st
     try:
         if timings is not None:
             timings.build_s += time.perf_counter() - t0
-        velocities = _step_slice(eng, chain, velocities, opts, n_steps, clock_fs, residue_count, callback, timings)
+        velocities = _step_slice(eng, chain, velocities, opts, n_steps, clock_fs, residue_count, callback, timings,
+                                 learned=base.born_mode == 1)
     finally:
         eng.close()
     return clock_fs + n_steps * opts.dt_fs, steps_done + n_steps, velocities
