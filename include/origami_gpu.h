@@ -228,7 +228,9 @@ og_status og_engine_finalize(og_engine* e);
  * step count stay on the device.  Device arrays grow by half again when
  * full; the step graph is re-captured at the next og_step.  The force and
  * energy results equal those of an engine built from `grown` (forces bit
- * for bit).  OG_E_BADARG when `grown` does not extend the system. */
+ * for bit).  OG_E_BADARG when `grown` does not extend the system or `sys`
+ * is not the last system; the engine is then unchanged.  After any other
+ * error (a failed device allocation or copy) the engine is to be destroyed. */
 og_status og_engine_append_atoms(og_engine* e, int32_t sys, const og_topology* grown, const double* xyz_new,
                                  const double* v_new);
 /* Host-only check (no GPU): *extends = 1 when `grown` extends `base` --
