@@ -161,3 +161,34 @@ def test_cotranslation_grown_in_place_equals_rebuilt(origami):
         out.append(ch.positions)
     assert out[0].shape == out[1].shape
     assert np.max(np.abs(out[0] - out[1])) < 1e-6
+
+
+def test_last_of_several_systems_grows(origami):
+    """Three systems in one engine, the last one grown: every system's
+    forces equal those of engines built from scratch, the first two
+    untouched; a system other than the last cannot grow."""
+    params = origami.Params.all_pairs(include_sasa=True, sasa_gamma_scale=0.25)
+    chains = [origami.Chain.build(s) for s in ("GAVLK", "MKTWE", "DEF")]
+    eng = origami.Engine(params)
+    for ch in chains:
+        eng.add_system(ch, ch.positions)
+    eng.finalize()
+    before = [eng.total_force(k) for k in range(2)]
+    last = chains[2]
+    for aa in "RYHQNSTPC":  # several tiles' worth of atoms
+        n_old = last.n_atoms
+        last.append(aa)
+        eng.append_atoms(2, last, last.positions[n_old:])
+    with pytest.raises(origami.OrigamiError):
+        grown0 = origami.Chain.build("GAVLK")
+        grown0.append("A")
+        eng.append_atoms(0, grown0, grown0.positions[chains[0].n_atoms:])
+    for k, ch in enumerate(chains):
+        fresh = origami.Engine(params)
+        fresh.add_system(ch, ch.positions)
+        fresh.finalize()
+        np.testing.assert_array_equal(eng.total_force(k), fresh.total_force(0), err_msg=str(k))
+        fresh.close()
+    for k in range(2):
+        np.testing.assert_array_equal(eng.total_force(k), before[k])
+    eng.close()
