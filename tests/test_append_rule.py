@@ -73,5 +73,25 @@ def test_changes_to_old_atoms_or_terms_are_refused():
     ok, why = og.topology_extends(base, t)
     assert not ok and "exclusions" in why
 
+    t = _copy(grown)
+    old = np.flatnonzero((t.dihedrals < base.n_atoms).all(axis=1))
+    t.term_k[t.dihedral_term_start[old[2]]] += 0.25  # one Fourier term of an old dihedral
+    ok, why = og.topology_extends(base, t)
+    assert not ok and "dihedrals" in why
+
+    t = _copy(grown)
+    old = np.flatnonzero((t.constraints < base.n_atoms).all(axis=1))
+    t.constraint_length[old[1]] *= 1.01
+    ok, why = og.topology_extends(base, t)
+    assert not ok and "constraints" in why
+
+    t = _copy(grown)  # an old improper dropped
+    old = np.flatnonzero((t.impropers < base.n_atoms).all(axis=1))
+    keep = np.ones(len(t.improper_k), bool)
+    keep[old[0]] = False
+    t.impropers, t.improper_k, t.improper_psi0 = t.impropers[keep], t.improper_k[keep], t.improper_psi0[keep]
+    ok, why = og.topology_extends(base, t)
+    assert not ok and "impropers" in why
+
     ok, why = og.topology_extends(base, base)
     assert not ok and "no new atoms" in why
